@@ -1,0 +1,127 @@
+/*
+ * velo_obl.h -- C ABI of the B200 (sm_100a) oblivious operator library.
+ *
+ * Plain pointers and sizes only.  Every `d_*` pointer is device memory owned
+ * by the caller; `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).  Entry points enqueue work on the stream and return
+ * without synchronising unless stated otherwise.  All kernels are
+ * data-oblivious: for two inputs of the same public size they issue the same
+ * launches, the same global/shared memory addresses and the same branches.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the reference project root).  Sizes are public: outputs are padded to
+ * public bounds instead of revealing true cardinalities, except where a
+ * function documents that it returns a count (as the reference operators do).
+ */
+#ifndef VELO_OBL_H
+#define VELO_OBL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* status codes (replace the reference's VELODB_THROW / CHECKED_CALL_THROW,  */
+/* include/cuda/helper.hpp:26-48)                                           */
+/* ------------------------------------------------------------------------ */
+typedef int32_t velo_status;
+#define VELO_OK 0
+#define VELO_EINVAL (-1)    /* bad argument (size, alignment, capacity, type) */
+#define VELO_ENOMEM (-2)    /* scratch / arena too small */
+#define VELO_ECUDA (-3)     /* a CUDA runtime call failed; see velo_last_error */
+#define VELO_ETIMEDOUT (-4) /* a bounded wait ran out (host or device side) */
+#define VELO_EOVERFLOW (-5) /* a public bound was exceeded by the data */
+#define VELO_ESTATE (-6)    /* call not valid in the current state */
+#define VELO_ENOTSUP (-7)   /* type or configuration not supported */
+
+/* Column types, numerically equal to DataTypeId
+ * (include/data/data_type.hpp:12-26; device types per
+ * include/data/type_traits.hpp:10-19). */
+typedef enum velo_type {
+    VELO_BOOLEAN = 1,  /* uint8_t */
+    VELO_TINYINT = 2,  /* int8_t */
+    VELO_SMALLINT = 3, /* int16_t */
+    VELO_INTEGER = 4,  /* int32_t */
+    VELO_BIGINT = 5,   /* int64_t */
+    VELO_FLOAT = 6,    /* float */
+    VELO_DOUBLE = 7,   /* double */
+    VELO_VARCHAR = 8,  /* size_t ordinal */
+    VELO_DATE = 10     /* uint32_t */
+} velo_type;
+
+/* Tile configuration of the network kernels: tile = 2^tile_log2 rows per CTA
+ * (11..13; 14 for 12-byte rows), threads = 256/512/1024.  NULL = defaults. */
+typedef struct velo_tune {
+    uint32_t tile_log2;
+    uint32_t threads;
+} velo_tune;
+
+/* nextPow2 (include/cuda/helper.hpp:50-62). */
+size_t velo_next_pow2(size_t x);
+
+/* Text of the last error raised on this host thread ("" if none). */
+const char* velo_last_error_text(void);
+
+/* ------------------------------------------------------------------------ */
+/* Bitonic network sort                                                     */
+/* ------------------------------------------------------------------------ */
+
+/* Oblivious bitonic sort of (u64 key, u32 payload) rows, ascending on
+ * (key, payload).  Replaces OP_SORT / executeBitonicSort
+ * (include/cuda/sort.cuh:70-118, include/cuda/commands.hpp:68-76) for two
+ * sort columns: same network (k ascending, j descending, partner i^j,
+ * direction (i&k)==0), same exchange rule (swap iff strictly out of order),
+ * so the output is identical to the reference network's.  Buffers hold
+ * capacity >= velo_next_pow2(n) rows; rows [n, next_pow2(n)) are filled with
+ * the sentinel (UINT64_MAX, UINT32_MAX) and sort last. */
+velo_status velo_osort_kp(uint64_t* d_keys, uint32_t* d_payload, size_t n, size_t capacity, const velo_tune* tune,
+                          void* stream);
+
+/* Multi-column sort with the reference OP_SORT contract
+ * (include/cuda/sort.cuh:70-118, src/operator/sort_operator.cpp:52-79):
+ * up to 8 sort columns of any velo_type, per-column ascending flags, columns
+ * sorted in place over capacity >= next_pow2(n) rows padded with
+ * max()/lowest(), and d_indices (int64, capacity rows) receiving the
+ * permutation.  Columns are encoded into order-preserving unsigned keys and
+ * sorted by the same network, so ties resolve exactly as in the reference
+ * (floating-point -0.0/+0.0 are ordered by bit pattern; NaN is unsupported).
+ * d_scratch: velo_sort_scratch_bytes() bytes. */
+velo_status velo_sort_columns(void* const* d_cols, const uint32_t* types, const uint8_t* ascending, uint32_t n_cols,
+                              size_t n, size_t capacity, int64_t* d_indices, void* d_scratch, size_t scratch_bytes,
+                              void* stream);
+size_t velo_sort_scratch_bytes(const uint32_t* types, uint32_t n_cols, size_t n);
+
+/* ------------------------------------------------------------------------ */
+/* ORCompact (order-preserving oblivious compaction)                        */
+/* ------------------------------------------------------------------------ */
+
+/* Oblivious compaction of (u64 key, u32 payload, u8 mark) rows: marked rows
+ * move to the front in their original order, unmarked rows follow.  The
+ * routing network is ORCompact as in liboblivious
+ * (obliviator/operator_1/third_party/liboblivious/algorithms.c:116-213),
+ * run over the next_pow2(n) padded rows; it replaces the non-oblivious
+ * OP_SCATTER + OP_GATHER pair (include/cuda/scatter.cuh:16-81,
+ * include/cuda/gather.cuh:28-45, src/operator/filter_compaction_operator.cpp:65-184).
+ * *d_count (u64, device) receives the number of marked rows.
+ * d_scratch: velo_compact_scratch_bytes(capacity) bytes of device memory. */
+velo_status velo_ocompact_kpm(uint64_t* d_keys, uint32_t* d_payload, uint8_t* d_marks, size_t n, size_t capacity,
+                              uint64_t* d_count, void* d_scratch, size_t scratch_bytes, const velo_tune* tune,
+                              void* stream);
+size_t velo_compact_scratch_bytes(size_t capacity, const velo_tune* tune);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* VELO_OBL_H */

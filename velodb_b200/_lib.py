@@ -1,0 +1,75 @@
+"""Loader for ``libvelo_obl.so`` (the C ABI of include/velo_obl.h).
+
+The library is the product: there is no Python or CPU fallback.  If it is not
+built, every entry point raises instead of computing anything.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libvelo_obl.so")
+
+vp, sz, u32, u64, i32, i64, u8 = C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64, C.c_uint8
+
+# name -> (restype, argtypes); every function of include/velo_obl.h
+PROTOS = {
+    "velo_next_pow2": (sz, [sz]),
+    "velo_last_error_text": (C.c_char_p, []),
+    "velo_osort_kp": (i32, [vp, vp, sz, sz, vp, vp]),
+    "velo_sort_columns": (i32, [vp, vp, vp, u32, sz, sz, vp, vp, sz, vp]),
+    "velo_sort_scratch_bytes": (sz, [vp, u32, sz]),
+    "velo_ocompact_kpm": (i32, [vp, vp, vp, sz, sz, vp, vp, sz, vp, vp]),
+    "velo_compact_scratch_bytes": (sz, [sz, vp]),
+}
+
+STATUS = {0: "VELO_OK", -1: "VELO_EINVAL", -2: "VELO_ENOMEM", -3: "VELO_ECUDA", -4: "VELO_ETIMEDOUT",
+          -5: "VELO_EOVERFLOW", -6: "VELO_ESTATE", -7: "VELO_ENOTSUP"}
+
+
+class VeloError(RuntimeError):
+    def __init__(self, status: int, what: str, text: str):
+        super().__init__(f"{what}: {STATUS.get(status, status)}: {text}")
+        self.status = status
+
+
+_lib = None
+
+
+class VeloTune(C.Structure):
+    _fields_ = [("tile_log2", C.c_uint32), ("threads", C.c_uint32)]
+
+
+def lib() -> C.CDLL:
+    """The loaded library; raises if it was not built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m velodb_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in PROTOS.items():
+            if hasattr(L, name):
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    t = lib().velo_last_error_text()
+    return t.decode() if t else ""
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise VeloError(status, what, last_error())
+
+
+def tune_ref(tune):
+    """ctypes pointer for an optional (tile_log2, threads) tuple."""
+    if tune is None:
+        return None
+    t = VeloTune(int(tune[0]), int(tune[1]))
+    return C.byref(t)

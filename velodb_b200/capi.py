@@ -1,0 +1,111 @@
+"""Thin Python calls into the C ABI over torch device buffers.
+
+torch only provides device memory and streams here; every byte of the
+operators is computed by the sm_100a kernels in libvelo_obl.so.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ._lib import check, lib, tune_ref
+
+
+def _stream(stream):
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    return stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+
+
+def next_pow2(x: int) -> int:
+    return int(lib().velo_next_pow2(x))
+
+
+def to_dev_u64(a: np.ndarray, capacity: int | None = None, device="cuda") -> torch.Tensor:
+    """Upload a uint64 array into an int64 device tensor of `capacity` rows."""
+    cap = len(a) if capacity is None else capacity
+    t = torch.empty(max(cap, 1), dtype=torch.int64, device=device)
+    if len(a):
+        t[: len(a)].copy_(torch.from_numpy(np.ascontiguousarray(a).view(np.int64)))
+    return t
+
+
+def to_dev_u32(a: np.ndarray, capacity: int | None = None, device="cuda") -> torch.Tensor:
+    cap = len(a) if capacity is None else capacity
+    t = torch.empty(max(cap, 1), dtype=torch.int32, device=device)
+    if len(a):
+        t[: len(a)].copy_(torch.from_numpy(np.ascontiguousarray(a).view(np.int32)))
+    return t
+
+
+def to_dev_u8(a: np.ndarray, capacity: int | None = None, device="cuda") -> torch.Tensor:
+    cap = len(a) if capacity is None else capacity
+    t = torch.zeros(max(cap, 1), dtype=torch.uint8, device=device)
+    if len(a):
+        t[: len(a)].copy_(torch.from_numpy(np.ascontiguousarray(a).astype(np.uint8)))
+    return t
+
+
+def host_u64(t: torch.Tensor, n: int | None = None) -> np.ndarray:
+    a = t.cpu().numpy().view(np.uint64)
+    return a if n is None else a[:n]
+
+
+def host_u32(t: torch.Tensor, n: int | None = None) -> np.ndarray:
+    a = t.cpu().numpy().view(np.uint32)
+    return a if n is None else a[:n]
+
+
+# --------------------------------------------------------------------------
+
+def osort_kp(keys: torch.Tensor, pay: torch.Tensor, n: int, tune=None, stream=None) -> None:
+    """In-place oblivious sort of (u64 key, u32 payload) rows (velo_osort_kp)."""
+    cap = min(keys.numel(), pay.numel())
+    check(lib().velo_osort_kp(keys.data_ptr(), pay.data_ptr(), n, cap, tune_ref(tune), _stream(stream)),
+          "velo_osort_kp")
+
+
+def compact_scratch_bytes(capacity: int, tune=None) -> int:
+    return int(lib().velo_compact_scratch_bytes(capacity, tune_ref(tune)))
+
+
+def ocompact_kpm(keys, pay, marks, n: int, tune=None, stream=None, scratch=None) -> torch.Tensor:
+    """In-place ORCompact of (key, payload, mark) rows; returns the device
+    count tensor (uint64 stored in an int64 tensor)."""
+    cap = min(keys.numel(), pay.numel(), marks.numel())
+    nbytes = compact_scratch_bytes(cap, tune)
+    if scratch is None:
+        scratch = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=keys.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=keys.device)
+    check(lib().velo_ocompact_kpm(keys.data_ptr(), pay.data_ptr(), marks.data_ptr(), n, cap, cnt.data_ptr(),
+                                  scratch.data_ptr(), scratch.numel(), tune_ref(tune), _stream(stream)),
+          "velo_ocompact_kpm")
+    return cnt
+
+
+def sort_scratch_bytes(types, n: int) -> int:
+    t = np.asarray(types, dtype=np.uint32)
+    return int(lib().velo_sort_scratch_bytes(t.ctypes.data, len(t), n))
+
+
+def sort_columns(cols, types, ascending, n: int, stream=None):
+    """Reference OP_SORT contract (velo_sort_columns): sorts the device
+    columns in place over next_pow2(n) rows and returns the int64 indices."""
+    t = np.asarray(types, dtype=np.uint32)
+    a = np.asarray([1 if x else 0 for x in ascending], dtype=np.uint8)
+    ptrs = np.asarray([c.data_ptr() for c in cols], dtype=np.uint64)
+    cap = min(c.numel() * c.element_size() // _elem_size(tt) for c, tt in zip(cols, types)) if cols else 0
+    dev = cols[0].device
+    idx = torch.empty(max(next_pow2(n), 1), dtype=torch.int64, device=dev)
+    nb = sort_scratch_bytes(types, n)
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device=dev)
+    check(lib().velo_sort_columns(ptrs.ctypes.data, t.ctypes.data, a.ctypes.data, len(cols), n, cap, idx.data_ptr(),
+                                  scratch.data_ptr(), scratch.numel(), _stream(stream)), "velo_sort_columns")
+    return idx
+
+
+_SIZES = {1: 1, 2: 1, 3: 2, 4: 4, 5: 8, 6: 4, 7: 8, 8: 8, 10: 4}
+
+
+def _elem_size(t: int) -> int:
+    return _SIZES[int(t)]

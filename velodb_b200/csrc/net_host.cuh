@@ -1,0 +1,155 @@
+// Host-side planning and launching of network passes (plain path: one kernel
+// launch per pass, stream-ordered).  Included by the .cu files that
+// instantiate row types.
+#pragma once
+
+#include <vector>
+
+#include "common.hpp"
+#include "network.cuh"
+
+namespace velo {
+
+template <class R, int LOG_NT, int LOG_E>
+__global__ void __launch_bounds__(1 << LOG_NT)
+    k_net(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
+{
+    extern __shared__ __align__(16) char sm[];
+    Net<R, LOG_NT, LOG_E>::run(c, g, p, tile_prefix, blockIdx.x, sm);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_count_marks(typename R::Cols c, size_t n, int LT, uint32_t* counts)
+{
+    __shared__ uint32_t tmp[33];
+    count_tile<R>(c, n, LT, blockIdx.x, counts, tmp);
+}
+
+__global__ void k_scan_tiles(const uint32_t* counts, int ntiles, uint32_t* prefix, uint64_t* d_count);
+
+// Bitonic pass list for Np = 2^logN rows and tile 2^LT; Lmax fused levels.
+inline void plan_sort(int logN, int LT, int Lmax, std::vector<NetPass>& out)
+{
+    out.push_back(NetPass { P_SORT_TILE, logN < LT ? logN : LT, 0, 0 });
+    for (int K = LT + 1; K <= logN; K++) {
+        int b = K - 1;
+        while (b >= LT) {
+            int L = b - LT + 1;
+            L = L < Lmax ? L : Lmax;
+            out.push_back(NetPass { P_SORT_GLOBAL, K, b, L });
+            b -= L;
+        }
+        out.push_back(NetPass { P_SORT_MERGE, K, 0, 0 });
+    }
+}
+
+// ORCompact pass list (levels bottom-up).
+inline void plan_compact(int logN, int LT, int Lmax, std::vector<NetPass>& out)
+{
+    out.push_back(NetPass { P_COMPACT_TILE, logN < LT ? logN : LT, 0, 0 });
+    int b = LT;
+    while (b < logN) {
+        int L = logN - b;
+        L = L < Lmax ? L : Lmax;
+        out.push_back(NetPass { P_COMPACT_GLOBAL, 0, b + L - 1, L });
+        b += L;
+    }
+}
+
+// Largest dynamic shared memory of one CTA on sm_100 (227 KB).
+constexpr size_t MAX_SMEM_BYTES = 232448;
+
+// Raises the dynamic shared-memory limit of `kern` once per device; `done`
+// must be a static owned by the caller's kernel instantiation.
+template <class Kern>
+inline velo_status ensure_smem(Kern kern, size_t bytes, int (&done)[64])
+{
+    int dev = 0;
+    VELO_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev >= 0 && dev < 64 && done[dev])
+        return VELO_OK;
+    VELO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                  "cudaFuncSetAttribute");
+    if (dev >= 0 && dev < 64)
+        done[dev] = 1;
+    return VELO_OK;
+}
+
+template <class R, int LOG_NT, int LOG_E>
+inline velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::vector<NetPass>& passes,
+                              const uint32_t* tile_prefix, cudaStream_t st)
+{
+    using N = Net<R, LOG_NT, LOG_E>;
+    auto kern = k_net<R, LOG_NT, LOG_E>;
+    bool compact = false;
+    for (const NetPass& p : passes)
+        compact |= (p.kind == P_COMPACT_TILE) || (p.kind == P_COMPACT_GLOBAL);
+    const size_t smem = compact ? N::smem_bytes_compact() : N::smem_bytes_sort();
+    if (smem > MAX_SMEM_BYTES)
+        return einval("tile configuration needs more shared memory than a CTA can have");
+    static int smem_done[64] = {};
+    velo_status rc = ensure_smem(kern, MAX_SMEM_BYTES, smem_done);
+    if (rc != VELO_OK)
+        return rc;
+    const int lt = N::LT;
+    const size_t grid = g.logN > lt ? ((size_t)1 << (g.logN - lt)) : 1;
+    for (const NetPass& p : passes)
+        kern<<<(unsigned)grid, 1 << LOG_NT, smem, st>>>(c, g, p, tile_prefix);
+    VELO_CUDA_TRY(cudaGetLastError(), "network pass launch");
+    return VELO_OK;
+}
+
+template <class R>
+inline velo_status launch_count_scan(const typename R::Cols& c, size_t n, int logN, int LT, uint32_t* counts,
+                                     uint32_t* prefix, uint64_t* d_count, cudaStream_t st)
+{
+    const int ntiles = logN > LT ? 1 << (logN - LT) : 1;
+    k_count_marks<R><<<ntiles, 256, 0, st>>>(c, n, LT, counts);
+    k_scan_tiles<<<1, 1024, 0, st>>>(counts, ntiles, prefix, d_count);
+    VELO_CUDA_TRY(cudaGetLastError(), "mark count launch");
+    return VELO_OK;
+}
+
+// (LOG_NT, LOG_E) pairs compiled for the tunable row types; tile 2^11..2^14
+// rows, 256..1024 threads.
+#define VELO_FOR_TUNES(X)                                                                                              \
+    X(8, 3)                                                                                                            \
+    X(9, 2)                                                                                                            \
+    X(10, 1)                                                                                                           \
+    X(8, 4)                                                                                                            \
+    X(9, 3)                                                                                                            \
+    X(10, 2)                                                                                                           \
+    X(8, 5)                                                                                                            \
+    X(9, 4)                                                                                                            \
+    X(10, 3)                                                                                                           \
+    X(10, 4)
+
+inline bool tune_supported(int log_nt, int log_e)
+{
+#define X(a, b)                                                                                                        \
+    if (log_nt == a && log_e == b)                                                                                     \
+        return true;
+    VELO_FOR_TUNES(X)
+#undef X
+    return false;
+}
+
+inline velo_status resolve_tune(const velo_tune* tune, int def_log_nt, int def_log_e, int* log_nt, int* log_e)
+{
+    if (!tune || tune->tile_log2 == 0) {
+        *log_nt = def_log_nt;
+        *log_e = def_log_e;
+        return VELO_OK;
+    }
+    const int nt = ilog2_floor(tune->threads);
+    if (tune->threads == 0 || (1u << nt) != tune->threads)
+        return einval("velo_tune.threads must be a power of two");
+    const int le = (int)tune->tile_log2 - nt;
+    if (!tune_supported(nt, le))
+        return einval("unsupported velo_tune (tile_log2, threads) combination");
+    *log_nt = nt;
+    *log_e = le;
+    return VELO_OK;
+}
+
+} // namespace velo

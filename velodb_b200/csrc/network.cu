@@ -1,0 +1,145 @@
+// Plain-path entry points of the two networks for (u64 key, u32 payload)
+// rows: velo_osort_kp and velo_ocompact_kpm.
+#include <mutex>
+#include <string>
+
+#include "net_host.cuh"
+
+namespace velo {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg)
+{
+    g_last_error = msg;
+}
+
+__global__ void k_scan_tiles(const uint32_t* counts, int ntiles, uint32_t* prefix, uint64_t* d_count)
+{
+    __shared__ uint32_t tmp[33];
+    scan_tiles(counts, ntiles, prefix, d_count, tmp);
+}
+
+template <class R>
+static velo_status sort_dispatch(const typename R::Cols& c, size_t n, int logN, int log_nt, int log_e,
+                                 cudaStream_t st)
+{
+    std::vector<NetPass> passes;
+    NetGeom g { n, logN, 0 };
+#define X(a, b)                                                                                                        \
+    if (log_nt == a && log_e == b) {                                                                                   \
+        const int lt = a + b;                                                                                          \
+        plan_sort(logN, lt, lt - 5 < 8 ? lt - 5 : 8, passes);                                                          \
+        return launch_net<R, a, b>(c, g, passes, nullptr, st);                                                         \
+    }
+    VELO_FOR_TUNES(X)
+#undef X
+    return einval("unsupported tile configuration");
+}
+
+template <class R>
+static velo_status compact_dispatch(const typename R::Cols& c, size_t n, int logN, int log_nt, int log_e,
+                                    uint32_t* counts, uint32_t* prefix, uint64_t* d_count, cudaStream_t st)
+{
+    std::vector<NetPass> passes;
+    NetGeom g { n, logN, 0 };
+#define X(a, b)                                                                                                        \
+    if (log_nt == a && log_e == b) {                                                                                   \
+        const int lt = a + b;                                                                                          \
+        velo_status rc = launch_count_scan<R>(c, n, logN, lt, counts, prefix, d_count, st);                            \
+        if (rc != VELO_OK)                                                                                             \
+            return rc;                                                                                                 \
+        plan_compact(logN, lt, lt - 5 < 8 ? lt - 5 : 8, passes);                                                       \
+        return launch_net<R, a, b>(c, g, passes, prefix, st);                                                          \
+    }
+    VELO_FOR_TUNES(X)
+#undef X
+    return einval("unsupported tile configuration");
+}
+
+size_t compact_scratch_for(size_t capacity, int lt)
+{
+    const int logN = ilog2_floor(next_pow2(capacity));
+    const size_t ntiles = logN > lt ? (size_t)1 << (logN - lt) : 1;
+    return align_up(ntiles * 4, 256) + align_up((ntiles + 1) * 4, 256);
+}
+
+} // namespace velo
+
+using namespace velo;
+
+extern "C" size_t velo_next_pow2(size_t x)
+{
+    return next_pow2(x);
+}
+
+extern "C" const char* velo_last_error_text(void)
+{
+    return g_last_error.c_str();
+}
+
+extern "C" velo_status velo_osort_kp(uint64_t* d_keys, uint32_t* d_payload, size_t n, size_t capacity,
+                                     const velo_tune* tune, void* stream)
+{
+    if (n == 0)
+        return VELO_OK;
+    if (!d_keys || !d_payload)
+        return einval("velo_osort_kp: null buffer");
+    const size_t np = next_pow2(n);
+    const int logN = ilog2_floor(np);
+    if (logN > MAX_LOGN)
+        return einval("velo_osort_kp: n too large");
+    if (capacity < np)
+        return einval("velo_osort_kp: capacity must be >= next_pow2(n)");
+    int log_nt, log_e;
+    velo_status rc = resolve_tune(tune, 9, 4, &log_nt, &log_e);
+    if (rc != VELO_OK)
+        return rc;
+    if (np == 1)
+        return VELO_OK;
+    RowKP::Cols c { d_keys, d_payload };
+    return sort_dispatch<RowKP>(c, n, logN, log_nt, log_e, (cudaStream_t)stream);
+}
+
+extern "C" size_t velo_compact_scratch_bytes(size_t capacity, const velo_tune* tune)
+{
+    int log_nt = 9, log_e = 4;
+    if (resolve_tune(tune, 9, 4, &log_nt, &log_e) != VELO_OK)
+        return 0;
+    return compact_scratch_for(capacity, log_nt + log_e);
+}
+
+extern "C" velo_status velo_ocompact_kpm(uint64_t* d_keys, uint32_t* d_payload, uint8_t* d_marks, size_t n,
+                                         size_t capacity, uint64_t* d_count, void* d_scratch, size_t scratch_bytes,
+                                         const velo_tune* tune, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n == 0) {
+        if (d_count)
+            VELO_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), st), "cudaMemsetAsync");
+        return VELO_OK;
+    }
+    if (!d_keys || !d_payload || !d_marks)
+        return einval("velo_ocompact_kpm: null buffer");
+    const size_t np = next_pow2(n);
+    const int logN = ilog2_floor(np);
+    if (logN > MAX_LOGN)
+        return einval("velo_ocompact_kpm: n too large");
+    if (capacity < np)
+        return einval("velo_ocompact_kpm: capacity must be >= next_pow2(n)");
+    int log_nt, log_e;
+    velo_status rc = resolve_tune(tune, 9, 4, &log_nt, &log_e);
+    if (rc != VELO_OK)
+        return rc;
+    const int lt = log_nt + log_e;
+    const size_t need = compact_scratch_for(np, lt);
+    if (!d_scratch || scratch_bytes < need) {
+        set_error("velo_ocompact_kpm: scratch must hold velo_compact_scratch_bytes(capacity) bytes");
+        return VELO_ENOMEM;
+    }
+    const size_t ntiles = logN > lt ? (size_t)1 << (logN - lt) : 1;
+    uint32_t* counts = static_cast<uint32_t*>(d_scratch);
+    uint32_t* prefix = reinterpret_cast<uint32_t*>(static_cast<char*>(d_scratch) + align_up(ntiles * 4, 256));
+    RowKPM::Cols c { d_keys, d_payload, d_marks };
+    return compact_dispatch<RowKPM>(c, n, logN, log_nt, log_e, counts, prefix, d_count, st);
+}

@@ -1,0 +1,445 @@
+// Pass kernels of the two oblivious networks on top of the tile engine.
+//
+// Bitonic sort of Np = 2^logN rows with tile T = 2^LT (reference network
+// order, include/cuda/sort.cuh:104-117):
+//   SORT_TILE          phases k = 2..min(T, Np) entirely inside each tile
+//   SORT_GLOBAL(K,b,L) L consecutive levels j = 2^b .. 2^(b-L+1) (all >= T)
+//                      of phase k = 2^K, fused: each CTA holds 2^L strided
+//                      row groups x 2^(LT-L) consecutive rows
+//   SORT_MERGE(K)      levels j = T/2 .. 1 of phase k = 2^K inside each tile
+// ORCompact over Np rows (liboblivious algorithms.c:116-213, evaluated level
+// by level; block offsets come from a prefix count of the marks):
+//   COMPACT_TILE       levels with block size 2 .. T inside each tile
+//   COMPACT_GLOBAL     L consecutive levels with block sizes > T, fused
+#pragma once
+
+#include "engine.cuh"
+
+namespace velo {
+
+enum PassKind : int {
+    P_SORT_TILE = 0,
+    P_SORT_MERGE = 1,
+    P_SORT_GLOBAL = 2,
+    P_COMPACT_TILE = 3,
+    P_COMPACT_GLOBAL = 4,
+};
+
+struct NetGeom {
+    size_t n;  // real rows (public)
+    int logN;  // log2 of the padded size
+    int pad_;
+};
+
+struct NetPass {
+    int kind;
+    int K;    // sort phase (log2 k) / highest tile level for *_TILE passes
+    int b_hi; // GLOBAL: highest global bit of the fused levels
+    int L;    // GLOBAL: number of fused levels
+};
+
+// mark of the row stored at global index g (count pass)
+template <class R>
+struct MarkAt;
+template <>
+struct MarkAt<RowKP> {
+    __device__ __forceinline__ static bool get(const RowKP::Cols&, size_t) { return false; }
+};
+template <>
+struct MarkAt<RowKPM> {
+    __device__ __forceinline__ static bool get(const RowKPM::Cols& c, size_t g) { return c.m[g] != 0; }
+};
+template <int W, int KW>
+struct MarkAt<RowRec<W, KW>> {
+    __device__ __forceinline__ static bool get(const typename RowRec<W, KW>::Cols& c, size_t g)
+    {
+        return (((c.w[0][g] >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
+    }
+};
+
+// exclusive scan of one u32 per thread across the CTA; tmp holds >= 33 u32
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* tmp, uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        inc += (lane >= o) ? y : 0u;
+    }
+    __syncthreads();
+    if (lane == 31)
+        tmp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nw ? tmp[lane] : 0u;
+        uint32_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+            wi += (lane >= o) ? y : 0u;
+        }
+        if (lane < nw)
+            tmp[lane] = wi - w;
+        if (lane == 31)
+            tmp[32] = wi;
+    }
+    __syncthreads();
+    uint32_t r = tmp[warp] + inc - x;
+    *total = tmp[32];
+    return r;
+}
+
+template <class R, int LOG_NT, int LOG_E>
+struct Net {
+    using TL = Tile<LOG_NT, LOG_E>;
+    using Cols = typename R::Cols;
+    static constexpr int E = TL::E;
+    static constexpr int LT = TL::LOG_T;
+    static constexpr int T = TL::T;
+    static constexpr int S0 = LT - LOG_E; // load/store layout (lanes <-> rows 0..31)
+
+    static constexpr size_t smem_rows() { return ((size_t)T * R::SMEM_BYTES + 15) & ~(size_t)15; }
+    static constexpr size_t smem_bytes_sort() { return smem_rows(); }
+    static constexpr size_t smem_bytes_compact() { return smem_rows() + (size_t)T * 4 + 33 * 4; }
+
+    // ---- bitonic compare-exchange on register bit Q -----------------------
+    template <int Q>
+    __device__ __forceinline__ static void bitonic_level(R (&v)[E], const Cols& c, int s, int K, bool dconst,
+                                                         bool asc_c)
+    {
+        const int tid = threadIdx.x;
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            if (e & (1 << Q))
+                continue;
+            const int e2 = e | (1 << Q);
+            const int l = TL::local(s, e, tid);
+            const bool asc = dconst ? asc_c : (((l >> K) & 1) == 0);
+            const bool gt = R::gt(v[e], v[e2], c);
+            const bool lt = R::gt(v[e2], v[e], c);
+            const bool sw = asc ? gt : lt;
+            const R a = R::select(sw, v[e2], v[e]);
+            const R b = R::select(sw, v[e], v[e2]);
+            v[e] = a;
+            v[e2] = b;
+        }
+    }
+
+    __device__ __forceinline__ static void bitonic_q(int q, R (&v)[E], const Cols& c, int s, int K, bool dconst,
+                                                     bool asc_c)
+    {
+        switch (q) {
+        case 0:
+            bitonic_level<0>(v, c, s, K, dconst, asc_c);
+            break;
+        case 1:
+            if constexpr (LOG_E > 1)
+                bitonic_level<1>(v, c, s, K, dconst, asc_c);
+            break;
+        case 2:
+            if constexpr (LOG_E > 2)
+                bitonic_level<2>(v, c, s, K, dconst, asc_c);
+            break;
+        case 3:
+            if constexpr (LOG_E > 3)
+                bitonic_level<3>(v, c, s, K, dconst, asc_c);
+            break;
+        case 4:
+            if constexpr (LOG_E > 4)
+                bitonic_level<4>(v, c, s, K, dconst, asc_c);
+            break;
+        default:
+            break;
+        }
+    }
+
+    // ---- ORCompact exchange on register bit Q (tile-local level) ----------
+    // Level with block size 2^(b+1): pair (l, l + 2^b) inside block S; the
+    // block's offset is P[S] mod 2^(b+1) and its left-half mark count is
+    // P[S + 2^b] - P[S] (P = exclusive prefix of the original marks; block
+    // counts are invariant under the permutations of lower levels).
+    template <int Q>
+    __device__ __forceinline__ static void compact_level_tile(R (&v)[E], const Cols& c, int s, int b,
+                                                              uint32_t p_tile, const uint32_t* pre)
+    {
+        const int tid = threadIdx.x;
+        const uint32_t half = 1u << b;
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            if (e & (1 << Q))
+                continue;
+            const int e2 = e | (1 << Q);
+            const int l = TL::local(s, e, tid);
+            const int S = l & ~(int)(2 * half - 1);
+            const uint32_t ps = p_tile + pre[S];
+            bool sw;
+            if (b == 0) {
+                // compact_offset, n == 2 (algorithms.c:123-128)
+                const bool ml = MarkOf<R>::get(v[e], c), mr = MarkOf<R>::get(v[e2], c);
+                sw = ((!ml) & mr) != ((ps & 1u) == 1u);
+            } else {
+                // compact_offset, n > 2 (algorithms.c:130-152)
+                const uint32_t left = pre[S + half] - pre[S];
+                const uint32_t off = ps & (2 * half - 1);
+                const uint32_t i = (uint32_t)(l - S);
+                const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
+                sw = sb != (i >= ((off + left) & (half - 1)));
+            }
+            const R a = R::select(sw, v[e2], v[e]);
+            const R bb = R::select(sw, v[e], v[e2]);
+            v[e] = a;
+            v[e2] = bb;
+        }
+    }
+
+    template <int Q>
+    __device__ __forceinline__ static void compact_level_global(R (&v)[E], const Cols& c, int s, int b,
+                                                                const uint32_t* tile_prefix, int C, int b_lo,
+                                                                size_t cta_bits)
+    {
+        const int tid = threadIdx.x;
+        const uint64_t half = 1ull << b;
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            if (e & (1 << Q))
+                continue;
+            const int e2 = e | (1 << Q);
+            const int l = TL::local(s, e, tid);
+            const uint64_t g = (uint64_t)(l & ((1 << C) - 1)) | ((uint64_t)(l >> C) << b_lo) | cta_bits;
+            const uint64_t S = g & ~(2 * half - 1);
+            const uint32_t ps = tile_prefix[S >> LT];
+            const uint32_t pm = tile_prefix[(S + half) >> LT];
+            const uint64_t left = pm - ps;
+            const uint64_t off = ps & (2 * half - 1);
+            const uint64_t i = g - S;
+            const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
+            const bool sw = sb != (i >= ((off + left) & (half - 1)));
+            const R a = R::select(sw, v[e2], v[e]);
+            const R bb = R::select(sw, v[e], v[e2]);
+            v[e] = a;
+            v[e2] = bb;
+        }
+    }
+
+    __device__ __forceinline__ static void compact_tile_q(int q, R (&v)[E], const Cols& c, int s, int b,
+                                                          uint32_t p_tile, const uint32_t* pre)
+    {
+        switch (q) {
+        case 0:
+            compact_level_tile<0>(v, c, s, b, p_tile, pre);
+            break;
+        case 1:
+            if constexpr (LOG_E > 1)
+                compact_level_tile<1>(v, c, s, b, p_tile, pre);
+            break;
+        case 2:
+            if constexpr (LOG_E > 2)
+                compact_level_tile<2>(v, c, s, b, p_tile, pre);
+            break;
+        case 3:
+            if constexpr (LOG_E > 3)
+                compact_level_tile<3>(v, c, s, b, p_tile, pre);
+            break;
+        case 4:
+            if constexpr (LOG_E > 4)
+                compact_level_tile<4>(v, c, s, b, p_tile, pre);
+            break;
+        default:
+            break;
+        }
+    }
+
+    __device__ __forceinline__ static void compact_global_q(int q, R (&v)[E], const Cols& c, int s, int b,
+                                                            const uint32_t* tp, int C, int b_lo, size_t cta_bits)
+    {
+        switch (q) {
+        case 0:
+            compact_level_global<0>(v, c, s, b, tp, C, b_lo, cta_bits);
+            break;
+        case 1:
+            if constexpr (LOG_E > 1)
+                compact_level_global<1>(v, c, s, b, tp, C, b_lo, cta_bits);
+            break;
+        case 2:
+            if constexpr (LOG_E > 2)
+                compact_level_global<2>(v, c, s, b, tp, C, b_lo, cta_bits);
+            break;
+        case 3:
+            if constexpr (LOG_E > 3)
+                compact_level_global<3>(v, c, s, b, tp, C, b_lo, cta_bits);
+            break;
+        case 4:
+            if constexpr (LOG_E > 4)
+                compact_level_global<4>(v, c, s, b, tp, C, b_lo, cta_bits);
+            break;
+        default:
+            break;
+        }
+    }
+
+    // ---- one pass over one tile (CTA `cta`) --------------------------------
+    __device__ static void run(const Cols& c, const NetGeom& g, const NetPass& p, const uint32_t* tile_prefix,
+                               int cta, char* sm)
+    {
+        const int tid = threadIdx.x;
+        const size_t Np = (size_t)1 << g.logN;
+        const bool is_global = (p.kind == P_SORT_GLOBAL) || (p.kind == P_COMPACT_GLOBAL);
+        int C = LT, b_lo = 0;
+        size_t cta_bits = (size_t)cta << LT;
+        if (is_global) {
+            C = LT - p.L;
+            b_lo = p.b_hi - p.L + 1;
+            const int lo_bits = b_lo - C;
+            cta_bits = ((size_t)(cta & ((1 << lo_bits) - 1)) << C) | ((size_t)(cta >> lo_bits) << (p.b_hi + 1));
+        }
+        auto gidx = [&](int l) -> size_t {
+            if (!is_global)
+                return cta_bits | (size_t)l;
+            return (size_t)(l & ((1 << C) - 1)) | ((size_t)(l >> C) << b_lo) | cta_bits;
+        };
+        const int smin = is_global ? (C < S0 ? C : S0) : 0;
+
+        R v[E];
+        int s = is_global && p.kind == P_COMPACT_GLOBAL ? smin : S0;
+        const bool first = (p.kind == P_SORT_TILE) || (p.kind == P_COMPACT_TILE);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const size_t gi = gidx(TL::local(s, e, tid));
+            if (first)
+                v[e] = (gi < g.n) ? R::load(c, gi) : R::pad(c);
+            else
+                v[e] = R::load(c, gi);
+        }
+
+        if (p.kind == P_SORT_TILE) {
+            for (int K = 1; K <= p.K; K++) {
+                const bool dconst = K >= LT;
+                const bool asc_c = ((cta_bits >> K) & 1) == 0;
+                for (int b = K - 1; b >= 0; b--) {
+                    const int ns = window_down(b, LOG_E, LT);
+                    if (ns != s) {
+                        TL::transpose(v, s, ns, sm);
+                        s = ns;
+                    }
+                    bitonic_q(b - s, v, c, s, K, dconst, asc_c);
+                }
+            }
+        } else if (p.kind == P_SORT_MERGE) {
+            const bool asc_c = ((cta_bits >> p.K) & 1) == 0;
+            for (int b = LT - 1; b >= 0; b--) {
+                const int ns = window_down(b, LOG_E, LT);
+                if (ns != s) {
+                    TL::transpose(v, s, ns, sm);
+                    s = ns;
+                }
+                bitonic_q(b - s, v, c, s, p.K, true, asc_c);
+            }
+        } else if (p.kind == P_SORT_GLOBAL) {
+            const bool asc_c = ((gidx(0) >> p.K) & 1) == 0;
+            for (int b = p.b_hi; b >= b_lo; b--) {
+                const int lp = C + (b - b_lo);
+                int ns = window_down(lp, LOG_E, LT);
+                ns = ns < smin ? smin : ns;
+                if (ns != s) {
+                    TL::transpose(v, s, ns, sm);
+                    s = ns;
+                }
+                bitonic_q(lp - s, v, c, s, p.K, true, asc_c);
+            }
+        } else if (p.kind == P_COMPACT_TILE) {
+            // prefix of the original marks over the tile, in local-index order
+            uint32_t* pre = reinterpret_cast<uint32_t*>(sm + smem_rows());
+            uint32_t* tmp = pre + T;
+            TL::transpose(v, s, 0, sm);
+            s = 0;
+            uint32_t cnt = 0, m[E];
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                m[e] = cnt;
+                cnt += MarkOf<R>::get(v[e], c) ? 1u : 0u;
+            }
+            uint32_t total;
+            const uint32_t base = block_exclusive_scan(cnt, tmp, &total);
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                pre[TL::local(0, e, tid)] = base + m[e];
+            __syncthreads();
+            const uint32_t p_tile = tile_prefix[cta];
+            for (int b = 0; b < p.K; b++) {
+                const int ns = window_up(b, LOG_E, LT);
+                if (ns != s) {
+                    TL::transpose(v, s, ns, sm);
+                    s = ns;
+                }
+                compact_tile_q(b - s, v, c, s, b, p_tile, pre);
+            }
+        } else { // P_COMPACT_GLOBAL
+            for (int b = b_lo; b <= p.b_hi; b++) {
+                const int lp = C + (b - b_lo);
+                int ns = window_up(lp, LOG_E, LT);
+                ns = ns < smin ? smin : ns;
+                if (ns != s) {
+                    TL::transpose(v, s, ns, sm);
+                    s = ns;
+                }
+                compact_global_q(lp - s, v, c, s, b, tile_prefix, C, b_lo, cta_bits);
+            }
+        }
+
+        if (s < 5) {
+            TL::transpose(v, s, S0, sm);
+            s = S0;
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const size_t gi = gidx(TL::local(s, e, tid));
+            if (gi < Np)
+                R::store(c, gi, v[e]);
+        }
+    }
+};
+
+// mark count of each tile (rows >= n count as unmarked)
+template <class R>
+__device__ __forceinline__ void count_tile(const typename R::Cols& c, size_t n, int LT, int cta, uint32_t* counts,
+                                           uint32_t* tmp)
+{
+    const size_t base = (size_t)cta << LT;
+    const int T = 1 << LT;
+    uint32_t cnt = 0;
+    for (int i = threadIdx.x; i < T; i += blockDim.x) {
+        const size_t gi = base + i;
+        const bool in = gi < n;
+        const size_t gs = in ? gi : 0; // every row index is public: read row 0 for pads
+        cnt += (in & MarkAt<R>::get(c, gs)) ? 1u : 0u;
+    }
+    uint32_t total;
+    block_exclusive_scan(cnt, tmp, &total);
+    if (threadIdx.x == 0)
+        counts[cta] = total;
+}
+
+// exclusive scan of the tile counts into prefix[0..ntiles]; one CTA
+__device__ __forceinline__ void scan_tiles(const uint32_t* counts, int ntiles, uint32_t* prefix, uint64_t* d_count,
+                                           uint32_t* tmp)
+{
+    uint32_t carry = 0;
+    for (int base = 0; base < ntiles; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const uint32_t x = i < ntiles ? counts[i] : 0u;
+        uint32_t total;
+        const uint32_t ex = block_exclusive_scan(x, tmp, &total);
+        if (i < ntiles)
+            prefix[i] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        prefix[ntiles] = carry;
+        if (d_count)
+            *d_count = carry;
+    }
+}
+
+} // namespace velo
