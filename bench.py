@@ -1,0 +1,447 @@
+#!/usr/bin/env python3
+"""Benchmark of the oblivious operator hot path on B200.
+
+Default workload: oblivious filter + group-by over the synthetic
+6,001,215-row lineitem-shaped fact table (predicate -> ORCompact -> bitonic
+sort on (flag1, flag2) -> segmented int64 sums, output padded to 8 groups).
+One step = one pass of that pipeline over one batch of input.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload groupby|sort]
+
+Multi-GPU: one process per GPU (torchrun); the path does not shard, so every
+rank runs an independent replica of the workload ("replicas only") and the
+aggregate throughput is the total rows of all ranks over the slowest rank's
+time.  `--impl reference` times the reference's CPU algorithm (the C oracle
+port in the reference's network order, all host cores) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# --------------------------------------------------------------------------
+# pass-count model (mirrors plan_sort / plan_compact of the library)
+# --------------------------------------------------------------------------
+
+def sort_passes(logn: int, lt: int, lmax: int) -> int:
+    p = 1
+    for k in range(lt + 1, logn + 1):
+        p += -(-(k - lt) // lmax) + 1
+    return p
+
+
+def compact_passes(logn: int, lt: int, lmax: int) -> int:
+    return 1 + (-(-(max(0, logn - lt)) // lmax) if logn > lt else 0)
+
+
+def rdm_psort(np_rows: int) -> int:
+    """Pass count of the survey's algorithmic-bytes model: T = 2^13, L = 8."""
+    m = max(0, int(np.log2(np_rows)) - 13)
+    return 1 + sum(-(-i // 8) + 1 for i in range(1, m + 1))
+
+
+def rdm_pcomp(np_rows: int) -> int:
+    m = max(0, int(np.log2(np_rows)) - 13)
+    return 1 + -(-m // 8)
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"velo_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# workloads (ours)
+# --------------------------------------------------------------------------
+
+class GroupBy:
+    """Config-1 shape: filter + group-by over 6,001,215 rows."""
+    name = "filter_groupby"
+
+    def __init__(self, torch, capi, W, device):
+        self.torch, self.capi = torch, capi
+        self.n = W.LINEITEM_ROWS
+        self.pred = W.LINEITEM_PRED
+        self.G = W.LINEITEM_GROUP_BOUND
+        self.host = W.lineitem(self.n)
+        self.pinned = {k: torch.from_numpy(v).pin_memory() for k, v in self.host.items()}
+        self.dev = {k: torch.empty_like(v, device=device) for k, v in self.pinned.items()}
+        for k in self.dev:
+            self.dev[k].copy_(self.pinned[k])
+        self.scratch = torch.empty(capi.filter_groupby_scratch_bytes(self.n, self.G), dtype=torch.uint8,
+                                   device=device)
+        self.out = torch.empty((self.G, 6), dtype=torch.int64, device=device)
+        self.counts = torch.empty(2, dtype=torch.int64, device=device)
+        self.out_host = torch.empty((self.G, 6), dtype=torch.int64).pin_memory()
+        self.counts_host = torch.empty(2, dtype=torch.int64).pin_memory()
+        self.in_bytes = sum(v.numel() * v.element_size() for v in self.pinned.values())
+        self.np_rows = 1 << int(np.ceil(np.log2(self.n)))
+        self.rec_bytes = 24
+        self.flush_l2 = False  # inputs (156 MB) and records (201 MB) exceed the 126 MB L2
+
+    def step(self):
+        self.capi.filter_groupby(self.dev, self.n, self.pred, self.G, scratch=self.scratch, out=self.out,
+                                 counts=self.counts)
+
+    def step_e2e(self):
+        for k in self.dev:
+            self.dev[k].copy_(self.pinned[k], non_blocking=True)
+        self.step()
+        self.out_host.copy_(self.out, non_blocking=True)
+        self.counts_host.copy_(self.counts, non_blocking=True)
+
+    def d2h_bytes(self):
+        return self.out.numel() * 8 + self.counts.numel() * 8
+
+    def launches(self):
+        logn = int(np.log2(self.np_rows))
+        return 2 + compact_passes(logn, 12, 7) + sort_passes(logn, 12, 7) + 4
+
+    def rdm_bytes(self):
+        npr = self.np_rows
+        pred = self.n * 9
+        comp = self.n * 5 + 2 * npr * 24 * rdm_pcomp(npr)
+        srt = 2 * npr * 40 * rdm_psort(npr)
+        heads = 2 * npr * 40
+        return pred + comp + srt + heads
+
+    def check(self, orc):
+        g, keys, sums = orc.filter_groupby(self.host, self.pred, self.G)
+        out = self.out.cpu().numpy()
+        cnt = self.counts.cpu().numpy()
+        ok = int(cnt[1]) == g and np.array_equal(out[:g, 0], keys.astype(np.int64)) and np.array_equal(
+            out[:g, 1:], sums)
+        return bool(ok)
+
+    def dominant(self, device):
+        """Times the bitonic passes of the pipeline's sort (the dominant
+        kernel) on the pipeline's own record shape: 2^23 rows x 3 words."""
+        return None
+
+
+def make_workload(name, torch, capi, W, device):
+    if name == "groupby":
+        return GroupBy(torch, capi, W, device)
+    if name == "sort":
+        return SortKP(torch, capi, W, device)
+    raise SystemExit(f"unknown workload {name}")
+
+
+class SortKP:
+    """Config-0 shape: plain oblivious sort of 2^20 (u64 key, u32 payload) rows."""
+    name = "plain_sort_2^20"
+
+    def __init__(self, torch, capi, W, device):
+        self.torch, self.capi = torch, capi
+        self.n = 1 << 20
+        keys, pay = W.sort_kp(self.n)
+        self.pinned_k = torch.from_numpy(keys.view(np.int64)).pin_memory()
+        self.pinned_p = torch.from_numpy(pay.view(np.int32)).pin_memory()
+        self.k0 = self.pinned_k.to(device)
+        self.p0 = self.pinned_p.to(device)
+        self.k = torch.empty_like(self.k0)
+        self.p = torch.empty_like(self.p0)
+        self.kh = torch.empty_like(self.pinned_k).pin_memory()
+        self.ph = torch.empty_like(self.pinned_p).pin_memory()
+        self.in_bytes = self.n * 12
+        self.np_rows = self.n
+        self.rec_bytes = 12
+        self.flush_l2 = True  # 12.6 MB fits in L2: flushed between steps
+
+    def step(self):
+        # the network sorts in place: restore the unsorted input first (the
+        # restore is a device copy inside the timed step)
+        self.k.copy_(self.k0)
+        self.p.copy_(self.p0)
+        self.capi.osort_kp(self.k, self.p, self.n)
+
+    def step_e2e(self):
+        self.k.copy_(self.pinned_k, non_blocking=True)
+        self.p.copy_(self.pinned_p, non_blocking=True)
+        self.capi.osort_kp(self.k, self.p, self.n)
+        self.kh.copy_(self.k, non_blocking=True)
+        self.ph.copy_(self.p, non_blocking=True)
+
+    def d2h_bytes(self):
+        return self.n * 12
+
+    def launches(self):
+        return sort_passes(20, 13, 8)
+
+    def rdm_bytes(self):
+        return 2 * self.n * 12 * rdm_psort(self.n)
+
+    def check(self, orc):
+        k = self.k.cpu().numpy().view(np.uint64)
+        p = self.p.cpu().numpy().view(np.uint32)
+        ok_, op_ = orc.bitonic_kp(self.k0.cpu().numpy().view(np.uint64), self.p0.cpu().numpy().view(np.uint32))
+        return bool(np.array_equal(k, ok_) and np.array_equal(p, op_))
+
+    def dominant(self, device):
+        return None
+
+
+# --------------------------------------------------------------------------
+
+def time_steps(torch, fn, steps, flush=None, stream=None):
+    """Per-step CUDA-event durations (ms) of `fn`, flushing L2 between steps
+    outside the timed events when asked."""
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for s, e in evs:
+        if flush is not None:
+            flush()
+        s.record()
+        fn()
+        e.record()
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in evs]
+
+
+def cpu_baseline_groupby(W, orc):
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    n = 1 << 21
+    cols = W.lineitem(n)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores)
+        reps += 1
+        if time.perf_counter() - t0 > 10.0 or reps >= 50:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    del mp
+    return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
+            "sample": f"first {n} rows of the 6,001,215-row table, {reps} runs, OpenMP over all cores"}
+
+
+def cpu_baseline_sort(W, orc):
+    cores = os.cpu_count() or 1
+    n = 1 << 20
+    keys, pay = W.sort_kp(n)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        orc.bitonic_kp(keys, pay, n_threads=cores)
+        reps += 1
+        if time.perf_counter() - t0 > 10.0 or reps >= 200:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
+            "sample": f"full 2^20-row sort, {reps} runs, OpenMP over all cores"}
+
+
+def run_reference(args, rank):
+    """CPU reference arm: the reference's algorithm for the path (the oracle
+    port in the reference's network order) on all host cores, rank 0 only."""
+    if rank != 0:
+        return
+    import oracle as orc
+    from velodb_b200 import workloads as W
+
+    orc.lib()
+    cores = os.cpu_count() or 1
+    if args.workload == "sort":
+        n = 1 << 20
+        keys, pay = W.sort_kp(n)
+        fn = lambda: orc.bitonic_kp(keys, pay, n_threads=cores)  # noqa: E731
+        sample, metric_rows = "full 2^20-row sort per step", n
+    else:
+        # the reference reveals the filtered count and sorts next_pow2(count)
+        # rows (src/operator/filter_compaction_operator.cpp:171-178)
+        n = W.LINEITEM_ROWS
+        cols = W.lineitem(n)
+        fn = lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores)  # noqa: E731
+        sample, metric_rows = "full 6,001,215-row table per step (filtered count revealed)", n
+    for _ in range(args.warmup):
+        fn()
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    ms = 1e3 * float(np.mean(ts))
+    value = metric_rows / (ms / 1e3) / 1e6
+    wl = "plain_sort_2^20" if args.workload == "sort" else "filter_groupby"
+    line = {
+        "impl": "reference", "metric": metric_name(args.workload), "value": value, "unit": "Mrows/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": wl, "rows": metric_rows},
+        "cpu_baseline": {"value": value, "unit": "Mrows/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def metric_name(workload):
+    if workload == "sort":
+        return "oblivious bitonic sort throughput (2^20 rows, u64 key + u32 payload)"
+    return "oblivious filter+group-by input throughput (6,001,215-row fact table)"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "sort"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from velodb_b200 import capi, workloads as W
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
+
+    wl = make_workload(args.workload, torch, capi, W, device)
+    l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=device) if wl.flush_l2 else None
+    flush = (lambda: l2_flush.fill_(1)) if l2_flush is not None else None
+
+    for _ in range(args.warmup):
+        wl.step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    ts = time_steps(torch, wl.step, args.steps, flush)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    ms = float(np.mean(ts))
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    rows_per_step = wl.n
+    value = world * rows_per_step / (ms / 1e3) / 1e6
+
+    # end to end through the public API with host buffers
+    for _ in range(2):
+        wl.step_e2e()
+    torch.cuda.synchronize()
+    te = time_steps(torch, wl.step_e2e, max(3, args.steps // 2))
+    ems = float(np.mean(te))
+    if world > 1:
+        t = torch.tensor([ems], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    e2e = {"value": world * rows_per_step / (ems / 1e3) / 1e6, "unit": "Mrows/s",
+           "h2d_bytes_per_step": int(wl.in_bytes), "d2h_bytes_per_step": int(wl.d2h_bytes()), "ms_per_step": ems}
+
+    # the result of the last step is checked against the oracle (rank 0)
+    peak, peak_kind = hbm_peak()
+    rdm = wl.rdm_bytes()
+    line = {
+        "metric": metric_name(args.workload), "value": value, "unit": "Mrows/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": wl.name, "rows": rows_per_step, "padded_rows": wl.np_rows,
+                   "record_bytes": wl.rec_bytes, "parallelism": f"replicas{world}",
+                   "l2": "flushed between steps" if wl.flush_l2 else "inputs larger than L2"},
+        "e2e": e2e,
+        "gpu_launches": int(wl.launches() * args.steps),
+        "rdm": {"bytes_per_step": int(rdm), "achieved_gbs": rdm / (ms / 1e3) / 1e9,
+                "frac_of_hbm": rdm / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
+        "clocks": clk,
+    }
+    if rank == 0:
+        import oracle as orc
+
+        orc.lib()
+        line["checked_against_oracle"] = wl.check(orc)
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = (cpu_baseline_sort if args.workload == "sort" else cpu_baseline_groupby)(W, orc)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -116,6 +116,84 @@ velo_status velo_ocompact_kpm(uint64_t* d_keys, uint32_t* d_payload, uint8_t* d_
                               void* stream);
 size_t velo_compact_scratch_bytes(size_t capacity, const velo_tune* tune);
 
+/* ------------------------------------------------------------------------ */
+/* Filter + group-by (oblivious)                                            */
+/* ------------------------------------------------------------------------ */
+
+/* Columns of a lineitem-shaped fact table (device pointers, n rows each). */
+typedef struct velo_lineitem {
+    const int32_t* qty;      /* quantity */
+    const int64_t* price;    /* extended price, cents */
+    const int32_t* disc;     /* discount, percent */
+    const int32_t* tax;      /* tax, percent */
+    const int32_t* shipdate; /* ship date, days */
+    const uint8_t* flag1;    /* first group column */
+    const uint8_t* flag2;    /* second group column */
+} velo_lineitem;
+
+/* Conjunctive range predicate lo <= col <= hi on shipdate, disc and qty. */
+typedef struct velo_lineitem_pred {
+    int32_t ship_lo, ship_hi;
+    int32_t disc_lo, disc_hi;
+    int32_t qty_lo, qty_hi;
+} velo_lineitem_pred;
+
+/* flags: sort only next_pow2(filtered count) rows after compaction, reading
+ * the count back to the host first (the reference FilterCompactionOperator
+ * reveals it, src/operator/filter_compaction_operator.cpp:171-178).  Without
+ * this flag the whole pipeline is oblivious and never synchronises. */
+#define VELO_REVEAL_COUNT 1u
+
+/* Oblivious filter + GROUP BY (flag1, flag2) with exact int64 sums:
+ * predicate and record packing on the GPU (replacing the CPU predicate of
+ * src/operator/seq_scan_operator.cpp:38-45), ORCompact of passing rows
+ * (replacing src/operator/filter_compaction_operator.cpp:65-184), bitonic
+ * sort on the group key, segmented sums
+ * (obliviator/operator_2/enclave/scalable_oblivious_join.c:221-262, int64
+ * instead of float), output padded to the public bound group_bound (1..16).
+ * d_out: group_bound rows x 6 int64 = (flag1 << 8 | flag2, count, sum qty,
+ * sum price, sum price*(100-disc), sum price*(100-disc)*(100+tax)) in key
+ * order, unused rows zero.  d_counts: 2 u64 = (rows passing the filter,
+ * number of groups; more groups than group_bound means the bound was too
+ * small and only the first group_bound are written). */
+size_t velo_filter_groupby_scratch_bytes(size_t n, uint32_t group_bound);
+velo_status velo_filter_groupby(const velo_lineitem* cols, size_t n, const velo_lineitem_pred* pred,
+                                uint32_t group_bound, uint32_t flags, int64_t* d_out, uint64_t* d_counts,
+                                void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* PK-FK join + group-by + top-k (oblivious)                                */
+/* ------------------------------------------------------------------------ */
+
+typedef struct velo_join_tables {
+    const int32_t* dim_key;    /* unique keys of the dimension table */
+    const int32_t* dim_date;   /* dimension attribute filtered by date_hi */
+    size_t n_dim;
+    const int32_t* fact_fk;    /* foreign keys into dim_key */
+    const int64_t* fact_price; /* fact attribute, cents; summed per fk */
+    size_t n_fact;
+} velo_join_tables;
+
+typedef struct velo_join_pred {
+    int32_t date_hi;  /* dimension rows with dim_date < date_hi join */
+    int32_t pad_;
+    int64_t price_hi; /* fact rows with fact_price < price_hi join */
+} velo_join_pred;
+
+/* Oblivious PK-FK join, GROUP BY fk with SUM(price) and COUNT, then the k
+ * groups with the largest sums (ties: smaller fk first).  Replaces the
+ * reference's sort-merge join kernels and operator
+ * (include/cuda/sort_merge_join.cuh:63-199,
+ * src/operator/sort_merge_join_operator.cpp:27-257) with union -> bitonic
+ * sort on (key, tag) -> forward fill -> ORCompact -> segmented sums ->
+ * ORCompact of the groups (public bound n_dim) -> bitonic sort on
+ * (sum desc, fk asc).  d_out: k rows x 3 int64 = (fk, sum price, count),
+ * unused rows zero.  d_counts: 2 u64 = (joined fact rows, groups). */
+size_t velo_join_groupby_topk_scratch_bytes(size_t n_dim, size_t n_fact);
+velo_status velo_join_groupby_topk(const velo_join_tables* tables, const velo_join_pred* pred, uint32_t k,
+                                   int64_t* d_out, uint64_t* d_counts, void* d_scratch, size_t scratch_bytes,
+                                   void* stream);
+
 #ifdef __cplusplus
 }
 #endif

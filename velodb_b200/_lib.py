@@ -22,6 +22,10 @@ PROTOS = {
     "velo_sort_scratch_bytes": (sz, [vp, u32, sz]),
     "velo_ocompact_kpm": (i32, [vp, vp, vp, sz, sz, vp, vp, sz, vp, vp]),
     "velo_compact_scratch_bytes": (sz, [sz, vp]),
+    "velo_filter_groupby_scratch_bytes": (sz, [sz, u32]),
+    "velo_filter_groupby": (i32, [vp, sz, vp, u32, u32, vp, vp, vp, sz, vp]),
+    "velo_join_groupby_topk_scratch_bytes": (sz, [sz, sz]),
+    "velo_join_groupby_topk": (i32, [vp, vp, u32, vp, vp, vp, sz, vp]),
 }
 
 STATUS = {0: "VELO_OK", -1: "VELO_EINVAL", -2: "VELO_ENOMEM", -3: "VELO_ECUDA", -4: "VELO_ETIMEDOUT",
@@ -65,6 +69,23 @@ def last_error() -> str:
 def check(status: int, what: str) -> None:
     if status != 0:
         raise VeloError(status, what, last_error())
+
+
+class VeloLineitem(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("qty", "price", "disc", "tax", "shipdate", "flag1", "flag2")]
+
+
+class VeloLineitemPred(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("ship_lo", "ship_hi", "disc_lo", "disc_hi", "qty_lo", "qty_hi")]
+
+
+class VeloJoinTables(C.Structure):
+    _fields_ = [("dim_key", C.c_void_p), ("dim_date", C.c_void_p), ("n_dim", C.c_size_t),
+                ("fact_fk", C.c_void_p), ("fact_price", C.c_void_p), ("n_fact", C.c_size_t)]
+
+
+class VeloJoinPred(C.Structure):
+    _fields_ = [("date_hi", C.c_int32), ("pad_", C.c_int32), ("price_hi", C.c_int64)]
 
 
 def tune_ref(tune):

@@ -109,3 +109,71 @@ _SIZES = {1: 1, 2: 1, 3: 2, 4: 4, 5: 8, 6: 4, 7: 8, 8: 8, 10: 4}
 
 def _elem_size(t: int) -> int:
     return _SIZES[int(t)]
+
+
+REVEAL_COUNT = 1
+LINEITEM_COLS = ("qty", "price", "disc", "tax", "shipdate", "flag1", "flag2")
+
+
+def lineitem_to_device(cols: dict, device="cuda") -> dict:
+    return {k: torch.from_numpy(np.ascontiguousarray(cols[k])).to(device) for k in LINEITEM_COLS}
+
+
+def filter_groupby_scratch_bytes(n: int, group_bound: int) -> int:
+    return int(lib().velo_filter_groupby_scratch_bytes(n, group_bound))
+
+
+def filter_groupby(dcols: dict, n: int, pred: dict, group_bound: int = 8, reveal_count: bool = False,
+                   scratch=None, out=None, counts=None, stream=None):
+    """Oblivious filter + group-by (velo_filter_groupby).  Returns the device
+    tensors (out[group_bound, 6] int64, counts[2] int64)."""
+    from ._lib import VeloLineitem, VeloLineitemPred
+
+    dev = dcols["qty"].device
+    cols = VeloLineitem(*[dcols[k].data_ptr() for k in LINEITEM_COLS])
+    p = VeloLineitemPred(*[int(pred[k]) for k in ("ship_lo", "ship_hi", "disc_lo", "disc_hi", "qty_lo", "qty_hi")])
+    if scratch is None:
+        scratch = torch.empty(filter_groupby_scratch_bytes(n, group_bound), dtype=torch.uint8, device=dev)
+    if out is None:
+        out = torch.empty((group_bound, 6), dtype=torch.int64, device=dev)
+    if counts is None:
+        counts = torch.empty(2, dtype=torch.int64, device=dev)
+    import ctypes as C
+
+    check(lib().velo_filter_groupby(C.byref(cols), n, C.byref(p), group_bound, REVEAL_COUNT if reveal_count else 0,
+                                    out.data_ptr(), counts.data_ptr(), scratch.data_ptr(), scratch.numel(),
+                                    _stream(stream)), "velo_filter_groupby")
+    return out, counts
+
+
+def join_to_device(dim: dict, fact: dict, device="cuda") -> dict:
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+    return dict(dim_key=t(dim["key"]), dim_date=t(dim["date"]), fact_fk=t(fact["fk"]), fact_price=t(fact["price"]))
+
+
+def join_groupby_topk_scratch_bytes(n_dim: int, n_fact: int) -> int:
+    return int(lib().velo_join_groupby_topk_scratch_bytes(n_dim, n_fact))
+
+
+def join_groupby_topk(dt: dict, pred: dict, k: int = 10, scratch=None, out=None, counts=None, stream=None):
+    """Oblivious PK-FK join + group-by + top-k (velo_join_groupby_topk).
+    Returns device tensors out[k, 3] (fk, sum, count) and counts[2]."""
+    import ctypes as C
+
+    from ._lib import VeloJoinPred, VeloJoinTables
+
+    nd, nf = dt["dim_key"].numel(), dt["fact_fk"].numel()
+    dev = dt["dim_key"].device
+    tabs = VeloJoinTables(dt["dim_key"].data_ptr(), dt["dim_date"].data_ptr(), nd, dt["fact_fk"].data_ptr(),
+                          dt["fact_price"].data_ptr(), nf)
+    p = VeloJoinPred(int(pred["date_hi"]), 0, int(pred["price_hi"]))
+    if scratch is None:
+        scratch = torch.empty(join_groupby_topk_scratch_bytes(nd, nf), dtype=torch.uint8, device=dev)
+    if out is None:
+        out = torch.empty((k, 3), dtype=torch.int64, device=dev)
+    if counts is None:
+        counts = torch.empty(2, dtype=torch.int64, device=dev)
+    check(lib().velo_join_groupby_topk(C.byref(tabs), C.byref(p), k, out.data_ptr(), counts.data_ptr(),
+                                       scratch.data_ptr(), scratch.numel(), _stream(stream)),
+          "velo_join_groupby_topk")
+    return out, counts

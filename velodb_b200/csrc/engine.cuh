@@ -44,6 +44,7 @@ struct RowKP {
         uint32_t* p;
     };
     static constexpr int SMEM_BYTES = 12;
+    static constexpr bool FULL_KEY = true;
     __device__ __forceinline__ static RowKP load(const Cols& c, size_t g) { return RowKP { c.k[g], c.p[g] }; }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowKP& r)
     {
@@ -84,6 +85,7 @@ struct RowKPM {
         uint8_t* m;
     };
     static constexpr int SMEM_BYTES = 13;
+    static constexpr bool FULL_KEY = false;
     __device__ __forceinline__ static RowKPM load(const Cols& c, size_t g)
     {
         return RowKPM { c.k[g], c.p[g], (uint32_t)c.m[g] };
@@ -131,6 +133,7 @@ struct RowRec {
         int mark_inv;
     };
     static constexpr int SMEM_BYTES = 8 * W;
+    static constexpr bool FULL_KEY = false;
     __device__ __forceinline__ static RowRec load(const Cols& c, size_t g)
     {
         RowRec r;

@@ -10,14 +10,6 @@
 
 namespace velo {
 
-template <class R, int LOG_NT, int LOG_E>
-__global__ void __launch_bounds__(1 << LOG_NT)
-    k_net(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
-{
-    extern __shared__ __align__(16) char sm[];
-    Net<R, LOG_NT, LOG_E>::run(c, g, p, tile_prefix, blockIdx.x, sm);
-}
-
 template <class R>
 __global__ void __launch_bounds__(256) k_count_marks(typename R::Cols c, size_t n, int LT, uint32_t* counts)
 {
@@ -75,29 +67,12 @@ inline velo_status ensure_smem(Kern kern, size_t bytes, int (&done)[64])
     return VELO_OK;
 }
 
+// Launches `passes` (all bitonic or all ORCompact kinds) over the tiles; one
+// kernel launch per pass.  Defined in net_impl.cuh and explicitly
+// instantiated per row type and tile configuration (net_inst_*.cu).
 template <class R, int LOG_NT, int LOG_E>
-inline velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::vector<NetPass>& passes,
-                              const uint32_t* tile_prefix, cudaStream_t st)
-{
-    using N = Net<R, LOG_NT, LOG_E>;
-    auto kern = k_net<R, LOG_NT, LOG_E>;
-    bool compact = false;
-    for (const NetPass& p : passes)
-        compact |= (p.kind == P_COMPACT_TILE) || (p.kind == P_COMPACT_GLOBAL);
-    const size_t smem = compact ? N::smem_bytes_compact() : N::smem_bytes_sort();
-    if (smem > MAX_SMEM_BYTES)
-        return einval("tile configuration needs more shared memory than a CTA can have");
-    static int smem_done[64] = {};
-    velo_status rc = ensure_smem(kern, MAX_SMEM_BYTES, smem_done);
-    if (rc != VELO_OK)
-        return rc;
-    const int lt = N::LT;
-    const size_t grid = g.logN > lt ? ((size_t)1 << (g.logN - lt)) : 1;
-    for (const NetPass& p : passes)
-        kern<<<(unsigned)grid, 1 << LOG_NT, smem, st>>>(c, g, p, tile_prefix);
-    VELO_CUDA_TRY(cudaGetLastError(), "network pass launch");
-    return VELO_OK;
-}
+velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::vector<NetPass>& passes,
+                       const uint32_t* tile_prefix, cudaStream_t st);
 
 template <class R>
 inline velo_status launch_count_scan(const typename R::Cols& c, size_t n, int logN, int LT, uint32_t* counts,
@@ -123,6 +98,18 @@ inline velo_status launch_count_scan(const typename R::Cols& c, size_t n, int lo
     X(9, 4)                                                                                                            \
     X(10, 3)                                                                                                           \
     X(10, 4)
+
+// the same grid without 2^14-row tiles (compaction rows + prefix exceed smem)
+#define VELO_FOR_TUNES_COMPACT(X)                                                                                      \
+    X(8, 3)                                                                                                            \
+    X(9, 2)                                                                                                            \
+    X(10, 1)                                                                                                           \
+    X(8, 4)                                                                                                            \
+    X(9, 3)                                                                                                            \
+    X(10, 2)                                                                                                           \
+    X(8, 5)                                                                                                            \
+    X(9, 4)                                                                                                            \
+    X(10, 3)
 
 inline bool tune_supported(int log_nt, int log_e)
 {

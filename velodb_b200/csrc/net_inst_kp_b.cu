@@ -1,0 +1,6 @@
+// Instantiations of the network passes for RowKP (tile configurations of the autotuner).
+#include "net_impl.cuh"
+
+VELO_INSTANTIATE_NET(velo::RowKP, 8, 4)
+VELO_INSTANTIATE_NET(velo::RowKP, 9, 3)
+VELO_INSTANTIATE_NET(velo::RowKP, 10, 2)

@@ -52,7 +52,7 @@ static velo_status compact_dispatch(const typename R::Cols& c, size_t n, int log
         plan_compact(logN, lt, lt - 5 < 8 ? lt - 5 : 8, passes);                                                       \
         return launch_net<R, a, b>(c, g, passes, prefix, st);                                                          \
     }
-    VELO_FOR_TUNES(X)
+    VELO_FOR_TUNES_COMPACT(X)
 #undef X
     return einval("unsupported tile configuration");
 }

@@ -13,6 +13,8 @@
 //   COMPACT_GLOBAL     L consecutive levels with block sizes > T, fused
 #pragma once
 
+#include <type_traits>
+
 #include "engine.cuh"
 
 namespace velo {
@@ -90,6 +92,32 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* t
     return r;
 }
 
+// calls f(std::integral_constant<int, v>) for a runtime v in [0, N)
+template <int I, int N, class F>
+__device__ __forceinline__ void static_switch(int v, F& f)
+{
+    if constexpr (I < N) {
+        if (v == I)
+            f(std::integral_constant<int, I> {});
+        else
+            static_switch<I + 1, N>(v, f);
+    }
+}
+
+// exchange decision for the pair (a at the lower index, b): ascending swaps
+// iff a > b, descending iff a < b (strict, as include/cuda/sort.cuh:31-40)
+template <class R>
+__device__ __forceinline__ bool need_swap(const R& a, const R& b, bool desc, const typename R::Cols& c)
+{
+    if constexpr (R::FULL_KEY) {
+        // every field is compared, so equal rows are identical and swapping
+        // them is a no-op: one comparison decides both directions
+        return R::gt(a, b, c) != desc;
+    } else {
+        return desc ? R::gt(b, a, c) : R::gt(a, b, c);
+    }
+}
+
 template <class R, int LOG_NT, int LOG_E>
 struct Net {
     using TL = Tile<LOG_NT, LOG_E>;
@@ -98,27 +126,61 @@ struct Net {
     static constexpr int LT = TL::LOG_T;
     static constexpr int T = TL::T;
     static constexpr int S0 = LT - LOG_E; // load/store layout (lanes <-> rows 0..31)
+    static constexpr int NS = S0 + 1;     // layouts 0..S0
 
     static constexpr size_t smem_rows() { return ((size_t)T * R::SMEM_BYTES + 15) & ~(size_t)15; }
     static constexpr size_t smem_bytes_sort() { return smem_rows(); }
     static constexpr size_t smem_bytes_compact() { return smem_rows() + (size_t)T * 4 + 33 * 4; }
 
-    // ---- bitonic compare-exchange on register bit Q -----------------------
-    template <int Q>
-    __device__ __forceinline__ static void bitonic_level(R (&v)[E], const Cols& c, int s, int K, bool dconst,
-                                                         bool asc_c)
+    // thread part of the local row index in layout S
+    template <int S>
+    __device__ __forceinline__ static int tidpart()
     {
         const int tid = threadIdx.x;
+        return (tid & ((1 << S) - 1)) | ((tid >> S) << (S + LOG_E));
+    }
+
+    template <int S>
+    __device__ __forceinline__ static void sstore_all(const R (&v)[E], char* sm)
+    {
+        const int tp = tidpart<S>();
+#pragma unroll
+        for (int e = 0; e < E; e++)
+            R::sstore(sm, T, TL::swz(tp | (e << S)), v[e]);
+    }
+    template <int S>
+    __device__ __forceinline__ static void sload_all(R (&v)[E], const char* sm)
+    {
+        const int tp = tidpart<S>();
+#pragma unroll
+        for (int e = 0; e < E; e++)
+            v[e] = R::sload(sm, T, TL::swz(tp | (e << S)));
+    }
+
+    // re-layout the tile from layout `from` to layout `to` through smem
+    __device__ __forceinline__ static void transpose(R (&v)[E], int from, int to, char* sm)
+    {
+        __syncthreads();
+        auto st = [&](auto sc) { sstore_all<decltype(sc)::value>(v, sm); };
+        static_switch<0, NS>(from, st);
+        __syncthreads();
+        auto ld = [&](auto sc) { sload_all<decltype(sc)::value>(v, sm); };
+        static_switch<0, NS>(to, ld);
+    }
+
+    // ---- bitonic compare-exchange on register bit Q in layout S -----------
+    template <int S, int Q>
+    __device__ __forceinline__ static void bitonic_level(R (&v)[E], const Cols& c, int K, bool dconst, bool asc_c)
+    {
+        const int tp = tidpart<S>();
+        const bool tdesc = ((tp >> K) & 1) != 0; // thread part of the direction bit
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
                 continue;
             const int e2 = e | (1 << Q);
-            const int l = TL::local(s, e, tid);
-            const bool asc = dconst ? asc_c : (((l >> K) & 1) == 0);
-            const bool gt = R::gt(v[e], v[e2], c);
-            const bool lt = R::gt(v[e2], v[e], c);
-            const bool sw = asc ? gt : lt;
+            const bool desc = dconst ? !asc_c : (tdesc | ((((e << S) >> K) & 1) != 0));
+            const bool sw = need_swap(v[e], v[e2], desc, c);
             const R a = R::select(sw, v[e2], v[e]);
             const R b = R::select(sw, v[e], v[e2]);
             v[e] = a;
@@ -126,53 +188,36 @@ struct Net {
         }
     }
 
-    __device__ __forceinline__ static void bitonic_q(int q, R (&v)[E], const Cols& c, int s, int K, bool dconst,
-                                                     bool asc_c)
+    __device__ __forceinline__ static void bitonic(int s, int q, R (&v)[E], const Cols& c, int K, bool dconst,
+                                                   bool asc_c)
     {
-        switch (q) {
-        case 0:
-            bitonic_level<0>(v, c, s, K, dconst, asc_c);
-            break;
-        case 1:
-            if constexpr (LOG_E > 1)
-                bitonic_level<1>(v, c, s, K, dconst, asc_c);
-            break;
-        case 2:
-            if constexpr (LOG_E > 2)
-                bitonic_level<2>(v, c, s, K, dconst, asc_c);
-            break;
-        case 3:
-            if constexpr (LOG_E > 3)
-                bitonic_level<3>(v, c, s, K, dconst, asc_c);
-            break;
-        case 4:
-            if constexpr (LOG_E > 4)
-                bitonic_level<4>(v, c, s, K, dconst, asc_c);
-            break;
-        default:
-            break;
-        }
+        auto fs = [&](auto sc) {
+            constexpr int S = decltype(sc)::value;
+            auto fq = [&](auto qc) { bitonic_level<S, decltype(qc)::value>(v, c, K, dconst, asc_c); };
+            static_switch<0, LOG_E>(q, fq);
+        };
+        static_switch<0, NS>(s, fs);
     }
 
-    // ---- ORCompact exchange on register bit Q (tile-local level) ----------
-    // Level with block size 2^(b+1): pair (l, l + 2^b) inside block S; the
-    // block's offset is P[S] mod 2^(b+1) and its left-half mark count is
-    // P[S + 2^b] - P[S] (P = exclusive prefix of the original marks; block
-    // counts are invariant under the permutations of lower levels).
-    template <int Q>
-    __device__ __forceinline__ static void compact_level_tile(R (&v)[E], const Cols& c, int s, int b,
-                                                              uint32_t p_tile, const uint32_t* pre)
+    // ---- ORCompact exchange (tile-local level, block size 2^(b+1)) --------
+    // Pair (l, l + 2^b) inside block S; the block's offset is P[S] mod 2^(b+1)
+    // and its left-half mark count is P[S + 2^b] - P[S] (P = exclusive prefix
+    // of the original marks; block counts are invariant under the
+    // permutations of lower levels).
+    template <int S, int Q>
+    __device__ __forceinline__ static void compact_level_tile(R (&v)[E], const Cols& c, int b, uint32_t p_tile,
+                                                              const uint32_t* pre)
     {
-        const int tid = threadIdx.x;
+        const int tp = tidpart<S>();
         const uint32_t half = 1u << b;
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
                 continue;
             const int e2 = e | (1 << Q);
-            const int l = TL::local(s, e, tid);
-            const int S = l & ~(int)(2 * half - 1);
-            const uint32_t ps = p_tile + pre[S];
+            const int l = tp | (e << S);
+            const int blk = l & ~(int)(2 * half - 1);
+            const uint32_t ps = p_tile + pre[blk];
             bool sw;
             if (b == 0) {
                 // compact_offset, n == 2 (algorithms.c:123-128)
@@ -180,9 +225,9 @@ struct Net {
                 sw = ((!ml) & mr) != ((ps & 1u) == 1u);
             } else {
                 // compact_offset, n > 2 (algorithms.c:130-152)
-                const uint32_t left = pre[S + half] - pre[S];
+                const uint32_t left = pre[blk + half] - pre[blk];
                 const uint32_t off = ps & (2 * half - 1);
-                const uint32_t i = (uint32_t)(l - S);
+                const uint32_t i = (uint32_t)(l - blk);
                 const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
                 sw = sb != (i >= ((off + left) & (half - 1)));
             }
@@ -193,26 +238,26 @@ struct Net {
         }
     }
 
-    template <int Q>
-    __device__ __forceinline__ static void compact_level_global(R (&v)[E], const Cols& c, int s, int b,
+    template <int S, int Q>
+    __device__ __forceinline__ static void compact_level_global(R (&v)[E], const Cols& c, int b,
                                                                 const uint32_t* tile_prefix, int C, int b_lo,
                                                                 size_t cta_bits)
     {
-        const int tid = threadIdx.x;
+        const int tp = tidpart<S>();
         const uint64_t half = 1ull << b;
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
                 continue;
             const int e2 = e | (1 << Q);
-            const int l = TL::local(s, e, tid);
+            const int l = tp | (e << S);
             const uint64_t g = (uint64_t)(l & ((1 << C) - 1)) | ((uint64_t)(l >> C) << b_lo) | cta_bits;
-            const uint64_t S = g & ~(2 * half - 1);
-            const uint32_t ps = tile_prefix[S >> LT];
-            const uint32_t pm = tile_prefix[(S + half) >> LT];
+            const uint64_t blk = g & ~(2 * half - 1);
+            const uint32_t ps = tile_prefix[blk >> LT];
+            const uint32_t pm = tile_prefix[(blk + half) >> LT];
             const uint64_t left = pm - ps;
             const uint64_t off = ps & (2 * half - 1);
-            const uint64_t i = g - S;
+            const uint64_t i = g - blk;
             const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
             const bool sw = sb != (i >= ((off + left) & (half - 1)));
             const R a = R::select(sw, v[e2], v[e]);
@@ -222,63 +267,9 @@ struct Net {
         }
     }
 
-    __device__ __forceinline__ static void compact_tile_q(int q, R (&v)[E], const Cols& c, int s, int b,
-                                                          uint32_t p_tile, const uint32_t* pre)
-    {
-        switch (q) {
-        case 0:
-            compact_level_tile<0>(v, c, s, b, p_tile, pre);
-            break;
-        case 1:
-            if constexpr (LOG_E > 1)
-                compact_level_tile<1>(v, c, s, b, p_tile, pre);
-            break;
-        case 2:
-            if constexpr (LOG_E > 2)
-                compact_level_tile<2>(v, c, s, b, p_tile, pre);
-            break;
-        case 3:
-            if constexpr (LOG_E > 3)
-                compact_level_tile<3>(v, c, s, b, p_tile, pre);
-            break;
-        case 4:
-            if constexpr (LOG_E > 4)
-                compact_level_tile<4>(v, c, s, b, p_tile, pre);
-            break;
-        default:
-            break;
-        }
-    }
-
-    __device__ __forceinline__ static void compact_global_q(int q, R (&v)[E], const Cols& c, int s, int b,
-                                                            const uint32_t* tp, int C, int b_lo, size_t cta_bits)
-    {
-        switch (q) {
-        case 0:
-            compact_level_global<0>(v, c, s, b, tp, C, b_lo, cta_bits);
-            break;
-        case 1:
-            if constexpr (LOG_E > 1)
-                compact_level_global<1>(v, c, s, b, tp, C, b_lo, cta_bits);
-            break;
-        case 2:
-            if constexpr (LOG_E > 2)
-                compact_level_global<2>(v, c, s, b, tp, C, b_lo, cta_bits);
-            break;
-        case 3:
-            if constexpr (LOG_E > 3)
-                compact_level_global<3>(v, c, s, b, tp, C, b_lo, cta_bits);
-            break;
-        case 4:
-            if constexpr (LOG_E > 4)
-                compact_level_global<4>(v, c, s, b, tp, C, b_lo, cta_bits);
-            break;
-        default:
-            break;
-        }
-    }
-
     // ---- one pass over one tile (CTA `cta`) --------------------------------
+    // SORT = true compiles only the bitonic pass kinds, false only ORCompact.
+    template <bool SORT>
     __device__ static void run(const Cols& c, const NetGeom& g, const NetPass& p, const uint32_t* tile_prefix,
                                int cta, char* sm)
     {
@@ -301,57 +292,67 @@ struct Net {
         const int smin = is_global ? (C < S0 ? C : S0) : 0;
 
         R v[E];
-        int s = is_global && p.kind == P_COMPACT_GLOBAL ? smin : S0;
+        int s = (p.kind == P_COMPACT_GLOBAL) ? smin : S0;
         const bool first = (p.kind == P_SORT_TILE) || (p.kind == P_COMPACT_TILE);
+        {
+            auto ld = [&](auto sc) {
+                constexpr int S = decltype(sc)::value;
+                const int tp = tidpart<S>();
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            const size_t gi = gidx(TL::local(s, e, tid));
-            if (first)
-                v[e] = (gi < g.n) ? R::load(c, gi) : R::pad(c);
-            else
-                v[e] = R::load(c, gi);
+                for (int e = 0; e < E; e++) {
+                    const size_t gi = gidx(tp | (e << S));
+                    if (first)
+                        v[e] = (gi < g.n) ? R::load(c, gi) : R::pad(c);
+                    else
+                        v[e] = R::load(c, gi);
+                }
+            };
+            static_switch<0, NS>(s, ld);
         }
 
+        if constexpr (SORT) {
         if (p.kind == P_SORT_TILE) {
             for (int K = 1; K <= p.K; K++) {
                 const bool dconst = K >= LT;
                 const bool asc_c = ((cta_bits >> K) & 1) == 0;
                 for (int b = K - 1; b >= 0; b--) {
-                    const int ns = window_down(b, LOG_E, LT);
-                    if (ns != s) {
-                        TL::transpose(v, s, ns, sm);
+                    if (b < s || b >= s + LOG_E) {
+                        const int ns = window_down(b, LOG_E, LT);
+                        transpose(v, s, ns, sm);
                         s = ns;
                     }
-                    bitonic_q(b - s, v, c, s, K, dconst, asc_c);
+                    bitonic(s, b - s, v, c, K, dconst, asc_c);
                 }
             }
         } else if (p.kind == P_SORT_MERGE) {
             const bool asc_c = ((cta_bits >> p.K) & 1) == 0;
             for (int b = LT - 1; b >= 0; b--) {
-                const int ns = window_down(b, LOG_E, LT);
-                if (ns != s) {
-                    TL::transpose(v, s, ns, sm);
+                if (b < s || b >= s + LOG_E) {
+                    const int ns = window_down(b, LOG_E, LT);
+                    transpose(v, s, ns, sm);
                     s = ns;
                 }
-                bitonic_q(b - s, v, c, s, p.K, true, asc_c);
+                bitonic(s, b - s, v, c, p.K, true, asc_c);
             }
         } else if (p.kind == P_SORT_GLOBAL) {
             const bool asc_c = ((gidx(0) >> p.K) & 1) == 0;
             for (int b = p.b_hi; b >= b_lo; b--) {
                 const int lp = C + (b - b_lo);
-                int ns = window_down(lp, LOG_E, LT);
-                ns = ns < smin ? smin : ns;
-                if (ns != s) {
-                    TL::transpose(v, s, ns, sm);
+                if (lp < s || lp >= s + LOG_E) {
+                    int ns = window_down(lp, LOG_E, LT);
+                    ns = ns < smin ? smin : ns;
+                    transpose(v, s, ns, sm);
                     s = ns;
                 }
-                bitonic_q(lp - s, v, c, s, p.K, true, asc_c);
+                bitonic(s, lp - s, v, c, p.K, true, asc_c);
             }
-        } else if (p.kind == P_COMPACT_TILE) {
+        }
+        } else {
+        if (p.kind == P_COMPACT_TILE) {
             // prefix of the original marks over the tile, in local-index order
             uint32_t* pre = reinterpret_cast<uint32_t*>(sm + smem_rows());
             uint32_t* tmp = pre + T;
-            TL::transpose(v, s, 0, sm);
+            transpose(v, s, 0, sm);
             s = 0;
             uint32_t cnt = 0, m[E];
 #pragma unroll
@@ -361,41 +362,62 @@ struct Net {
             }
             uint32_t total;
             const uint32_t base = block_exclusive_scan(cnt, tmp, &total);
+            const int tp0 = tidpart<0>();
 #pragma unroll
             for (int e = 0; e < E; e++)
-                pre[TL::local(0, e, tid)] = base + m[e];
+                pre[tp0 | e] = base + m[e];
             __syncthreads();
             const uint32_t p_tile = tile_prefix[cta];
             for (int b = 0; b < p.K; b++) {
-                const int ns = window_up(b, LOG_E, LT);
-                if (ns != s) {
-                    TL::transpose(v, s, ns, sm);
+                if (b < s || b >= s + LOG_E) {
+                    const int ns = window_up(b, LOG_E, LT);
+                    transpose(v, s, ns, sm);
                     s = ns;
                 }
-                compact_tile_q(b - s, v, c, s, b, p_tile, pre);
+                auto fs = [&](auto sc) {
+                    constexpr int S = decltype(sc)::value;
+                    auto fq = [&](auto qc) { compact_level_tile<S, decltype(qc)::value>(v, c, b, p_tile, pre); };
+                    static_switch<0, LOG_E>(b - S, fq);
+                };
+                static_switch<0, NS>(s, fs);
             }
         } else { // P_COMPACT_GLOBAL
             for (int b = b_lo; b <= p.b_hi; b++) {
                 const int lp = C + (b - b_lo);
-                int ns = window_up(lp, LOG_E, LT);
-                ns = ns < smin ? smin : ns;
-                if (ns != s) {
-                    TL::transpose(v, s, ns, sm);
+                if (lp < s || lp >= s + LOG_E) {
+                    int ns = window_up(lp, LOG_E, LT);
+                    ns = ns < smin ? smin : ns;
+                    transpose(v, s, ns, sm);
                     s = ns;
                 }
-                compact_global_q(lp - s, v, c, s, b, tile_prefix, C, b_lo, cta_bits);
+                auto fs = [&](auto sc) {
+                    constexpr int S = decltype(sc)::value;
+                    auto fq = [&](auto qc) {
+                        compact_level_global<S, decltype(qc)::value>(v, c, b, tile_prefix, C, b_lo, cta_bits);
+                    };
+                    static_switch<0, LOG_E>(lp - S, fq);
+                };
+                static_switch<0, NS>(s, fs);
             }
+        }
         }
 
         if (s < 5) {
-            TL::transpose(v, s, S0, sm);
+            transpose(v, s, S0, sm);
             s = S0;
         }
+        {
+            auto stf = [&](auto sc) {
+                constexpr int S = decltype(sc)::value;
+                const int tp = tidpart<S>();
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            const size_t gi = gidx(TL::local(s, e, tid));
-            if (gi < Np)
-                R::store(c, gi, v[e]);
+                for (int e = 0; e < E; e++) {
+                    const size_t gi = gidx(tp | (e << S));
+                    if (gi < Np)
+                        R::store(c, gi, v[e]);
+                }
+            };
+            static_switch<0, NS>(s, stf);
         }
     }
 };

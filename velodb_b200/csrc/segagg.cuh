@@ -1,0 +1,536 @@
+// Oblivious segmented aggregation over key-sorted records with a small public
+// output bound G (group-by tail of the filter + group-by pipeline).
+//
+// The algorithm is the segmented-sum group-by of the reference's oblivious
+// aggregation (obliviator/operator_2/enclave/scalable_oblivious_join.c:221-262:
+// forward segmented sum, group boundaries, compaction of one row per group),
+// organised for the GPU in three passes over tiles of TS sorted rows:
+//   A  per tile: first/last key, sum of the trailing key run, number of
+//      complete groups ending inside the tile
+//   B  one CTA: carries between tiles (segmented scan over tiles) and the
+//      exclusive group-count prefix
+//   C  per tile: in-tile segmented scan + carry; the last row of each valid
+//      group carries the group total; the group with rank r (its position in
+//      key order) is accumulated into output slot r by masked sums over all
+//      G slots -- every row touches every slot, so addresses never depend on
+//      the data
+//   D  one CTA: slot-wise sum of the per-tile slot vectors.
+// Rows whose "valid" flag is clear form their own key runs (the flag is part
+// of the key) and never produce output.
+#pragma once
+
+#include <cstdint>
+
+namespace velo {
+
+constexpr int SEG_TS = 2048;     // rows per tile
+constexpr int SEG_THREADS = 256; // 8 contiguous rows per thread
+constexpr int SEG_RPT = SEG_TS / SEG_THREADS;
+constexpr int SEG_MAX_G = 16;
+
+struct SegTileAgg {
+    uint64_t head_key;
+    uint64_t tail_key;
+    uint32_t uniform;    // whole tile is one key run
+    uint32_t tails;      // valid groups ending inside the tile (excluding its last row)
+    uint32_t tail_valid; // the tile's last row is valid
+    uint32_t pad_;
+};
+
+// Block-wide inclusive segmented scan (flag = "a new run starts at this
+// thread's first row"; the operator resets at flags).  V int64 values.
+template <int V>
+__device__ __forceinline__ void block_seg_scan(bool& flag, int64_t (&x)[V], int64_t* sm_vals, uint32_t* sm_flags)
+{
+    const int t = threadIdx.x;
+    for (int off = 1; off < SEG_THREADS; off <<= 1) {
+        __syncthreads();
+        sm_flags[t] = flag ? 1u : 0u;
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            sm_vals[i * SEG_THREADS + t] = x[i];
+        __syncthreads();
+        if (t >= off) {
+            const bool pf = sm_flags[t - off] != 0;
+            if (!flag) {
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    x[i] += sm_vals[i * SEG_THREADS + t - off];
+            }
+            flag = flag | pf;
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t block_sum_u32(uint32_t x, uint32_t* tmp)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+        tmp[threadIdx.x >> 5] = x;
+    __syncthreads();
+    uint32_t s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+        s += tmp[w];
+    return s;
+}
+
+__device__ __forceinline__ int64_t warp_sum_i64(int64_t x)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// Agg: static constexpr int W (record words), V (values);
+//      static uint64_t key(const uint64_t* w)      -- run key (includes validity)
+//      static bool valid(const uint64_t* w)
+//      static void values(const uint64_t* w, int64_t (&v)[V])  -- zero when invalid
+//      static int64_t out_key(const uint64_t* w)
+template <class Agg>
+struct SegAgg {
+    static constexpr int W = Agg::W;
+    static constexpr int V = Agg::V;
+    // the tile area holds the W input words, later the 1+V output words
+    static constexpr int TW = W > 1 + V ? W : 1 + V;
+    static constexpr size_t SMEM = (size_t)SEG_TS * TW * 8 + (size_t)V * SEG_THREADS * 8 + SEG_THREADS * 4 + 64;
+
+    // stage the tile's records in smem (coalesced), then thread t owns rows
+    // [t*RPT, t*RPT + RPT)
+    __device__ static void load_tile(uint64_t* const* words, size_t base, uint64_t* sw)
+    {
+        for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
+#pragma unroll
+            for (int x = 0; x < W; x++)
+                sw[x * SEG_TS + i] = words[x][base + i];
+        }
+        __syncthreads();
+    }
+
+    __device__ static void row(const uint64_t* sw, int i, uint64_t (&w)[W])
+    {
+#pragma unroll
+        for (int x = 0; x < W; x++)
+            w[x] = sw[x * SEG_TS + i];
+    }
+
+    // pass A
+    __device__ static void tile_summary(uint64_t* const* words, int tile, SegTileAgg* aggs, int64_t* tail_runs,
+                                        char* smem)
+    {
+        uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
+        uint32_t* tmp = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS * TW * 8);
+        int64_t* red = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS * TW * 8 + 256);
+        const size_t base = (size_t)tile * SEG_TS;
+        load_tile(words, base, sw);
+        uint64_t wl[W];
+        row(sw, SEG_TS - 1, wl);
+        const uint64_t tail_key = Agg::key(wl);
+        int64_t run[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            run[i] = 0;
+        uint32_t tails = 0;
+        const int r0 = threadIdx.x * SEG_RPT;
+#pragma unroll
+        for (int r = 0; r < SEG_RPT; r++) {
+            uint64_t w[W], wn[W];
+            row(sw, r0 + r, w);
+            const int nxt = r0 + r + 1 < SEG_TS ? r0 + r + 1 : SEG_TS - 1;
+            row(sw, nxt, wn);
+            const uint64_t k = Agg::key(w);
+            int64_t v[V];
+            Agg::values(w, v);
+            const bool in_run = (k == tail_key);
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                run[i] += in_run ? v[i] : 0;
+            const bool internal = (r0 + r + 1 < SEG_TS);
+            tails += (internal & (k != Agg::key(wn)) & Agg::valid(w)) ? 1u : 0u;
+        }
+        const uint32_t t_all = block_sum_u32(tails, tmp);
+        // reduce the run sums: warp shuffles, then one value per warp
+#pragma unroll
+        for (int i = 0; i < V; i++) {
+            const int64_t s = warp_sum_i64(run[i]);
+            if ((threadIdx.x & 31) == 0)
+                red[i * 8 + (threadIdx.x >> 5)] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint64_t w0[W];
+            row(sw, 0, w0);
+            SegTileAgg a;
+            a.head_key = Agg::key(w0);
+            a.tail_key = tail_key;
+            a.uniform = (a.head_key == tail_key) ? 1u : 0u;
+            a.tails = t_all;
+            a.tail_valid = Agg::valid(wl) ? 1u : 0u;
+            a.pad_ = 0;
+            aggs[tile] = a;
+#pragma unroll
+            for (int i = 0; i < V; i++) {
+                int64_t s = 0;
+                for (int w = 0; w < SEG_THREADS / 32; w++)
+                    s += red[i * 8 + w];
+                tail_runs[(size_t)tile * V + i] = s;
+            }
+        }
+    }
+
+    // pass B: one CTA of 1024 threads
+    __device__ static void carries(const SegTileAgg* aggs, const int64_t* tail_runs, int ntiles, int64_t* carry_in,
+                                   uint32_t* tail_prefix, uint64_t* n_groups, char* smem)
+    {
+        // thread-sequential over a contiguous chunk, then a block scan of the
+        // chunk aggregates (chunks are at most ntiles/1024 tiles)
+        const int nt = blockDim.x;
+        const int per = (ntiles + nt - 1) / nt;
+        const int t0 = threadIdx.x * per;
+        const int t1 = min(ntiles, t0 + per);
+        // segmented scan state for carry_out over my chunk
+        bool f = false; // a run boundary occurred in my chunk (reset)
+        int64_t acc[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            acc[i] = 0;
+        uint32_t tcount = 0;
+        for (int t = t0; t < t1; t++) {
+            const SegTileAgg a = aggs[t];
+            const bool cont = (t > 0) && (aggs[t - 1].tail_key == a.head_key) && a.uniform;
+            if (!cont) {
+                f = true;
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    acc[i] = 0;
+            }
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                acc[i] += tail_runs[(size_t)t * V + i];
+            const bool last_tail = (t + 1 < ntiles) ? (a.tail_key != aggs[t + 1].head_key) : true;
+            tcount += a.tails + ((last_tail & (a.tail_valid != 0)) ? 1u : 0u);
+        }
+        // block-level exclusive segmented scan of (f, acc) and of tcount
+        int64_t* sv = reinterpret_cast<int64_t*>(smem);
+        uint32_t* sf = reinterpret_cast<uint32_t*>(smem + (size_t)V * 1024 * 8);
+        uint32_t* sc = sf + 1024;
+        int64_t inc[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            inc[i] = acc[i];
+        bool fl = f;
+        uint32_t cinc = tcount;
+        for (int off = 1; off < nt; off <<= 1) {
+            __syncthreads();
+            sf[threadIdx.x] = fl ? 1u : 0u;
+            sc[threadIdx.x] = cinc;
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                sv[i * 1024 + threadIdx.x] = inc[i];
+            __syncthreads();
+            if ((int)threadIdx.x >= off) {
+                const bool pf = sf[threadIdx.x - off] != 0;
+                if (!fl) {
+#pragma unroll
+                    for (int i = 0; i < V; i++)
+                        inc[i] += sv[i * 1024 + threadIdx.x - off];
+                }
+                fl = fl | pf;
+                cinc += sc[threadIdx.x - off];
+            }
+        }
+        __syncthreads();
+        // exclusive values for my chunk = inclusive of thread - 1
+        sf[threadIdx.x] = fl ? 1u : 0u;
+        sc[threadIdx.x] = cinc;
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            sv[i * 1024 + threadIdx.x] = inc[i];
+        __syncthreads();
+        int64_t run_out[V]; // carry_out of the tile before my chunk
+        uint32_t cpre = 0;
+        if (threadIdx.x > 0) {
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                run_out[i] = sv[i * 1024 + threadIdx.x - 1];
+            cpre = sc[threadIdx.x - 1];
+        } else {
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                run_out[i] = 0;
+        }
+        // replay my chunk producing carry_in and tail_prefix per tile
+        for (int t = t0; t < t1; t++) {
+            const SegTileAgg a = aggs[t];
+            const bool joins = (t > 0) && (aggs[t - 1].tail_key == a.head_key);
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                carry_in[(size_t)t * V + i] = joins ? run_out[i] : 0;
+            tail_prefix[t] = cpre;
+            const bool cont = joins && a.uniform;
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                run_out[i] = (cont ? run_out[i] : 0) + tail_runs[(size_t)t * V + i];
+            const bool last_tail = (t + 1 < ntiles) ? (a.tail_key != aggs[t + 1].head_key) : true;
+            cpre += a.tails + ((last_tail & (a.tail_valid != 0)) ? 1u : 0u);
+        }
+        if (threadIdx.x == nt - 1)
+            *n_groups = cinc;
+    }
+
+    // pass C
+    __device__ static void emit(uint64_t* const* words, int tile, int ntiles, const SegTileAgg* aggs,
+                                const int64_t* carry_in, const uint32_t* tail_prefix, int G, int64_t* tile_out,
+                                char* smem)
+    {
+        uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
+        int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS * TW * 8);
+        uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS * TW * 8 + (size_t)V * SEG_THREADS * 8);
+        const size_t base = (size_t)tile * SEG_TS;
+        load_tile(words, base, sw);
+        const uint64_t next_head = (tile + 1 < ntiles) ? aggs[tile + 1].head_key : ~0ull;
+        const bool last_tile = (tile + 1 >= ntiles);
+        const uint64_t head_key = aggs[tile].head_key;
+        const int r0 = threadIdx.x * SEG_RPT;
+
+        // thread-local inclusive segmented scan of my rows
+        int64_t pref[SEG_RPT][V];
+        uint64_t keys[SEG_RPT];
+        bool tail[SEG_RPT];
+        bool start_flag = false; // a run starts inside my rows (at row r0 or later)
+        {
+            uint64_t wprev[W];
+            row(sw, r0 > 0 ? r0 - 1 : 0, wprev);
+            uint64_t prev_key = Agg::key(wprev);
+            int64_t run[V];
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                run[i] = 0;
+#pragma unroll
+            for (int r = 0; r < SEG_RPT; r++) {
+                uint64_t w[W];
+                row(sw, r0 + r, w);
+                const uint64_t k = Agg::key(w);
+                int64_t v[V];
+                Agg::values(w, v);
+                const bool starts = (r0 + r == 0) ? true : (k != prev_key);
+                start_flag = start_flag | starts;
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    run[i] = (starts ? 0 : run[i]) + v[i];
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    pref[r][i] = run[i];
+                keys[r] = k;
+                prev_key = k;
+                uint64_t wn[W];
+                const int nxt = r0 + r + 1 < SEG_TS ? r0 + r + 1 : SEG_TS - 1;
+                row(sw, nxt, wn);
+                const uint64_t kn = (r0 + r + 1 < SEG_TS) ? Agg::key(wn) : next_head;
+                const bool ends = (r0 + r + 1 < SEG_TS || !last_tile) ? (k != kn) : true;
+                tail[r] = ends & Agg::valid(w);
+            }
+        }
+        // exclusive block segmented scan of thread aggregates: my carry-in is
+        // the inclusive result of thread-1 unless a run starts at my row r0
+        int64_t agg[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            agg[i] = pref[SEG_RPT - 1][i];
+        bool fl = start_flag;
+        block_seg_scan<V>(fl, agg, svals, sflags);
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            svals[i * SEG_THREADS + threadIdx.x] = agg[i];
+        __syncthreads();
+        int64_t cin[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            cin[i] = (threadIdx.x > 0) ? svals[i * SEG_THREADS + threadIdx.x - 1] : 0;
+        // the tile-level carry applies to rows of the tile's first run
+        int64_t tc[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            tc[i] = carry_in[(size_t)tile * V + i];
+        // rank of my first tail: tail prefix of the tile + tails of threads before me
+        uint32_t my_tails = 0;
+#pragma unroll
+        for (int r = 0; r < SEG_RPT; r++)
+            my_tails += tail[r] ? 1u : 0u;
+        __syncthreads();
+        uint32_t* cnt = reinterpret_cast<uint32_t*>(svals);
+        cnt[threadIdx.x] = my_tails;
+        __syncthreads();
+        uint32_t before = 0;
+        for (int t = 0; t < (int)threadIdx.x; t++)
+            before += cnt[t];
+        const uint32_t rank0 = tail_prefix[tile] + before;
+
+        // my leading rows continue the run open at the end of thread t-1
+        // unless a new run starts exactly at my first row
+        bool lead = (r0 > 0);
+        if (r0 > 0) {
+            uint64_t wp[W];
+            row(sw, r0 - 1, wp);
+            lead = (Agg::key(wp) == keys[0]);
+        }
+        // segment totals up to each row: my prefix, the in-tile carry of the
+        // preceding threads, and the cross-tile carry of the tile's first run
+#pragma unroll
+        for (int r = 0; r < SEG_RPT; r++) {
+            if (r > 0)
+                lead = lead & (keys[r] == keys[r - 1]);
+            const bool first_run_of_tile = (keys[r] == head_key);
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                pref[r][i] += (lead ? cin[i] : 0) + (first_run_of_tile ? tc[i] : 0);
+        }
+        // output slot j receives (key, totals) of the tail whose rank is j;
+        // every row is folded into every slot with a mask
+        __syncthreads();
+        int64_t* red = reinterpret_cast<int64_t*>(smem); // reuse the tile area
+        for (int j = 0; j < G; j++) {
+            int64_t acc[1 + V];
+#pragma unroll
+            for (int i = 0; i <= V; i++)
+                acc[i] = 0;
+            uint32_t rank = rank0;
+#pragma unroll
+            for (int r = 0; r < SEG_RPT; r++) {
+                const bool hit = tail[r] & (rank == (uint32_t)j);
+                acc[0] += hit ? Agg::out_key_from(keys[r]) : 0;
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    acc[1 + i] += hit ? pref[r][i] : 0;
+                rank += tail[r] ? 1u : 0u;
+            }
+#pragma unroll
+            for (int i = 0; i <= V; i++) {
+                const int64_t sum = warp_sum_i64(acc[i]);
+                if ((threadIdx.x & 31) == 0)
+                    red[(j * (1 + V) + i) * 8 + (threadIdx.x >> 5)] = sum;
+            }
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < G * (1 + V); q += SEG_THREADS) {
+            int64_t sum = 0;
+            for (int w = 0; w < SEG_THREADS / 32; w++)
+                sum += red[q * 8 + w];
+            tile_out[(size_t)tile * G * (1 + V) + q] = sum;
+        }
+    }
+
+    // pass C for a large output bound: every row writes a group record
+    // (o0 = [63] not the last row of a valid group | [31:0] Agg::out_bits,
+    // o1.. = the group's sums, valid only on the group's last row); an
+    // ORCompact of the records then yields the groups in key order.
+    __device__ static void emit_rows(uint64_t* const* words, int tile, int ntiles, const SegTileAgg* aggs,
+                                     const int64_t* carry_in, uint64_t* const* out, char* smem)
+    {
+        uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
+        int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS * TW * 8);
+        uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS * TW * 8 + (size_t)V * SEG_THREADS * 8);
+        const size_t base = (size_t)tile * SEG_TS;
+        load_tile(words, base, sw);
+        const uint64_t next_head = (tile + 1 < ntiles) ? aggs[tile + 1].head_key : ~0ull;
+        const bool last_tile = (tile + 1 >= ntiles);
+        const uint64_t head_key = aggs[tile].head_key;
+        const int r0 = threadIdx.x * SEG_RPT;
+        int64_t pref[SEG_RPT][V];
+        uint64_t keys[SEG_RPT];
+        bool tail[SEG_RPT];
+        bool start_flag = false;
+        {
+            uint64_t wprev[W];
+            row(sw, r0 > 0 ? r0 - 1 : 0, wprev);
+            uint64_t prev_key = Agg::key(wprev);
+            int64_t run[V];
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                run[i] = 0;
+#pragma unroll
+            for (int r = 0; r < SEG_RPT; r++) {
+                uint64_t w[W];
+                row(sw, r0 + r, w);
+                const uint64_t k = Agg::key(w);
+                int64_t v[V];
+                Agg::values(w, v);
+                const bool starts = (r0 + r == 0) ? true : (k != prev_key);
+                start_flag = start_flag | starts;
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    run[i] = (starts ? 0 : run[i]) + v[i];
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    pref[r][i] = run[i];
+                keys[r] = k;
+                prev_key = k;
+                uint64_t wn[W];
+                const int nxt = r0 + r + 1 < SEG_TS ? r0 + r + 1 : SEG_TS - 1;
+                row(sw, nxt, wn);
+                const uint64_t kn = (r0 + r + 1 < SEG_TS) ? Agg::key(wn) : next_head;
+                const bool ends = (r0 + r + 1 < SEG_TS || !last_tile) ? (k != kn) : true;
+                tail[r] = ends & Agg::valid(w);
+            }
+        }
+        int64_t agg[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            agg[i] = pref[SEG_RPT - 1][i];
+        bool fl = start_flag;
+        block_seg_scan<V>(fl, agg, svals, sflags);
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            svals[i * SEG_THREADS + threadIdx.x] = agg[i];
+        __syncthreads();
+        int64_t cin[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            cin[i] = (threadIdx.x > 0) ? svals[i * SEG_THREADS + threadIdx.x - 1] : 0;
+        int64_t tc[V];
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            tc[i] = carry_in[(size_t)tile * V + i];
+        bool lead = (r0 > 0);
+        if (r0 > 0) {
+            uint64_t wp[W];
+            row(sw, r0 - 1, wp);
+            lead = (Agg::key(wp) == keys[0]);
+        }
+        __syncthreads();
+        // stage the output records in smem so the global stores stay coalesced
+        uint64_t* so = sw;
+#pragma unroll
+        for (int r = 0; r < SEG_RPT; r++) {
+            if (r > 0)
+                lead = lead & (keys[r] == keys[r - 1]);
+            const bool first_run_of_tile = (keys[r] == head_key);
+            so[r0 + r] = ((uint64_t)(!tail[r]) << 63) | Agg::out_bits(keys[r]);
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                so[(size_t)(1 + i) * SEG_TS + r0 + r] =
+                    (uint64_t)(pref[r][i] + (lead ? cin[i] : 0) + (first_run_of_tile ? tc[i] : 0));
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
+#pragma unroll
+            for (int x = 0; x <= V; x++)
+                out[x][base + i] = so[(size_t)x * SEG_TS + i];
+        }
+    }
+
+    // pass D: out[j] = sum over tiles of tile_out[tile][j] (one CTA)
+    __device__ static void finish(const int64_t* tile_out, int ntiles, int G, int64_t* out)
+    {
+        for (int q = threadIdx.x; q < G * (1 + V); q += blockDim.x) {
+            int64_t sum = 0;
+            for (int t = 0; t < ntiles; t++)
+                sum += tile_out[(size_t)t * G * (1 + V) + q];
+            out[q] = sum;
+        }
+    }
+};
+
+} // namespace velo

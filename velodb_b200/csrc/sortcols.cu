@@ -10,7 +10,7 @@
 // reference (so equal keys keep the reference's arrangement), and the columns
 // are decoded back in place.  All three steps are streaming or network passes
 // with data-independent addresses.
-#include "net_host.cuh"
+#include "net_impl.cuh"
 
 namespace velo {
 
