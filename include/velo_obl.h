@@ -116,6 +116,22 @@ velo_status velo_ocompact_kpm(uint64_t* d_keys, uint32_t* d_payload, uint8_t* d_
                               void* stream);
 size_t velo_compact_scratch_bytes(size_t capacity, const velo_tune* tune);
 
+/* Same compaction as velo_ocompact_kpm with the default tile configuration,
+ * for callers that cannot allocate device memory -- an engine whose HBM is
+ * owned by its own pool allocator, a latency-critical path that cannot take
+ * cudaMalloc's implicit device synchronisation, a plugin host without an
+ * allocation hook.  It takes no scratch argument and allocates nothing: its
+ * scratch is a fixed 256.5 KiB array in the library's device memory, held on
+ * every GPU that loads the library until the process exits.  Limit: n up to
+ * 2^28 rows (larger n returns VELO_EINVAL).  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller.  Every call rewrites
+ * the array before reading it, so results never depend on earlier calls.
+ * This entry point has no counterpart in the reference. */
+velo_status velo_ocompact_kpm_noalloc(uint64_t* d_keys, uint32_t* d_payload, uint8_t* d_marks, size_t n,
+                                      size_t capacity, uint64_t* d_count, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Filter + group-by (oblivious)                                            */
 /* ------------------------------------------------------------------------ */

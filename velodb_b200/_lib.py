@@ -22,6 +22,7 @@ PROTOS = {
     "velo_sort_scratch_bytes": (sz, [vp, u32, sz]),
     "velo_ocompact_kpm": (i32, [vp, vp, vp, sz, sz, vp, vp, sz, vp, vp]),
     "velo_compact_scratch_bytes": (sz, [sz, vp]),
+    "velo_ocompact_kpm_noalloc": (i32, [vp, vp, vp, sz, sz, vp, vp]),
     "velo_filter_groupby_scratch_bytes": (sz, [sz, u32]),
     "velo_filter_groupby": (i32, [vp, sz, vp, u32, u32, vp, vp, vp, sz, vp]),
     "velo_join_groupby_topk_scratch_bytes": (sz, [sz, sz]),
