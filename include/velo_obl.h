@@ -98,6 +98,20 @@ velo_status velo_sort_columns(void* const* d_cols, const uint32_t* types, const 
                               void* stream);
 size_t velo_sort_scratch_bytes(const uint32_t* types, uint32_t n_cols, size_t n);
 
+/* Oblivious bitonic sort of records of n_words u64 words (SoA: d_words[w]
+ * points at word w of every row; 1..3 words), ordered on word 0 AND-ed with
+ * key_mask; the other words ride along.  Rows [n, next_pow2(n)) are filled
+ * with all-ones words (they sort last).  flags: VELO_SORT_STRICT keeps the
+ * reference's tie rule (include/cuda/sort.cuh:31-40: equal keys are never
+ * exchanged), so the arrangement of equal keys is exactly the reference
+ * network's; without it equal keys may be exchanged in descending merges
+ * (one comparison per exchange), for consumers that aggregate over ties.
+ * This is the row-record form the operators use for ORDER BY and group-by
+ * inputs whose payload is packed next to the key. */
+#define VELO_SORT_STRICT 1u
+velo_status velo_osort_records(uint64_t* const* d_words, uint32_t n_words, uint64_t key_mask, size_t n,
+                               size_t capacity, uint32_t flags, const velo_tune* tune, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* ORCompact (order-preserving oblivious compaction)                        */
 /* ------------------------------------------------------------------------ */

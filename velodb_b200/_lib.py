@@ -20,6 +20,7 @@ PROTOS = {
     "velo_osort_kp": (i32, [vp, vp, sz, sz, vp, vp]),
     "velo_sort_columns": (i32, [vp, vp, vp, u32, sz, sz, vp, vp, sz, vp]),
     "velo_sort_scratch_bytes": (sz, [vp, u32, sz]),
+    "velo_osort_records": (i32, [vp, u32, u64, sz, sz, u32, vp, vp]),
     "velo_ocompact_kpm": (i32, [vp, vp, vp, sz, sz, vp, vp, sz, vp, vp]),
     "velo_compact_scratch_bytes": (sz, [sz, vp]),
     "velo_ocompact_kpm_noalloc": (i32, [vp, vp, vp, sz, sz, vp, vp]),

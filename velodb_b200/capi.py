@@ -177,3 +177,16 @@ def join_groupby_topk(dt: dict, pred: dict, k: int = 10, scratch=None, out=None,
                                        scratch.data_ptr(), scratch.numel(), _stream(stream)),
           "velo_join_groupby_topk")
     return out, counts
+
+
+SORT_STRICT = 1
+
+
+def osort_records(words, n: int, key_mask: int, strict: bool = False, tune=None, stream=None) -> None:
+    """In-place oblivious sort of 1..3-word records (velo_osort_records);
+    `words` are int64 device tensors of equal capacity (SoA)."""
+    ptrs = np.asarray([w.data_ptr() for w in words], dtype=np.uint64)
+    cap = min(w.numel() for w in words)
+    check(lib().velo_osort_records(ptrs.ctypes.data, len(words), key_mask & 0xFFFFFFFFFFFFFFFF, n, cap,
+                                   SORT_STRICT if strict else 0, tune_ref(tune), _stream(stream)),
+          "velo_osort_records")

@@ -26,7 +26,85 @@
 namespace velo {
 
 // ---------------------------------------------------------------------------
-// row types: SoA columns in global memory, SoA arrays in shared memory
+// multi-limb unsigned comparison: 0xFFFFFFFF if x > y else 0, from the borrow
+// of y - x (limb 0 least significant); one carry chain, no branches
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t gt_mask2(uint32_t x0, uint32_t x1, uint32_t y0, uint32_t y1)
+{
+    uint32_t r;
+    asm("{\n\t.reg .u32 t;\n\t"
+        "sub.cc.u32 t, %1, %3;\n\t"
+        "subc.cc.u32 t, %2, %4;\n\t"
+        "subc.u32 %0, 0, 0;\n\t}"
+        : "=r"(r)
+        : "r"(y0), "r"(y1), "r"(x0), "r"(x1));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t gt_mask3(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t y0, uint32_t y1,
+                                             uint32_t y2)
+{
+    uint32_t r;
+    asm("{\n\t.reg .u32 t;\n\t"
+        "sub.cc.u32 t, %1, %4;\n\t"
+        "subc.cc.u32 t, %2, %5;\n\t"
+        "subc.cc.u32 t, %3, %6;\n\t"
+        "subc.u32 %0, 0, 0;\n\t}"
+        : "=r"(r)
+        : "r"(y0), "r"(y1), "r"(y2), "r"(x0), "r"(x1), "r"(x2));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t gt_mask4(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3, uint32_t y0,
+                                             uint32_t y1, uint32_t y2, uint32_t y3)
+{
+    uint32_t r;
+    asm("{\n\t.reg .u32 t;\n\t"
+        "sub.cc.u32 t, %1, %5;\n\t"
+        "subc.cc.u32 t, %2, %6;\n\t"
+        "subc.cc.u32 t, %3, %7;\n\t"
+        "subc.cc.u32 t, %4, %8;\n\t"
+        "subc.u32 %0, 0, 0;\n\t}"
+        : "=r"(r)
+        : "r"(y0), "r"(y1), "r"(y2), "r"(y3), "r"(x0), "r"(x1), "r"(x2), "r"(x3));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t lo32(uint64_t x) { return (uint32_t)x; }
+__device__ __forceinline__ uint32_t hi32(uint64_t x) { return (uint32_t)(x >> 32); }
+
+// 0xFFFFFFFF if the KW-word key x (word 0 most significant) exceeds y
+template <int KW>
+__device__ __forceinline__ uint32_t key_gt_mask(const uint64_t* x, const uint64_t* y)
+{
+    if constexpr (KW == 1) {
+        return gt_mask2(lo32(x[0]), hi32(x[0]), lo32(y[0]), hi32(y[0]));
+    } else if constexpr (KW == 2) {
+        return gt_mask4(lo32(x[1]), hi32(x[1]), lo32(x[0]), hi32(x[0]), lo32(y[1]), hi32(y[1]), lo32(y[0]), hi32(y[0]));
+    } else {
+        // lexicographic from the most significant word
+        bool res = false, eq = true;
+#pragma unroll
+        for (int i = 0; i < KW; i++) {
+            res = res | (eq & (x[i] > y[i]));
+            eq = eq & (x[i] == y[i]);
+        }
+        return res ? 0xFFFFFFFFu : 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// row types: SoA columns in global memory, SoA arrays in shared memory.
+//
+// swap_mask(a, b, desc) is the compare-exchange decision for the pair
+// (a at the lower index, b): ascending swaps iff a > b, descending iff a < b.
+// STRICT types follow the reference exactly on ties (include/cuda/sort.cuh:
+// 31-40: no swap when equal).  Non-strict types are used where the
+// arrangement of equal keys is invisible to the consumer (every field is
+// compared, or the consumer aggregates over ties); they decide both
+// directions with one comparison, swapping equal keys when descending,
+// which still sorts.
 // ---------------------------------------------------------------------------
 
 template <class T>
@@ -36,6 +114,7 @@ __device__ __forceinline__ T sel(bool c, T a, T b)
 }
 
 // (u64 key, u32 payload), ordered lexicographically on both (plain sort rows).
+// Every field is compared, so the sorted output is unique.
 struct RowKP {
     uint64_t k;
     uint32_t p;
@@ -44,7 +123,6 @@ struct RowKP {
         uint32_t* p;
     };
     static constexpr int SMEM_BYTES = 12;
-    static constexpr bool FULL_KEY = true;
     __device__ __forceinline__ static RowKP load(const Cols& c, size_t g) { return RowKP { c.k[g], c.p[g] }; }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowKP& r)
     {
@@ -61,10 +139,9 @@ struct RowKP {
     {
         return RowKP { reinterpret_cast<const uint64_t*>(sm)[i], reinterpret_cast<const uint32_t*>(sm + 8 * T)[i] };
     }
-    // a > b in the row order
-    __device__ __forceinline__ static bool gt(const RowKP& a, const RowKP& b, const Cols&)
+    __device__ __forceinline__ static uint32_t swap_mask(const RowKP& a, const RowKP& b, uint32_t desc, const Cols&)
     {
-        return (a.k > b.k) | ((a.k == b.k) & (a.p > b.p));
+        return gt_mask3(a.p, lo32(a.k), hi32(a.k), b.p, lo32(b.k), hi32(b.k)) ^ desc;
     }
     __device__ __forceinline__ static RowKP select(bool c, const RowKP& a, const RowKP& b)
     {
@@ -73,8 +150,8 @@ struct RowKP {
     __device__ __forceinline__ static bool marked(const RowKP&) { return false; }
 };
 
-// (u64 key, u32 payload, u8 mark): compaction rows; the order compares
-// (key, payload) so the same rows can also be sorted.
+// (u64 key, u32 payload, u8 mark): compaction rows; ordered on (key, payload)
+// with the mark carried, strictly.
 struct RowKPM {
     uint64_t k;
     uint32_t p;
@@ -85,7 +162,6 @@ struct RowKPM {
         uint8_t* m;
     };
     static constexpr int SMEM_BYTES = 13;
-    static constexpr bool FULL_KEY = false;
     __device__ __forceinline__ static RowKPM load(const Cols& c, size_t g)
     {
         return RowKPM { c.k[g], c.p[g], (uint32_t)c.m[g] };
@@ -108,9 +184,11 @@ struct RowKPM {
         return RowKPM { reinterpret_cast<const uint64_t*>(sm)[i], reinterpret_cast<const uint32_t*>(sm + 8 * T)[i],
                         (uint32_t) reinterpret_cast<const uint8_t*>(sm + 12 * T)[i] };
     }
-    __device__ __forceinline__ static bool gt(const RowKPM& a, const RowKPM& b, const Cols&)
+    __device__ __forceinline__ static uint32_t swap_mask(const RowKPM& a, const RowKPM& b, uint32_t desc, const Cols&)
     {
-        return (a.k > b.k) | ((a.k == b.k) & (a.p > b.p));
+        const uint32_t gt = gt_mask3(a.p, lo32(a.k), hi32(a.k), b.p, lo32(b.k), hi32(b.k));
+        const uint32_t lt = gt_mask3(b.p, lo32(b.k), hi32(b.k), a.p, lo32(a.k), hi32(a.k));
+        return desc ? lt : gt;
     }
     __device__ __forceinline__ static RowKPM select(bool c, const RowKPM& a, const RowKPM& b)
     {
@@ -122,7 +200,7 @@ struct RowKPM {
 // W u64 words per row (SoA).  Ordered lexicographically on the first KW words,
 // each AND-ed with a mask; the mark (for compaction) is bit `mark_bit` of word
 // 0, inverted when mark_inv is set (so an "invalid" flag can sort last).
-template <int W, int KW>
+template <int W, int KW, bool STRICT = true>
 struct RowRec {
     uint64_t w[W];
     struct Cols {
@@ -133,7 +211,6 @@ struct RowRec {
         int mark_inv;
     };
     static constexpr int SMEM_BYTES = 8 * W;
-    static constexpr bool FULL_KEY = false;
     __device__ __forceinline__ static RowRec load(const Cols& c, size_t g)
     {
         RowRec r;
@@ -170,16 +247,22 @@ struct RowRec {
             r.w[x] = reinterpret_cast<const uint64_t*>(sm + (size_t)8 * T * x)[i];
         return r;
     }
-    __device__ __forceinline__ static bool gt(const RowRec& a, const RowRec& b, const Cols& c)
+    __device__ __forceinline__ static uint32_t swap_mask(const RowRec& a, const RowRec& b, uint32_t desc,
+                                                         const Cols& c)
     {
-        bool res = false, eq = true;
+        uint64_t ka[KW], kb[KW];
 #pragma unroll
         for (int x = 0; x < KW; x++) {
-            uint64_t aa = a.w[x] & c.mask[x], bb = b.w[x] & c.mask[x];
-            res = res | (eq & (aa > bb));
-            eq = eq & (aa == bb);
+            ka[x] = a.w[x] & c.mask[x];
+            kb[x] = b.w[x] & c.mask[x];
         }
-        return res;
+        if constexpr (STRICT) {
+            const uint32_t gt = key_gt_mask<KW>(ka, kb);
+            const uint32_t lt = key_gt_mask<KW>(kb, ka);
+            return desc ? lt : gt;
+        } else {
+            return key_gt_mask<KW>(ka, kb) ^ desc;
+        }
     }
     __device__ __forceinline__ static RowRec select(bool cnd, const RowRec& a, const RowRec& b)
     {
@@ -199,11 +282,11 @@ template <class R>
 struct MarkOf {
     __device__ __forceinline__ static bool get(const R& r, const typename R::Cols&) { return R::marked(r); }
 };
-template <int W, int KW>
-struct MarkOf<RowRec<W, KW>> {
-    __device__ __forceinline__ static bool get(const RowRec<W, KW>& r, const typename RowRec<W, KW>::Cols& c)
+template <int W, int KW, bool S>
+struct MarkOf<RowRec<W, KW, S>> {
+    __device__ __forceinline__ static bool get(const RowRec<W, KW, S>& r, const typename RowRec<W, KW, S>::Cols& c)
     {
-        return RowRec<W, KW>::marked_c(r, c);
+        return RowRec<W, KW, S>::marked_c(r, c);
     }
 };
 
@@ -219,27 +302,10 @@ struct Tile {
     static constexpr int T = 1 << LOG_T;
     static_assert(LOG_NT >= 5, "at least one warp per CTA");
 
-    __device__ __forceinline__ static int local(int s, int e, int tid)
-    {
-        return (tid & ((1 << s) - 1)) | (e << s) | ((tid >> s) << (s + LOG_E));
-    }
     // bank-spreading swizzle: XOR bits 5..9 into bits 0..4 (a bijection on
-    // every aligned group of 1024 rows, so it stays inside the tile)
-    __device__ __forceinline__ static int swz(int l) { return l ^ ((l >> 5) & 31); }
-
-    template <class R>
-    __device__ __forceinline__ static void transpose(R (&v)[E], int s_from, int s_to, char* sm)
-    {
-        const int tid = threadIdx.x;
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < E; e++)
-            R::sstore(sm, T, swz(local(s_from, e, tid)), v[e]);
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < E; e++)
-            v[e] = R::sload(sm, T, swz(local(s_to, e, tid)));
-    }
+    // every aligned group of 1024 rows, so it stays inside the tile).  It is
+    // linear over XOR, so swz(a | b) = swz(a) ^ swz(b) for disjoint a, b.
+    __host__ __device__ __forceinline__ static constexpr int swz(int l) { return l ^ ((l >> 5) & 31); }
 };
 
 // window start that covers bit p, going down (bitonic) or up (ORCompact)

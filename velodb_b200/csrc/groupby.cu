@@ -22,7 +22,8 @@
 
 namespace velo {
 
-using LiRec = RowRec<3, 1>;
+// the group-by consumer sums over ties, so their arrangement is irrelevant
+using LiRec = RowRec<3, 1, false>;
 constexpr uint64_t LI_KEYMASK = 0xFFFF800000000000ull;
 constexpr int LI_LOG_NT = 8, LI_LOG_E = 4; // 4096-row tiles for sort and compaction
 constexpr int LI_LT = LI_LOG_NT + LI_LOG_E;
@@ -283,7 +284,7 @@ extern "C" velo_status velo_filter_groupby(const velo_lineitem* cols, size_t n, 
                                                                                 s.tail_prefix, s.n_groups);
     k_seg_emit<<<ntiles_s, SEG_THREADS, LiSeg::SMEM, st>>>(rc3, ntiles_s, s.aggs, s.carry, s.tail_prefix,
                                                            (int)group_bound, s.tile_out);
-    k_seg_finish<<<1, 256, 0, st>>>(s.tile_out, ntiles_s, (int)group_bound, d_out, s.d_rows, s.n_groups, d_counts);
+    k_seg_finish<<<1, 1024, 0, st>>>(s.tile_out, ntiles_s, (int)group_bound, d_out, s.d_rows, s.n_groups, d_counts);
     VELO_CUDA_TRY(cudaGetLastError(), "group-by launch");
     return VELO_OK;
 }

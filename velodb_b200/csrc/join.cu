@@ -24,9 +24,10 @@
 
 namespace velo {
 
-using JRec = RowRec<2, 1>;
-using GRec = RowRec<3, 1>;
-using TRec = RowRec<3, 3>;
+// ties (fact rows of one key) are aggregated, their order is irrelevant
+using JRec = RowRec<2, 1, false>;
+using GRec = RowRec<3, 1, false>;
+using TRec = RowRec<3, 3, false>;
 constexpr uint64_t J_KEYTAG = 0xFFFFFFFF80000000ull;
 constexpr uint64_t J_JOINED = 1ull << 29;
 constexpr int J_LOG_NT = 8, J_LOG_E = 4; // 4096-row tiles

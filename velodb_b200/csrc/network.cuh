@@ -51,9 +51,9 @@ template <>
 struct MarkAt<RowKPM> {
     __device__ __forceinline__ static bool get(const RowKPM::Cols& c, size_t g) { return c.m[g] != 0; }
 };
-template <int W, int KW>
-struct MarkAt<RowRec<W, KW>> {
-    __device__ __forceinline__ static bool get(const typename RowRec<W, KW>::Cols& c, size_t g)
+template <int W, int KW, bool S>
+struct MarkAt<RowRec<W, KW, S>> {
+    __device__ __forceinline__ static bool get(const typename RowRec<W, KW, S>::Cols& c, size_t g)
     {
         return (((c.w[0][g] >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
     }
@@ -92,31 +92,40 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* t
     return r;
 }
 
-// calls f(std::integral_constant<int, v>) for a runtime v in [0, N)
-template <int I, int N, class F>
-__device__ __forceinline__ void static_switch(int v, F& f)
-{
-    if constexpr (I < N) {
-        if (v == I)
-            f(std::integral_constant<int, I> {});
-        else
-            static_switch<I + 1, N>(v, f);
+// compile-time loops over register bits: f(integral_constant<Q>) for
+// Q = HI down to 0, or 0 up to HI
+template <int Q>
+struct QDown {
+    template <class F>
+    __device__ __forceinline__ static void run(F& f)
+    {
+        f(std::integral_constant<int, Q> {});
+        QDown<Q - 1>::run(f);
     }
-}
-
-// exchange decision for the pair (a at the lower index, b): ascending swaps
-// iff a > b, descending iff a < b (strict, as include/cuda/sort.cuh:31-40)
-template <class R>
-__device__ __forceinline__ bool need_swap(const R& a, const R& b, bool desc, const typename R::Cols& c)
-{
-    if constexpr (R::FULL_KEY) {
-        // every field is compared, so equal rows are identical and swapping
-        // them is a no-op: one comparison decides both directions
-        return R::gt(a, b, c) != desc;
-    } else {
-        return desc ? R::gt(b, a, c) : R::gt(a, b, c);
+};
+template <>
+struct QDown<-1> {
+    template <class F>
+    __device__ __forceinline__ static void run(F&)
+    {
     }
-}
+};
+template <int Q, int HI>
+struct QUp {
+    template <class F>
+    __device__ __forceinline__ static void run(F& f)
+    {
+        f(std::integral_constant<int, Q> {});
+        QUp<Q + 1, HI>::run(f);
+    }
+};
+template <int HI>
+struct QUp<HI, HI> {
+    template <class F>
+    __device__ __forceinline__ static void run(F&)
+    {
+    }
+};
 
 template <class R, int LOG_NT, int LOG_E>
 struct Net {
@@ -126,61 +135,55 @@ struct Net {
     static constexpr int LT = TL::LOG_T;
     static constexpr int T = TL::T;
     static constexpr int S0 = LT - LOG_E; // load/store layout (lanes <-> rows 0..31)
-    static constexpr int NS = S0 + 1;     // layouts 0..S0
 
     static constexpr size_t smem_rows() { return ((size_t)T * R::SMEM_BYTES + 15) & ~(size_t)15; }
     static constexpr size_t smem_bytes_sort() { return smem_rows(); }
     static constexpr size_t smem_bytes_compact() { return smem_rows() + (size_t)T * 4 + 33 * 4; }
 
-    // thread part of the local row index in layout S
-    template <int S>
-    __device__ __forceinline__ static int tidpart()
+    // thread part of the local row index in layout s
+    __device__ __forceinline__ static int tidpart(int s)
     {
         const int tid = threadIdx.x;
-        return (tid & ((1 << S) - 1)) | ((tid >> S) << (S + LOG_E));
+        return (tid & ((1 << s) - 1)) | ((tid >> s) << (s + LOG_E));
     }
 
-    template <int S>
-    __device__ __forceinline__ static void sstore_all(const R (&v)[E], char* sm)
-    {
-        const int tp = tidpart<S>();
-#pragma unroll
-        for (int e = 0; e < E; e++)
-            R::sstore(sm, T, TL::swz(tp | (e << S)), v[e]);
-    }
-    template <int S>
-    __device__ __forceinline__ static void sload_all(R (&v)[E], const char* sm)
-    {
-        const int tp = tidpart<S>();
-#pragma unroll
-        for (int e = 0; e < E; e++)
-            v[e] = R::sload(sm, T, TL::swz(tp | (e << S)));
-    }
-
-    // re-layout the tile from layout `from` to layout `to` through smem
+    // re-layout the tile from layout `from` to layout `to` through smem; the
+    // slot of register e is swz(tp | e<<s) = swz(tp) ^ swz(e<<s)
     __device__ __forceinline__ static void transpose(R (&v)[E], int from, int to, char* sm)
     {
         __syncthreads();
-        auto st = [&](auto sc) { sstore_all<decltype(sc)::value>(v, sm); };
-        static_switch<0, NS>(from, st);
+        {
+            const int base = TL::swz(tidpart(from));
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                R::sstore(sm, T, base ^ TL::swz(e << from), v[e]);
+        }
         __syncthreads();
-        auto ld = [&](auto sc) { sload_all<decltype(sc)::value>(v, sm); };
-        static_switch<0, NS>(to, ld);
+        {
+            const int base = TL::swz(tidpart(to));
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                v[e] = R::sload(sm, T, base ^ TL::swz(e << to));
+        }
     }
 
-    // ---- bitonic compare-exchange on register bit Q in layout S -----------
-    template <int S, int Q>
-    __device__ __forceinline__ static void bitonic_level(R (&v)[E], const Cols& c, int K, bool dconst, bool asc_c)
+    // ---- bitonic compare-exchange on register bit Q -----------------------
+    // The direction of a pair is bit K of its local index (phase k = 2^K).
+    // It is one mask `dm` for all of a thread's pairs unless K falls inside
+    // the register window (only for phases k < 2^LOG_E), where pair e is
+    // descending iff bit `dbit` of e is set.
+    template <int Q, bool PER_E>
+    __device__ __forceinline__ static void bitonic_level(R (&v)[E], const Cols& c, uint32_t dm, int dbit)
     {
-        const int tp = tidpart<S>();
-        const bool tdesc = ((tp >> K) & 1) != 0; // thread part of the direction bit
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
                 continue;
             const int e2 = e | (1 << Q);
-            const bool desc = dconst ? !asc_c : (tdesc | ((((e << S) >> K) & 1) != 0));
-            const bool sw = need_swap(v[e], v[e2], desc, c);
+            uint32_t d = dm;
+            if constexpr (PER_E)
+                d = ((e >> dbit) & 1) ? ~0u : 0u;
+            const bool sw = R::swap_mask(v[e], v[e2], d, c) != 0;
             const R a = R::select(sw, v[e2], v[e]);
             const R b = R::select(sw, v[e], v[e2]);
             v[e] = a;
@@ -188,15 +191,24 @@ struct Net {
         }
     }
 
-    __device__ __forceinline__ static void bitonic(int s, int q, R (&v)[E], const Cols& c, int K, bool dconst,
-                                                   bool asc_c)
+    // levels on local bits b_hi down to b_lo, all inside the window of layout s
+    __device__ __forceinline__ static void bitonic_window(R (&v)[E], const Cols& c, int s, int b_hi, int b_lo, int K,
+                                                          bool dconst, bool asc_c)
     {
-        auto fs = [&](auto sc) {
-            constexpr int S = decltype(sc)::value;
-            auto fq = [&](auto qc) { bitonic_level<S, decltype(qc)::value>(v, c, K, dconst, asc_c); };
-            static_switch<0, LOG_E>(q, fq);
+        const bool per_e = !dconst && K >= s && K < s + LOG_E;
+        const uint32_t dm = dconst ? (asc_c ? 0u : ~0u) : ((((tidpart(s) >> K) & 1) != 0) ? ~0u : 0u);
+        const int dbit = K - s;
+        auto f = [&](auto qc) {
+            constexpr int Q = decltype(qc)::value;
+            const int b = s + Q;
+            if (b <= b_hi && b >= b_lo) {
+                if (per_e)
+                    bitonic_level<Q, true>(v, c, dm, dbit);
+                else
+                    bitonic_level<Q, false>(v, c, dm, dbit);
+            }
         };
-        static_switch<0, NS>(s, fs);
+        QDown<LOG_E - 1>::run(f);
     }
 
     // ---- ORCompact exchange (tile-local level, block size 2^(b+1)) --------
@@ -204,18 +216,18 @@ struct Net {
     // and its left-half mark count is P[S + 2^b] - P[S] (P = exclusive prefix
     // of the original marks; block counts are invariant under the
     // permutations of lower levels).
-    template <int S, int Q>
-    __device__ __forceinline__ static void compact_level_tile(R (&v)[E], const Cols& c, int b, uint32_t p_tile,
+    template <int Q>
+    __device__ __forceinline__ static void compact_level_tile(R (&v)[E], const Cols& c, int s, int b, uint32_t p_tile,
                                                               const uint32_t* pre)
     {
-        const int tp = tidpart<S>();
+        const int tp = tidpart(s);
         const uint32_t half = 1u << b;
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
                 continue;
             const int e2 = e | (1 << Q);
-            const int l = tp | (e << S);
+            const int l = tp | (e << s);
             const int blk = l & ~(int)(2 * half - 1);
             const uint32_t ps = p_tile + pre[blk];
             bool sw;
@@ -238,19 +250,19 @@ struct Net {
         }
     }
 
-    template <int S, int Q>
-    __device__ __forceinline__ static void compact_level_global(R (&v)[E], const Cols& c, int b,
+    template <int Q>
+    __device__ __forceinline__ static void compact_level_global(R (&v)[E], const Cols& c, int s, int b,
                                                                 const uint32_t* tile_prefix, int C, int b_lo,
                                                                 size_t cta_bits)
     {
-        const int tp = tidpart<S>();
+        const int tp = tidpart(s);
         const uint64_t half = 1ull << b;
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
                 continue;
             const int e2 = e | (1 << Q);
-            const int l = tp | (e << S);
+            const int l = tp | (e << s);
             const uint64_t g = (uint64_t)(l & ((1 << C) - 1)) | ((uint64_t)(l >> C) << b_lo) | cta_bits;
             const uint64_t blk = g & ~(2 * half - 1);
             const uint32_t ps = tile_prefix[blk >> LT];
@@ -273,7 +285,6 @@ struct Net {
     __device__ static void run(const Cols& c, const NetGeom& g, const NetPass& p, const uint32_t* tile_prefix,
                                int cta, char* sm)
     {
-        const int tid = threadIdx.x;
         const size_t Np = (size_t)1 << g.logN;
         const bool is_global = (p.kind == P_SORT_GLOBAL) || (p.kind == P_COMPACT_GLOBAL);
         int C = LT, b_lo = 0;
@@ -295,111 +306,111 @@ struct Net {
         int s = (p.kind == P_COMPACT_GLOBAL) ? smin : S0;
         const bool first = (p.kind == P_SORT_TILE) || (p.kind == P_COMPACT_TILE);
         {
-            auto ld = [&](auto sc) {
-                constexpr int S = decltype(sc)::value;
-                const int tp = tidpart<S>();
+            const int tp = tidpart(s);
 #pragma unroll
-                for (int e = 0; e < E; e++) {
-                    const size_t gi = gidx(tp | (e << S));
-                    if (first)
-                        v[e] = (gi < g.n) ? R::load(c, gi) : R::pad(c);
-                    else
-                        v[e] = R::load(c, gi);
-                }
-            };
-            static_switch<0, NS>(s, ld);
+            for (int e = 0; e < E; e++) {
+                const size_t gi = gidx(tp | (e << s));
+                if (first)
+                    v[e] = (gi < g.n) ? R::load(c, gi) : R::pad(c);
+                else
+                    v[e] = R::load(c, gi);
+            }
         }
 
         if constexpr (SORT) {
-        if (p.kind == P_SORT_TILE) {
-            for (int K = 1; K <= p.K; K++) {
-                const bool dconst = K >= LT;
-                const bool asc_c = ((cta_bits >> K) & 1) == 0;
-                for (int b = K - 1; b >= 0; b--) {
+            if (p.kind == P_SORT_TILE) {
+                for (int K = 1; K <= p.K; K++) {
+                    const bool dconst = K >= LT;
+                    const bool asc_c = ((cta_bits >> K) & 1) == 0;
+                    int b = K - 1;
+                    while (b >= 0) {
+                        if (b < s || b >= s + LOG_E) {
+                            const int ns = window_down(b, LOG_E, LT);
+                            transpose(v, s, ns, sm);
+                            s = ns;
+                        }
+                        bitonic_window(v, c, s, b, s, K, dconst, asc_c);
+                        b = s - 1;
+                    }
+                }
+            } else {
+                // MERGE: bits LT-1..0; GLOBAL: local bits C+L-1..C (the L fused
+                // global levels); the direction is fixed for the tile
+                const bool asc_c = (((p.kind == P_SORT_MERGE ? cta_bits : gidx(0)) >> p.K) & 1) == 0;
+                const int top = (p.kind == P_SORT_MERGE) ? LT - 1 : C + p.L - 1;
+                const int bottom = (p.kind == P_SORT_MERGE) ? 0 : C;
+                int b = top;
+                while (b >= bottom) {
                     if (b < s || b >= s + LOG_E) {
-                        const int ns = window_down(b, LOG_E, LT);
+                        int ns = window_down(b, LOG_E, LT);
+                        ns = ns < smin ? smin : ns;
                         transpose(v, s, ns, sm);
                         s = ns;
                     }
-                    bitonic(s, b - s, v, c, K, dconst, asc_c);
+                    const int lo = s > bottom ? s : bottom;
+                    bitonic_window(v, c, s, b, lo, p.K, true, asc_c);
+                    b = lo - 1;
                 }
             }
-        } else if (p.kind == P_SORT_MERGE) {
-            const bool asc_c = ((cta_bits >> p.K) & 1) == 0;
-            for (int b = LT - 1; b >= 0; b--) {
-                if (b < s || b >= s + LOG_E) {
-                    const int ns = window_down(b, LOG_E, LT);
-                    transpose(v, s, ns, sm);
-                    s = ns;
-                }
-                bitonic(s, b - s, v, c, p.K, true, asc_c);
-            }
-        } else if (p.kind == P_SORT_GLOBAL) {
-            const bool asc_c = ((gidx(0) >> p.K) & 1) == 0;
-            for (int b = p.b_hi; b >= b_lo; b--) {
-                const int lp = C + (b - b_lo);
-                if (lp < s || lp >= s + LOG_E) {
-                    int ns = window_down(lp, LOG_E, LT);
-                    ns = ns < smin ? smin : ns;
-                    transpose(v, s, ns, sm);
-                    s = ns;
-                }
-                bitonic(s, lp - s, v, c, p.K, true, asc_c);
-            }
-        }
         } else {
-        if (p.kind == P_COMPACT_TILE) {
-            // prefix of the original marks over the tile, in local-index order
-            uint32_t* pre = reinterpret_cast<uint32_t*>(sm + smem_rows());
-            uint32_t* tmp = pre + T;
-            transpose(v, s, 0, sm);
-            s = 0;
-            uint32_t cnt = 0, m[E];
+            if (p.kind == P_COMPACT_TILE) {
+                // prefix of the original marks over the tile, in local-index order
+                uint32_t* pre = reinterpret_cast<uint32_t*>(sm + smem_rows());
+                uint32_t* tmp = pre + T;
+                transpose(v, s, 0, sm);
+                s = 0;
+                uint32_t cnt = 0, m[E];
 #pragma unroll
-            for (int e = 0; e < E; e++) {
-                m[e] = cnt;
-                cnt += MarkOf<R>::get(v[e], c) ? 1u : 0u;
-            }
-            uint32_t total;
-            const uint32_t base = block_exclusive_scan(cnt, tmp, &total);
-            const int tp0 = tidpart<0>();
+                for (int e = 0; e < E; e++) {
+                    m[e] = cnt;
+                    cnt += MarkOf<R>::get(v[e], c) ? 1u : 0u;
+                }
+                uint32_t total;
+                const uint32_t base = block_exclusive_scan(cnt, tmp, &total);
+                const int tp0 = tidpart(0);
 #pragma unroll
-            for (int e = 0; e < E; e++)
-                pre[tp0 | e] = base + m[e];
-            __syncthreads();
-            const uint32_t p_tile = tile_prefix[cta];
-            for (int b = 0; b < p.K; b++) {
-                if (b < s || b >= s + LOG_E) {
-                    const int ns = window_up(b, LOG_E, LT);
-                    transpose(v, s, ns, sm);
-                    s = ns;
-                }
-                auto fs = [&](auto sc) {
-                    constexpr int S = decltype(sc)::value;
-                    auto fq = [&](auto qc) { compact_level_tile<S, decltype(qc)::value>(v, c, b, p_tile, pre); };
-                    static_switch<0, LOG_E>(b - S, fq);
-                };
-                static_switch<0, NS>(s, fs);
-            }
-        } else { // P_COMPACT_GLOBAL
-            for (int b = b_lo; b <= p.b_hi; b++) {
-                const int lp = C + (b - b_lo);
-                if (lp < s || lp >= s + LOG_E) {
-                    int ns = window_up(lp, LOG_E, LT);
-                    ns = ns < smin ? smin : ns;
-                    transpose(v, s, ns, sm);
-                    s = ns;
-                }
-                auto fs = [&](auto sc) {
-                    constexpr int S = decltype(sc)::value;
-                    auto fq = [&](auto qc) {
-                        compact_level_global<S, decltype(qc)::value>(v, c, b, tile_prefix, C, b_lo, cta_bits);
+                for (int e = 0; e < E; e++)
+                    pre[tp0 | e] = base + m[e];
+                __syncthreads();
+                const uint32_t p_tile = tile_prefix[cta];
+                int b = 0;
+                while (b < p.K) {
+                    if (b < s || b >= s + LOG_E) {
+                        const int ns = window_up(b, LOG_E, LT);
+                        transpose(v, s, ns, sm);
+                        s = ns;
+                    }
+                    const int hi = (s + LOG_E - 1 < p.K - 1) ? s + LOG_E - 1 : p.K - 1;
+                    auto f = [&](auto qc) {
+                        constexpr int Q = decltype(qc)::value;
+                        const int bb = s + Q;
+                        if (bb >= b && bb <= hi)
+                            compact_level_tile<Q>(v, c, s, bb, p_tile, pre);
                     };
-                    static_switch<0, LOG_E>(lp - S, fq);
-                };
-                static_switch<0, NS>(s, fs);
+                    QUp<0, LOG_E>::run(f);
+                    b = hi + 1;
+                }
+            } else { // P_COMPACT_GLOBAL: local bits C..C+L-1 bottom-up
+                int lb = C;
+                const int top = C + p.L - 1;
+                while (lb <= top) {
+                    if (lb < s || lb >= s + LOG_E) {
+                        int ns = window_up(lb, LOG_E, LT);
+                        ns = ns < smin ? smin : ns;
+                        transpose(v, s, ns, sm);
+                        s = ns;
+                    }
+                    const int hi = (s + LOG_E - 1 < top) ? s + LOG_E - 1 : top;
+                    auto f = [&](auto qc) {
+                        constexpr int Q = decltype(qc)::value;
+                        const int lp = s + Q;
+                        if (lp >= lb && lp <= hi)
+                            compact_level_global<Q>(v, c, s, b_lo + (lp - C), tile_prefix, C, b_lo, cta_bits);
+                    };
+                    QUp<0, LOG_E>::run(f);
+                    lb = hi + 1;
+                }
             }
-        }
         }
 
         if (s < 5) {
@@ -407,17 +418,13 @@ struct Net {
             s = S0;
         }
         {
-            auto stf = [&](auto sc) {
-                constexpr int S = decltype(sc)::value;
-                const int tp = tidpart<S>();
+            const int tp = tidpart(s);
 #pragma unroll
-                for (int e = 0; e < E; e++) {
-                    const size_t gi = gidx(tp | (e << S));
-                    if (gi < Np)
-                        R::store(c, gi, v[e]);
-                }
-            };
-            static_switch<0, NS>(s, stf);
+            for (int e = 0; e < E; e++) {
+                const size_t gi = gidx(tp | (e << s));
+                if (gi < Np)
+                    R::store(c, gi, v[e]);
+            }
         }
     }
 };

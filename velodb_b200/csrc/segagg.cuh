@@ -27,6 +27,10 @@ constexpr int SEG_TS = 2048;     // rows per tile
 constexpr int SEG_THREADS = 256; // 8 contiguous rows per thread
 constexpr int SEG_RPT = SEG_TS / SEG_THREADS;
 constexpr int SEG_MAX_G = 16;
+// smem row slot with one pad word per 8 rows, so the 8 contiguous rows of each
+// thread start on different banks
+__device__ __forceinline__ int seg_slot(int i) { return i + (i >> 3); }
+constexpr int SEG_TS_PAD = SEG_TS + SEG_TS / 8;
 
 struct SegTileAgg {
     uint64_t head_key;
@@ -95,7 +99,7 @@ struct SegAgg {
     static constexpr int V = Agg::V;
     // the tile area holds the W input words, later the 1+V output words
     static constexpr int TW = W > 1 + V ? W : 1 + V;
-    static constexpr size_t SMEM = (size_t)SEG_TS * TW * 8 + (size_t)V * SEG_THREADS * 8 + SEG_THREADS * 4 + 64;
+    static constexpr size_t SMEM = (size_t)SEG_TS_PAD * TW * 8 + (size_t)V * SEG_THREADS * 8 + SEG_THREADS * 4 + 256;
 
     // stage the tile's records in smem (coalesced), then thread t owns rows
     // [t*RPT, t*RPT + RPT)
@@ -104,7 +108,7 @@ struct SegAgg {
         for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
 #pragma unroll
             for (int x = 0; x < W; x++)
-                sw[x * SEG_TS + i] = words[x][base + i];
+                sw[x * SEG_TS_PAD + seg_slot(i)] = words[x][base + i];
         }
         __syncthreads();
     }
@@ -113,7 +117,7 @@ struct SegAgg {
     {
 #pragma unroll
         for (int x = 0; x < W; x++)
-            w[x] = sw[x * SEG_TS + i];
+            w[x] = sw[x * SEG_TS_PAD + seg_slot(i)];
     }
 
     // pass A
@@ -121,8 +125,8 @@ struct SegAgg {
                                         char* smem)
     {
         uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
-        uint32_t* tmp = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS * TW * 8);
-        int64_t* red = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS * TW * 8 + 256);
+        uint32_t* tmp = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS_PAD * TW * 8);
+        int64_t* red = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * TW * 8 + 256);
         const size_t base = (size_t)tile * SEG_TS;
         load_tile(words, base, sw);
         uint64_t wl[W];
@@ -286,8 +290,8 @@ struct SegAgg {
                                 char* smem)
     {
         uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
-        int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS * TW * 8);
-        uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS * TW * 8 + (size_t)V * SEG_THREADS * 8);
+        int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * TW * 8);
+        uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS_PAD * TW * 8 + (size_t)V * SEG_THREADS * 8);
         const size_t base = (size_t)tile * SEG_TS;
         load_tile(words, base, sw);
         const uint64_t next_head = (tile + 1 < ntiles) ? aggs[tile + 1].head_key : ~0ull;
@@ -359,13 +363,8 @@ struct SegAgg {
 #pragma unroll
         for (int r = 0; r < SEG_RPT; r++)
             my_tails += tail[r] ? 1u : 0u;
-        __syncthreads();
-        uint32_t* cnt = reinterpret_cast<uint32_t*>(svals);
-        cnt[threadIdx.x] = my_tails;
-        __syncthreads();
-        uint32_t before = 0;
-        for (int t = 0; t < (int)threadIdx.x; t++)
-            before += cnt[t];
+        uint32_t tails_total;
+        const uint32_t before = block_exclusive_scan(my_tails, reinterpret_cast<uint32_t*>(svals), &tails_total);
         const uint32_t rank0 = tail_prefix[tile] + before;
 
         // my leading rows continue the run open at the end of thread t-1
@@ -430,8 +429,8 @@ struct SegAgg {
                                      const int64_t* carry_in, uint64_t* const* out, char* smem)
     {
         uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
-        int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS * TW * 8);
-        uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS * TW * 8 + (size_t)V * SEG_THREADS * 8);
+        int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * TW * 8);
+        uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS_PAD * TW * 8 + (size_t)V * SEG_THREADS * 8);
         const size_t base = (size_t)tile * SEG_TS;
         load_tile(words, base, sw);
         const uint64_t next_head = (tile + 1 < ntiles) ? aggs[tile + 1].head_key : ~0ull;
@@ -507,28 +506,31 @@ struct SegAgg {
             if (r > 0)
                 lead = lead & (keys[r] == keys[r - 1]);
             const bool first_run_of_tile = (keys[r] == head_key);
-            so[r0 + r] = ((uint64_t)(!tail[r]) << 63) | Agg::out_bits(keys[r]);
+            so[seg_slot(r0 + r)] = ((uint64_t)(!tail[r]) << 63) | Agg::out_bits(keys[r]);
 #pragma unroll
             for (int i = 0; i < V; i++)
-                so[(size_t)(1 + i) * SEG_TS + r0 + r] =
+                so[(size_t)(1 + i) * SEG_TS_PAD + seg_slot(r0 + r)] =
                     (uint64_t)(pref[r][i] + (lead ? cin[i] : 0) + (first_run_of_tile ? tc[i] : 0));
         }
         __syncthreads();
         for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
 #pragma unroll
             for (int x = 0; x <= V; x++)
-                out[x][base + i] = so[(size_t)x * SEG_TS + i];
+                out[x][base + i] = so[(size_t)x * SEG_TS_PAD + seg_slot(i)];
         }
     }
 
     // pass D: out[j] = sum over tiles of tile_out[tile][j] (one CTA)
     __device__ static void finish(const int64_t* tile_out, int ntiles, int G, int64_t* out)
     {
-        for (int q = threadIdx.x; q < G * (1 + V); q += blockDim.x) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int q = warp; q < G * (1 + V); q += nw) {
             int64_t sum = 0;
-            for (int t = 0; t < ntiles; t++)
+            for (int t = lane; t < ntiles; t += 32)
                 sum += tile_out[(size_t)t * G * (1 + V) + q];
-            out[q] = sum;
+            sum = warp_sum_i64(sum);
+            if (lane == 0)
+                out[q] = sum;
         }
     }
 };
