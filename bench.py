@@ -30,6 +30,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+# DRAM bytes (read + write) per launch of the dominant kernel from one ncu
+# capture (profiles/), or None when not captured for the workload.
+TRAFFIC = {"groupby": None, "sort": None}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -178,9 +182,45 @@ class GroupBy:
         return bool(ok)
 
     def dominant(self, device):
-        """Times the bitonic passes of the pipeline's sort (the dominant
-        kernel) on the pipeline's own record shape: 2^23 rows x 3 words."""
-        return None
+        """The dominant kernel is the bitonic pass kernel of the pipeline's
+        sort (about 80 % of the step in the ncu launch list).  It is timed
+        here on the pipeline's own record shape and tile configuration:
+        next_pow2(6,001,215) = 2^23 records of 3 u64 words, 4096-row tiles of
+        256 threads.  Every launch reads and writes every record once, so
+        its algorithmic bytes are 2 x 2^23 x 24 B."""
+        torch, capi = self.torch, self.capi
+        from velodb_b200 import workloads as W
+
+        n = self.np_rows
+        src = [capi.to_dev_u64(W.splitmix64(7, n, i)) for i in range(3)]
+        ws = [x.clone() for x in src]
+        logn = int(np.log2(n))
+        launches = sort_passes(logn, 12, 7)
+
+        def run():
+            capi.osort_records(ws, n, 0xFFFF800000000000, tune=(12, 256))
+
+        return dominant_timing(torch, run, lambda: [a.copy_(b) for a, b in zip(ws, src)], launches,
+                               2 * n * 24, "k_sort_pass<RowRec<3,1>> (bitonic passes, 2^23 x 24 B records)")
+
+
+def dominant_timing(torch, run, reset, launches, bytes_per_launch, name, reps=5):
+    """Average launch duration of the dominant kernel from CUDA events around
+    whole sorts (each sort = `launches` launches of the kernel), with the
+    input restored between sorts outside the timed events."""
+    ts = []
+    for i in range(reps + 1):
+        reset()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        run()
+        e.record()
+        torch.cuda.synchronize()
+        if i:
+            ts.append(s.elapsed_time(e))
+    per_launch_ms = float(np.mean(ts)) / launches
+    return {"kernel": name, "launches_per_sort": launches, "avg_launch_us": per_launch_ms * 1e3,
+            "bytes_per_launch": int(bytes_per_launch)}
 
 
 def make_workload(name, torch, capi, W, device):
@@ -188,7 +228,127 @@ def make_workload(name, torch, capi, W, device):
         return GroupBy(torch, capi, W, device)
     if name == "sort":
         return SortKP(torch, capi, W, device)
+    if name == "batch":
+        return Batched(torch, capi, W, device)
     raise SystemExit(f"unknown workload {name}")
+
+
+class Batched:
+    """Config-3 shape: 512 independent instances (log-uniform 2^10..2^22
+    rows; even = sort of (u64 key, u32 payload), odd = compaction with
+    Bernoulli(0.3) keep flags), each padded to its own power of two, run by
+    ONE persistent launch captured in a CUDA graph, tile configuration picked
+    by the autotuner.  The plain path (one launch sequence per instance,
+    back to back) is timed beside it."""
+    name = "batched_512"
+
+    def __init__(self, torch, capi, W, device):
+        self.torch, self.capi = torch, capi
+        insts = W.batch_instances()
+        self.items = []
+        self.host = []
+        for it in insts:
+            n = it["n"]
+            cap = capi.next_pow2(n)
+            d = dict(kind=it["kind"], n=n, keys=capi.to_dev_u64(it["keys"], cap),
+                     pay=capi.to_dev_u32(it["pay"], cap))
+            if it["kind"] == "compact":
+                d["marks"] = capi.to_dev_u8(it["marks"], cap)
+                d["count"] = torch.zeros(1, dtype=torch.int64, device=device)
+            self.items.append(d)
+            self.host.append(it)
+        self.n = int(sum(it["n"] for it in insts))
+        self.np_rows = int(sum(capi.next_pow2(it["n"]) for it in insts))
+        self.rec_bytes = 12
+        self.flush_l2 = False  # 3.4 GB of instances, far beyond L2
+        self.in_bytes = int(sum(it["n"] * (12 + (1 if it["kind"] == "compact" else 0)) for it in insts))
+        self.tune, self.tune_ms = capi.batch_autotune(self.items, reps=1)
+        self.batch = capi.Batch(self.items, tune=self.tune)
+        self.stream = torch.cuda.Stream()
+        self.batch.launch(stream=self.stream)
+        self.batch.status(stream=self.stream)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=self.stream):
+            self.batch.launch(stream=self.stream)
+        self.pinned = [(torch.from_numpy(h["keys"].view(np.int64)).pin_memory(),
+                        torch.from_numpy(h["pay"].view(np.int32)).pin_memory()) for h in insts]
+        self.count_host = torch.zeros(len(self.items), dtype=torch.int64).pin_memory()
+
+    def step(self):
+        self.graph.replay()
+
+    def step_plain(self):
+        for it in self.items:
+            if it["kind"] == "sort":
+                self.capi.osort_kp(it["keys"], it["pay"], it["n"], tune=self.tune)
+            else:
+                self.capi.ocompact_kpm(it["keys"], it["pay"], it["marks"], it["n"], tune=self.tune)
+
+    def step_e2e(self):
+        for it, (k, p) in zip(self.items, self.pinned):
+            it["keys"][: it["n"]].copy_(k, non_blocking=True)
+            it["pay"][: it["n"]].copy_(p, non_blocking=True)
+        self.step()
+        for i, it in enumerate(self.items):
+            if "count" in it:
+                self.count_host[i: i + 1].copy_(it["count"], non_blocking=True)
+
+    def d2h_bytes(self):
+        return 8 * sum(1 for it in self.items if "count" in it)
+
+    def launches(self):
+        return 1  # one persistent kernel per step (plus one counter memset)
+
+    def rdm_bytes(self):
+        tot = 0
+        for it in self.items:
+            npr = self.capi.next_pow2(it["n"])
+            if it["kind"] == "sort":
+                tot += 2 * npr * 12 * rdm_psort(npr)
+            else:
+                tot += it["n"] * 5 + 2 * npr * 13 * rdm_pcomp(npr)
+        return tot
+
+    def check(self, orc):
+        self.batch.status(stream=self.stream)
+        ok = True
+        for it, h in list(zip(self.items, self.host))[:24]:
+            if it["kind"] == "sort":
+                k = it["keys"].cpu().numpy().view(np.uint64)[: it["n"]]
+                o = np.sort(h["keys"])
+                ok &= bool(np.array_equal(k, o))
+            else:
+                c = int(it["count"].item())
+                ok &= c == int(h["marks"].sum())
+                k = it["keys"].cpu().numpy().view(np.uint64)[:c]
+                ok &= bool(np.array_equal(k, h["keys"][h["marks"].astype(bool)]))
+        return ok
+
+    def dominant(self, device):
+        """The persistent scheduler kernel is the only kernel of the step;
+        its algorithmic bytes per launch are the batch's network bytes."""
+        torch = self.torch
+        ts = []
+        for i in range(4):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            self.graph.replay()
+            e.record()
+            torch.cuda.synchronize()
+            if i:
+                ts.append(s.elapsed_time(e))
+        bytes_ = 0
+        for it in self.items:
+            npr = self.capi.next_pow2(it["n"])
+            lt = self.tune[0]
+            lmax = min(8, lt - 5)
+            if it["kind"] == "sort":
+                bytes_ += 2 * npr * 12 * sort_passes(int(np.log2(npr)), lt, lmax)
+            else:
+                bytes_ += 2 * npr * 13 * compact_passes(int(np.log2(npr)), lt, lmax) + npr * 5
+        return {"kernel": f"k_sched (persistent, tile 2^{self.tune[0]} x {self.tune[1]} threads)",
+                "launches_per_sort": 1, "avg_launch_us": float(np.mean(ts)) * 1e3, "bytes_per_launch": int(bytes_)}
 
 
 class SortKP:
@@ -242,7 +402,16 @@ class SortKP:
         return bool(np.array_equal(k, ok_) and np.array_equal(p, op_))
 
     def dominant(self, device):
-        return None
+        """The bitonic pass kernel is the only kernel of the step; every
+        launch reads and writes every (8 B key + 4 B payload) row once."""
+        run = lambda: self.capi.osort_kp(self.k, self.p, self.n)  # noqa: E731
+
+        def reset():
+            self.k.copy_(self.k0)
+            self.p.copy_(self.p0)
+
+        return dominant_timing(self.torch, run, reset, self.launches(), 2 * self.n * 12,
+                               "k_sort_pass<RowKP> (bitonic passes, 2^20 x 12 B rows)")
 
 
 # --------------------------------------------------------------------------
@@ -340,6 +509,8 @@ def run_reference(args, rank):
 
 
 def metric_name(workload):
+    if workload == "batch":
+        return "batched oblivious sorts+compactions throughput (512 instances, 2^10..2^22 rows)"
     if workload == "sort":
         return "oblivious bitonic sort throughput (2^20 rows, u64 key + u32 payload)"
     return "oblivious filter+group-by input throughput (6,001,215-row fact table)"
@@ -351,7 +522,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "sort"])
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "sort", "batch"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -414,6 +585,18 @@ def main():
     e2e = {"value": world * rows_per_step / (ems / 1e3) / 1e6, "unit": "Mrows/s",
            "h2d_bytes_per_step": int(wl.in_bytes), "d2h_bytes_per_step": int(wl.d2h_bytes()), "ms_per_step": ems}
 
+    if hasattr(wl, "step_plain"):
+        for _ in range(2):
+            wl.step_plain()
+        torch.cuda.synchronize()
+        tp = time_steps(torch, wl.step_plain, max(3, args.steps // 2))
+        pms = float(np.mean(tp))
+        plain = {"ms_per_step": pms, "value": world * rows_per_step / (pms / 1e3) / 1e6,
+                 "speedup_batched_vs_plain": pms / ms, "tune": list(wl.tune),
+                 "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in wl.tune_ms.items()}}
+    else:
+        plain = None
+
     # the result of the last step is checked against the oracle (rank 0)
     peak, peak_kind = hbm_peak()
     rdm = wl.rdm_bytes()
@@ -430,13 +613,22 @@ def main():
                 "frac_of_hbm": rdm / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
         "clocks": clk,
     }
+    if plain is not None:
+        line["plain_path"] = plain
+    dom = wl.dominant(device)
+    achieved = dom["bytes_per_launch"] / (dom["avg_launch_us"] / 1e6) / 1e9
+    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                        if peak_kind == "measured" else "fallback", "traffic": TRAFFIC.get(args.workload),
+                        "kernel": dom["kernel"], "avg_launch_us": dom["avg_launch_us"],
+                        "algorithmic_bytes_per_launch": dom["bytes_per_launch"]}
     if rank == 0:
         import oracle as orc
 
         orc.lib()
         line["checked_against_oracle"] = wl.check(orc)
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = (cpu_baseline_sort if args.workload == "sort" else cpu_baseline_groupby)(W, orc)
+            line["cpu_baseline"] = (cpu_baseline_groupby if args.workload == "groupby" else cpu_baseline_sort)(W, orc)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

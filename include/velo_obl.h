@@ -147,6 +147,61 @@ velo_status velo_ocompact_kpm_noalloc(uint64_t* d_keys, uint32_t* d_payload, uin
                                       size_t capacity, uint64_t* d_count, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Batched form: one persistent launch for many independent commands        */
+/* ------------------------------------------------------------------------ */
+
+/* One command of a batch: an oblivious sort (as velo_osort_kp) or an
+ * ORCompact (as velo_ocompact_kpm) of caller-owned device buffers. */
+#define VELO_ITEM_SORT_KP 1u
+#define VELO_ITEM_COMPACT_KPM 2u
+typedef struct velo_batch_item {
+    uint32_t kind; /* VELO_ITEM_SORT_KP or VELO_ITEM_COMPACT_KPM */
+    uint32_t pad_;
+    uint64_t* d_keys;
+    uint32_t* d_payload;
+    uint8_t* d_marks;  /* compaction only */
+    size_t n;
+    size_t capacity;   /* >= next_pow2(n) rows */
+    uint64_t* d_count; /* compaction only: receives the number of marked rows */
+} velo_batch_item;
+
+typedef struct velo_batch velo_batch;
+
+/* Plans a batch: every command becomes a list of passes over tiles; all
+ * commands' (pass, tile) items are interleaved and run by one persistent
+ * kernel whose CTAs claim items in order and wait (bounded) only for the
+ * previous pass of the same command.  Replaces the reference's one-command-
+ * at-a-time persistent grid (src/cuda/persistent_kernel.cu:76-124,
+ * src/cuda/task_manager.cu:26-78).  Results are identical to running each
+ * command through velo_osort_kp / velo_ocompact_kpm with the same tune.
+ * Allocates the batch's device plan (cudaMalloc) here, never at launch. */
+velo_status velo_batch_create(const velo_batch_item* items, size_t n_items, const velo_tune* tune,
+                              velo_batch** out);
+/* Enqueues the whole batch on `stream`: a counter reset and ONE kernel
+ * launch, so the call can be captured into a CUDA graph and replayed. */
+velo_status velo_batch_launch(velo_batch* batch, void* stream);
+/* Synchronises `stream` and returns VELO_ETIMEDOUT if a device-side wait of
+ * the last launch ran out of time (the kernel never spins unbounded). */
+velo_status velo_batch_status(velo_batch* batch, void* stream);
+void velo_batch_destroy(velo_batch* batch);
+/* Limit of every device-side wait of the batch (default 2 s). */
+velo_status velo_batch_set_timeout(velo_batch* batch, uint64_t timeout_ns);
+/* Failure injection for tests: makes the first wait of command `item` wait
+ * for a completion count that is never reached, so it runs into the time
+ * limit; the launch still terminates and velo_batch_status reports
+ * VELO_ETIMEDOUT (the command's output is then undefined). */
+velo_status velo_batch_inject_unmet_wait(velo_batch* batch, uint32_t item);
+/* Autotuner: times the batch for every tile configuration of the search
+ * space (tiles 2^11, 2^12, 2^13 x 256, 512, 1024 threads; `reps` timed
+ * launches each), writes the fastest to *best and the per-configuration
+ * milliseconds to ms_out[9] (may be NULL).  Runs on the live buffers: the
+ * networks are data-oblivious, so the timing does not depend on the data;
+ * re-running keeps every sort's output and every compaction's marked prefix
+ * and count (the unmarked tail of a compaction is re-routed). */
+velo_status velo_batch_autotune(const velo_batch_item* items, size_t n_items, uint32_t reps, velo_tune* best,
+                                float* ms_out, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Filter + group-by (oblivious)                                            */
 /* ------------------------------------------------------------------------ */
 

@@ -24,6 +24,13 @@ PROTOS = {
     "velo_ocompact_kpm": (i32, [vp, vp, vp, sz, sz, vp, vp, sz, vp, vp]),
     "velo_compact_scratch_bytes": (sz, [sz, vp]),
     "velo_ocompact_kpm_noalloc": (i32, [vp, vp, vp, sz, sz, vp, vp]),
+    "velo_batch_create": (i32, [vp, sz, vp, vp]),
+    "velo_batch_launch": (i32, [vp, vp]),
+    "velo_batch_status": (i32, [vp, vp]),
+    "velo_batch_destroy": (None, [vp]),
+    "velo_batch_set_timeout": (i32, [vp, u64]),
+    "velo_batch_inject_unmet_wait": (i32, [vp, u32]),
+    "velo_batch_autotune": (i32, [vp, sz, u32, vp, vp, vp]),
     "velo_filter_groupby_scratch_bytes": (sz, [sz, u32]),
     "velo_filter_groupby": (i32, [vp, sz, vp, u32, u32, vp, vp, vp, sz, vp]),
     "velo_join_groupby_topk_scratch_bytes": (sz, [sz, sz]),
@@ -88,6 +95,11 @@ class VeloJoinTables(C.Structure):
 
 class VeloJoinPred(C.Structure):
     _fields_ = [("date_hi", C.c_int32), ("pad_", C.c_int32), ("price_hi", C.c_int64)]
+
+
+class VeloBatchItem(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("pad_", C.c_uint32), ("d_keys", C.c_void_p), ("d_payload", C.c_void_p),
+                ("d_marks", C.c_void_p), ("n", C.c_size_t), ("capacity", C.c_size_t), ("d_count", C.c_void_p)]
 
 
 def tune_ref(tune):

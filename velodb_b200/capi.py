@@ -190,3 +190,66 @@ def osort_records(words, n: int, key_mask: int, strict: bool = False, tune=None,
     check(lib().velo_osort_records(ptrs.ctypes.data, len(words), key_mask & 0xFFFFFFFFFFFFFFFF, n, cap,
                                    SORT_STRICT if strict else 0, tune_ref(tune), _stream(stream)),
           "velo_osort_records")
+
+
+ITEM_SORT_KP, ITEM_COMPACT_KPM = 1, 2
+
+
+class Batch:
+    """A planned batch of sorts/compactions run by one persistent launch
+    (velo_batch_*).  items: list of dicts with kind ('sort'|'compact'),
+    keys/pay/marks device tensors, n, and for compactions a count tensor."""
+
+    def __init__(self, items, tune=None):
+        import ctypes as C
+
+        from ._lib import VeloBatchItem
+
+        arr = (VeloBatchItem * max(1, len(items)))()
+        for i, it in enumerate(items):
+            kind = ITEM_SORT_KP if it["kind"] == "sort" else ITEM_COMPACT_KPM
+            cap = min(it["keys"].numel(), it["pay"].numel())
+            marks = it.get("marks")
+            cnt = it.get("count")
+            if marks is not None:
+                cap = min(cap, marks.numel())
+            arr[i] = VeloBatchItem(kind, 0, it["keys"].data_ptr(), it["pay"].data_ptr(),
+                                   marks.data_ptr() if marks is not None else None, it["n"], cap,
+                                   cnt.data_ptr() if cnt is not None else None)
+        self._arr = arr
+        self._n = len(items)
+        self.ptr = C.c_void_p()
+        check(lib().velo_batch_create(arr, len(items), tune_ref(tune), C.byref(self.ptr)), "velo_batch_create")
+
+    def launch(self, stream=None):
+        check(lib().velo_batch_launch(self.ptr, _stream(stream)), "velo_batch_launch")
+
+    def status(self, stream=None):
+        check(lib().velo_batch_status(self.ptr, _stream(stream)), "velo_batch_status")
+
+    def close(self):
+        if self.ptr:
+            lib().velo_batch_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_autotune(items, reps=2, stream=None):
+    """Runs the autotuner over the 9 tile configurations; returns
+    ((tile_log2, threads), {config: ms})."""
+    import ctypes as C
+
+    from ._lib import VeloTune
+
+    b = Batch(items)  # only to marshal the item array
+    best = VeloTune(0, 0)
+    ms = (C.c_float * 9)()
+    check(lib().velo_batch_autotune(b._arr, b._n, reps, C.byref(best), ms, _stream(stream)), "velo_batch_autotune")
+    b.close()
+    cands = [(11, 256), (11, 512), (11, 1024), (12, 256), (12, 512), (12, 1024), (13, 256), (13, 512), (13, 1024)]
+    return (best.tile_log2, best.threads), {c: float(m) for c, m in zip(cands, ms)}

@@ -13,6 +13,10 @@
 // write + read of the tile).  Global loads/stores use a layout with s >= 5 so
 // the 32 lanes of a warp touch 32 consecutive rows (fully coalesced).
 //
+// Global loads use ld.global.cg (cached in L2 only): within one persistent
+// launch a pass reads rows that other SMs wrote in the previous pass, so the
+// non-coherent L1 must not serve them.
+//
 // Every network step is data-independent: the same loads, stores and smem
 // accesses happen for any data of the same public size, and exchanges are
 // selects, never branches on data.
@@ -123,7 +127,10 @@ struct RowKP {
         uint32_t* p;
     };
     static constexpr int SMEM_BYTES = 12;
-    __device__ __forceinline__ static RowKP load(const Cols& c, size_t g) { return RowKP { c.k[g], c.p[g] }; }
+    __device__ __forceinline__ static RowKP load(const Cols& c, size_t g)
+    {
+        return RowKP { __ldcg(c.k + g), __ldcg(c.p + g) };
+    }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowKP& r)
     {
         c.k[g] = r.k;
@@ -164,7 +171,7 @@ struct RowKPM {
     static constexpr int SMEM_BYTES = 13;
     __device__ __forceinline__ static RowKPM load(const Cols& c, size_t g)
     {
-        return RowKPM { c.k[g], c.p[g], (uint32_t)c.m[g] };
+        return RowKPM { __ldcg(c.k + g), __ldcg(c.p + g), (uint32_t)__ldcg(c.m + g) };
     }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowKPM& r)
     {
@@ -216,7 +223,7 @@ struct RowRec {
         RowRec r;
 #pragma unroll
         for (int i = 0; i < W; i++)
-            r.w[i] = c.w[i][g];
+            r.w[i] = __ldcg(c.w[i] + g);
         return r;
     }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowRec& r)

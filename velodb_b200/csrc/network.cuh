@@ -49,13 +49,13 @@ struct MarkAt<RowKP> {
 };
 template <>
 struct MarkAt<RowKPM> {
-    __device__ __forceinline__ static bool get(const RowKPM::Cols& c, size_t g) { return c.m[g] != 0; }
+    __device__ __forceinline__ static bool get(const RowKPM::Cols& c, size_t g) { return __ldcg(c.m + g) != 0; }
 };
 template <int W, int KW, bool S>
 struct MarkAt<RowRec<W, KW, S>> {
     __device__ __forceinline__ static bool get(const typename RowRec<W, KW, S>::Cols& c, size_t g)
     {
-        return (((c.w[0][g] >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
+        return (((__ldcg(c.w[0] + g) >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
     }
 };
 
@@ -265,8 +265,8 @@ struct Net {
             const int l = tp | (e << s);
             const uint64_t g = (uint64_t)(l & ((1 << C) - 1)) | ((uint64_t)(l >> C) << b_lo) | cta_bits;
             const uint64_t blk = g & ~(2 * half - 1);
-            const uint32_t ps = tile_prefix[blk >> LT];
-            const uint32_t pm = tile_prefix[(blk + half) >> LT];
+            const uint32_t ps = __ldcg(tile_prefix + (blk >> LT));
+            const uint32_t pm = __ldcg(tile_prefix + ((blk + half) >> LT));
             const uint64_t left = pm - ps;
             const uint64_t off = ps & (2 * half - 1);
             const uint64_t i = g - blk;
@@ -372,7 +372,7 @@ struct Net {
                 for (int e = 0; e < E; e++)
                     pre[tp0 | e] = base + m[e];
                 __syncthreads();
-                const uint32_t p_tile = tile_prefix[cta];
+                const uint32_t p_tile = __ldcg(tile_prefix + cta);
                 int b = 0;
                 while (b < p.K) {
                     if (b < s || b >= s + LOG_E) {
@@ -456,7 +456,7 @@ __device__ __forceinline__ void scan_tiles(const uint32_t* counts, int ntiles, u
     uint32_t carry = 0;
     for (int base = 0; base < ntiles; base += blockDim.x) {
         const int i = base + threadIdx.x;
-        const uint32_t x = i < ntiles ? counts[i] : 0u;
+        const uint32_t x = i < ntiles ? __ldcg(counts + i) : 0u;
         uint32_t total;
         const uint32_t ex = block_exclusive_scan(x, tmp, &total);
         if (i < ntiles)

@@ -1,0 +1,6 @@
+// Instantiations of the persistent scheduler (autotuner tile configurations).
+#include "sched_impl.cuh"
+
+VELO_INSTANTIATE_SCHED(8, 5)
+VELO_INSTANTIATE_SCHED(9, 4)
+VELO_INSTANTIATE_SCHED(10, 3)
