@@ -390,7 +390,7 @@ class SortKP:
         return self.n * 12
 
     def launches(self):
-        return sort_passes(20, 13, 8)
+        return sort_passes(20, 12, 7)
 
     def rdm_bytes(self):
         return 2 * self.n * 12 * rdm_psort(self.n)

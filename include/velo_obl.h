@@ -57,7 +57,8 @@ typedef enum velo_type {
 } velo_type;
 
 /* Tile configuration of the network kernels: tile = 2^tile_log2 rows per CTA
- * (11..13; 14 for 12-byte rows), threads = 256/512/1024.  NULL = defaults. */
+ * (11..13), threads = 256/512/1024.  NULL = defaults (velo_osort_kp: 4096-row
+ * tiles of 256 threads; compaction: 8192-row tiles of 512 threads). */
 typedef struct velo_tune {
     uint32_t tile_log2;
     uint32_t threads;
@@ -145,6 +146,75 @@ size_t velo_compact_scratch_bytes(size_t capacity, const velo_tune* tune);
  * This entry point has no counterpart in the reference. */
 velo_status velo_ocompact_kpm_noalloc(uint64_t* d_keys, uint32_t* d_payload, uint8_t* d_marks, size_t n,
                                       size_t capacity, uint64_t* d_count, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Column operators of the reference command set (same semantics, including  */
+/* the reference's data-dependent addresses) -- for drop-in compatibility    */
+/* ------------------------------------------------------------------------ */
+
+/* OP_PERMUTE: out[i] = in[idx[i]], i < n (include/cuda/permute.cuh:24-40). */
+velo_status velo_permute(void* d_out, const void* d_in, const int64_t* d_indices, size_t n, uint32_t type,
+                         void* stream);
+/* OP_SCATTER: for rows with mask != 0, out_idx[i] = rank among kept rows
+ * (the order one block of include/cuda/scatter.cuh:16-81 produces; the
+ * reference's block order is nondeterministic); *d_count = kept rows. */
+size_t velo_scatter_scratch_bytes(size_t n);
+velo_status velo_scatter(const uint8_t* d_mask, size_t n, int32_t* d_out_indices, uint64_t* d_count, void* d_scratch,
+                         size_t scratch_bytes, void* stream);
+/* OP_GATHER: out[idx[i]] = in[i] where mask (NULL = all)
+ * (include/cuda/gather.cuh:28-45). */
+velo_status velo_gather(void* d_out, const void* d_in, const int32_t* d_indices, const uint8_t* d_mask, size_t n,
+                        uint32_t type, void* stream);
+/* OP_COMPARE_EQ: out[i] = (l[i] == r[i]); BOOLEAN and VARCHAR give all zeros
+ * and DATE compares as int32, as include/cuda/compare.cuh:25-91 does. */
+velo_status velo_compare_eq(const void* d_left, const void* d_right, uint8_t* d_out_mask, size_t n, uint32_t type,
+                            void* stream);
+/* OP_COMPOSE_POSITION_MAP: new[i] = old[sigma[i]]
+ * (include/cuda/oblivious_shuffle.cuh:10-21). */
+velo_status velo_compose_position_map(const uint32_t* d_old, const uint32_t* d_sigma, uint32_t* d_new, size_t n,
+                                      void* stream);
+/* OP_ENRICH_POSITIONS: pos[i] = map[rid[i]] (oblivious_shuffle.cuh:23-34).
+ * velo_ogather_u64 is the oblivious form. */
+velo_status velo_enrich_positions(const uint32_t* d_record_ids, const uint32_t* d_map, uint32_t* d_out, size_t n,
+                                  void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Oblivious shuffle, gather and PK-FK join                                 */
+/* ------------------------------------------------------------------------ */
+
+/* Oblivious re-shuffle of a position map on the device: map <- map o sigma
+ * with sigma the permutation that sorts the keys Philox4x32-10(i, counter,
+ * key) (Salmon et al., SC'11), applied by the bitonic network.  Replaces the
+ * host Fisher-Yates draw plus H2D copy of sigma plus the data-dependent
+ * compose (src/data/oblivious_table.cpp:170-202). */
+size_t velo_oshuffle_scratch_bytes(size_t n);
+velo_status velo_oshuffle_position_map(uint32_t* d_map, size_t n, uint64_t key, uint64_t counter, void* d_scratch,
+                                       size_t scratch_bytes, void* stream);
+
+/* Oblivious gather out[j] = table[rid[j]] (0 when rid >= table_n): union of
+ * table rows and requests, bitonic sort on (row, tag), forward fill, bitonic
+ * sort back to request order.  Replaces the data-dependent reads of
+ * OP_ENRICH_POSITIONS and of oblivious materialization
+ * (src/operator/materialization_operator.cpp:362-517, whose gather runs on the
+ * CPU with dummy reads); duplicate requests are served without dummies. */
+size_t velo_ogather_scratch_bytes(size_t table_n, size_t n_req);
+velo_status velo_ogather_u64(const uint64_t* d_table, size_t table_n, const uint32_t* d_rids, size_t n_req,
+                             uint64_t* d_out, void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* Oblivious PK-FK equi-join producing the reference join operators' output
+ * (pairs of build-side and probe-side row ids, as OP_SORT_MERGE_JOIN_WRITE
+ * and OP_HASH_JOIN_WRITE produce: include/cuda/sort_merge_join.cuh:141-199,
+ * include/cuda/hash_join.cuh:170-254), for a build side with unique keys.
+ * Rows with mask == 0 (NULL = all valid) do not join.  Output is padded to
+ * the public bound probe_n: rows [0, count) hold the pairs in key order,
+ * the rest -1.  d_counts: 2 u64 = (pairs, build rows whose key repeats an
+ * earlier build key -- nonzero means the build side was not a key).
+ * key_type: VELO_INTEGER or VELO_BIGINT. */
+size_t velo_ojoin_scratch_bytes(size_t build_n, size_t probe_n);
+velo_status velo_ojoin_pkfk(const void* d_build_keys, const uint8_t* d_build_mask, size_t build_n,
+                            const void* d_probe_keys, const uint8_t* d_probe_mask, size_t probe_n, uint32_t key_type,
+                            int64_t* d_out_build_rowid, int64_t* d_out_probe_rowid, uint64_t* d_counts,
+                            void* d_scratch, size_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Batched form: one persistent launch for many independent commands        */

@@ -246,3 +246,37 @@ def join_groupby_topk(dim: dict, fact: dict, pred: dict, k: int = 10, n_threads:
     g = int(g)
     m = min(g, k)
     return g, ofk[:m], osum[:m], ocnt[:m]
+
+
+# --------------------------------------------------------------------------
+# Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+# easy as 1, 2, 3", SC'11), restated in numpy: the keys of the device shuffle
+# --------------------------------------------------------------------------
+
+def philox_u64(idx: np.ndarray, counter: int, key: int) -> np.ndarray:
+    idx = np.asarray(idx, dtype=np.uint64)
+    m32 = np.uint64(0xFFFFFFFF)
+    c0 = idx & m32
+    c1 = idx >> np.uint64(32)
+    c2 = np.full_like(idx, counter & 0xFFFFFFFF)
+    c3 = np.full_like(idx, (counter >> 32) & 0xFFFFFFFF)
+    k0, k1 = key & 0xFFFFFFFF, (key >> 32) & 0xFFFFFFFF
+    with np.errstate(over="ignore"):
+        for _ in range(10):
+            p0 = np.uint64(0xD2511F53) * c0
+            p1 = np.uint64(0xCD9E8D57) * c2
+            hi0, lo0 = p0 >> np.uint64(32), p0 & m32
+            hi1, lo1 = p1 >> np.uint64(32), p1 & m32
+            c0, c1, c2, c3 = hi1 ^ c1 ^ np.uint64(k0), lo1, hi0 ^ c3 ^ np.uint64(k1), lo0
+            k0 = (k0 + 0x9E3779B9) & 0xFFFFFFFF
+            k1 = (k1 + 0xBB67AE85) & 0xFFFFFFFF
+    return (c1 << np.uint64(32)) | c0
+
+
+def shuffle_position_map(pmap: np.ndarray, key: int, counter: int) -> np.ndarray:
+    """map o sigma, sigma sorting the Philox keys (ties by map value, which the
+    network compares too)."""
+    n = len(pmap)
+    k = philox_u64(np.arange(n, dtype=np.uint64), counter, key)
+    order = np.lexsort((pmap.astype(np.uint64), k))
+    return pmap[order]

@@ -14,8 +14,7 @@ from velodb_b200 import capi, workloads as W
 
 pytestmark = pytest.mark.gpu
 
-TUNES = [(11, 256), (11, 512), (11, 1024), (12, 256), (12, 512), (12, 1024), (13, 256), (13, 512), (13, 1024),
-         (14, 1024)]
+TUNES = [(11, 256), (11, 512), (11, 1024), (12, 256), (12, 512), (12, 1024), (13, 256), (13, 512), (13, 1024)]
 
 
 def gpu_sort_kp(keys, pay, tune=None):

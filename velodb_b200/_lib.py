@@ -24,6 +24,19 @@ PROTOS = {
     "velo_ocompact_kpm": (i32, [vp, vp, vp, sz, sz, vp, vp, sz, vp, vp]),
     "velo_compact_scratch_bytes": (sz, [sz, vp]),
     "velo_ocompact_kpm_noalloc": (i32, [vp, vp, vp, sz, sz, vp, vp]),
+    "velo_permute": (i32, [vp, vp, vp, sz, u32, vp]),
+    "velo_scatter_scratch_bytes": (sz, [sz]),
+    "velo_scatter": (i32, [vp, sz, vp, vp, vp, sz, vp]),
+    "velo_gather": (i32, [vp, vp, vp, vp, sz, u32, vp]),
+    "velo_compare_eq": (i32, [vp, vp, vp, sz, u32, vp]),
+    "velo_compose_position_map": (i32, [vp, vp, vp, sz, vp]),
+    "velo_enrich_positions": (i32, [vp, vp, vp, sz, vp]),
+    "velo_oshuffle_scratch_bytes": (sz, [sz]),
+    "velo_oshuffle_position_map": (i32, [vp, sz, u64, u64, vp, sz, vp]),
+    "velo_ogather_scratch_bytes": (sz, [sz, sz]),
+    "velo_ogather_u64": (i32, [vp, sz, vp, sz, vp, vp, sz, vp]),
+    "velo_ojoin_scratch_bytes": (sz, [sz, sz]),
+    "velo_ojoin_pkfk": (i32, [vp, vp, sz, vp, vp, sz, u32, vp, vp, vp, vp, sz, vp]),
     "velo_batch_create": (i32, [vp, sz, vp, vp]),
     "velo_batch_launch": (i32, [vp, vp]),
     "velo_batch_status": (i32, [vp, vp]),

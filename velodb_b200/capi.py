@@ -253,3 +253,71 @@ def batch_autotune(items, reps=2, stream=None):
     b.close()
     cands = [(11, 256), (11, 512), (11, 1024), (12, 256), (12, 512), (12, 1024), (13, 256), (13, 512), (13, 1024)]
     return (best.tile_log2, best.threads), {c: float(m) for c, m in zip(cands, ms)}
+
+
+def _ptr(t):
+    return t.data_ptr() if t is not None else None
+
+
+def _scratch(nbytes, device):
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=device)
+
+
+def permute(out, inp, idx, n, type_id, stream=None):
+    check(lib().velo_permute(out.data_ptr(), inp.data_ptr(), idx.data_ptr(), n, type_id, _stream(stream)),
+          "velo_permute")
+
+
+def scatter(mask, n, out_idx, stream=None):
+    cnt = torch.zeros(1, dtype=torch.int64, device=mask.device)
+    sc = _scratch(lib().velo_scatter_scratch_bytes(n), mask.device)
+    check(lib().velo_scatter(mask.data_ptr(), n, out_idx.data_ptr(), cnt.data_ptr(), sc.data_ptr(), sc.numel(),
+                             _stream(stream)), "velo_scatter")
+    return cnt
+
+
+def gather(out, inp, idx, mask, n, type_id, stream=None):
+    check(lib().velo_gather(out.data_ptr(), inp.data_ptr(), idx.data_ptr(), _ptr(mask), n, type_id, _stream(stream)),
+          "velo_gather")
+
+
+def compare_eq(left, right, out, n, type_id, stream=None):
+    check(lib().velo_compare_eq(left.data_ptr(), right.data_ptr(), out.data_ptr(), n, type_id, _stream(stream)),
+          "velo_compare_eq")
+
+
+def compose_position_map(old, sigma, new, n, stream=None):
+    check(lib().velo_compose_position_map(old.data_ptr(), sigma.data_ptr(), new.data_ptr(), n, _stream(stream)),
+          "velo_compose_position_map")
+
+
+def enrich_positions(rids, pmap, out, n, stream=None):
+    check(lib().velo_enrich_positions(rids.data_ptr(), pmap.data_ptr(), out.data_ptr(), n, _stream(stream)),
+          "velo_enrich_positions")
+
+
+def oshuffle_position_map(pmap, n, key, counter, stream=None):
+    sc = _scratch(lib().velo_oshuffle_scratch_bytes(n), pmap.device)
+    check(lib().velo_oshuffle_position_map(pmap.data_ptr(), n, key & (2**64 - 1), counter & (2**64 - 1),
+                                           sc.data_ptr(), sc.numel(), _stream(stream)), "velo_oshuffle_position_map")
+
+
+def ogather_u64(table, table_n, rids, n_req, out, stream=None):
+    sc = _scratch(lib().velo_ogather_scratch_bytes(table_n, n_req), table.device)
+    check(lib().velo_ogather_u64(table.data_ptr(), table_n, rids.data_ptr(), n_req, out.data_ptr(), sc.data_ptr(),
+                                 sc.numel(), _stream(stream)), "velo_ogather_u64")
+
+
+def ojoin_pkfk(build_keys, build_mask, probe_keys, probe_mask, key_type, stream=None):
+    """Returns (build rowids, probe rowids, counts[2]) device tensors; rows
+    past counts[0] are -1."""
+    bn, pn = build_keys.numel(), probe_keys.numel()
+    dev = build_keys.device
+    ob = torch.empty(max(pn, 1), dtype=torch.int64, device=dev)
+    op = torch.empty(max(pn, 1), dtype=torch.int64, device=dev)
+    cnt = torch.zeros(2, dtype=torch.int64, device=dev)
+    sc = _scratch(lib().velo_ojoin_scratch_bytes(bn, pn), dev)
+    check(lib().velo_ojoin_pkfk(build_keys.data_ptr(), _ptr(build_mask), bn, probe_keys.data_ptr(), _ptr(probe_mask),
+                                pn, key_type, ob.data_ptr(), op.data_ptr(), cnt.data_ptr(), sc.data_ptr(), sc.numel(),
+                                _stream(stream)), "velo_ojoin_pkfk")
+    return ob, op, cnt

@@ -118,41 +118,50 @@ __device__ __forceinline__ T sel(bool c, T a, T b)
 }
 
 // (u64 key, u32 payload), ordered lexicographically on both (plain sort rows).
-// Every field is compared, so the sorted output is unique.
+// Every field is compared, so the sorted output is unique.  Registers hold
+// the key as two 32-bit halves so exchanges never repack 64-bit values.
 struct RowKP {
-    uint64_t k;
-    uint32_t p;
+    uint32_t kl, kh, p;
     struct Cols {
         uint64_t* k;
         uint32_t* p;
     };
-    static constexpr int SMEM_BYTES = 12;
+    static constexpr int SMEM_BYTES = 16; // one 16-byte slot per row (kl, kh, p, unused)
+    static constexpr int SWZ_BITS = 3;
     __device__ __forceinline__ static RowKP load(const Cols& c, size_t g)
     {
-        return RowKP { __ldcg(c.k + g), __ldcg(c.p + g) };
+        const uint64_t k = __ldcg(c.k + g);
+        return RowKP { lo32(k), hi32(k), __ldcg(c.p + g) };
     }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowKP& r)
     {
-        c.k[g] = r.k;
+        c.k[g] = ((uint64_t)r.kh << 32) | r.kl;
         c.p[g] = r.p;
     }
-    __device__ __forceinline__ static RowKP pad(const Cols&) { return RowKP { ~0ull, ~0u }; }
-    __device__ __forceinline__ static void sstore(char* sm, int T, int i, const RowKP& r)
+    __device__ __forceinline__ static RowKP pad(const Cols&) { return RowKP { ~0u, ~0u, ~0u }; }
+    __device__ __forceinline__ static void sstore(char* sm, int, int i, const RowKP& r)
     {
-        reinterpret_cast<uint64_t*>(sm)[i] = r.k;
-        reinterpret_cast<uint32_t*>(sm + 8 * T)[i] = r.p;
+        reinterpret_cast<uint4*>(sm)[i] = make_uint4(r.kl, r.kh, r.p, 0u);
     }
-    __device__ __forceinline__ static RowKP sload(const char* sm, int T, int i)
+    __device__ __forceinline__ static RowKP sload(const char* sm, int, int i)
     {
-        return RowKP { reinterpret_cast<const uint64_t*>(sm)[i], reinterpret_cast<const uint32_t*>(sm + 8 * T)[i] };
+        const uint4 x = reinterpret_cast<const uint4*>(sm)[i];
+        return RowKP { x.x, x.y, x.z };
     }
     __device__ __forceinline__ static uint32_t swap_mask(const RowKP& a, const RowKP& b, uint32_t desc, const Cols&)
     {
-        return gt_mask3(a.p, lo32(a.k), hi32(a.k), b.p, lo32(b.k), hi32(b.k)) ^ desc;
+        return gt_mask3(a.p, a.kl, a.kh, b.p, b.kl, b.kh) ^ desc;
     }
-    __device__ __forceinline__ static RowKP select(bool c, const RowKP& a, const RowKP& b)
+    // exchange a and b where m is all ones, in place
+    __device__ __forceinline__ static void cswap(RowKP& a, RowKP& b, uint32_t m)
     {
-        return RowKP { sel(c, a.k, b.k), sel(c, a.p, b.p) };
+        const uint32_t dl = (a.kl ^ b.kl) & m, dh = (a.kh ^ b.kh) & m, dp = (a.p ^ b.p) & m;
+        a.kl ^= dl;
+        b.kl ^= dl;
+        a.kh ^= dh;
+        b.kh ^= dh;
+        a.p ^= dp;
+        b.p ^= dp;
     }
     __device__ __forceinline__ static bool marked(const RowKP&) { return false; }
 };
@@ -160,46 +169,53 @@ struct RowKP {
 // (u64 key, u32 payload, u8 mark): compaction rows; ordered on (key, payload)
 // with the mark carried, strictly.
 struct RowKPM {
-    uint64_t k;
-    uint32_t p;
-    uint32_t m;
+    uint32_t kl, kh, p, m;
     struct Cols {
         uint64_t* k;
         uint32_t* p;
         uint8_t* m;
     };
-    static constexpr int SMEM_BYTES = 13;
+    static constexpr int SMEM_BYTES = 16; // one 16-byte slot per row (kl, kh, p, m)
+    static constexpr int SWZ_BITS = 3;
     __device__ __forceinline__ static RowKPM load(const Cols& c, size_t g)
     {
-        return RowKPM { __ldcg(c.k + g), __ldcg(c.p + g), (uint32_t)__ldcg(c.m + g) };
+        const uint64_t k = __ldcg(c.k + g);
+        return RowKPM { lo32(k), hi32(k), __ldcg(c.p + g), (uint32_t)__ldcg(c.m + g) };
     }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowKPM& r)
     {
-        c.k[g] = r.k;
+        c.k[g] = ((uint64_t)r.kh << 32) | r.kl;
         c.p[g] = r.p;
         c.m[g] = (uint8_t)r.m;
     }
-    __device__ __forceinline__ static RowKPM pad(const Cols&) { return RowKPM { ~0ull, ~0u, 0u }; }
-    __device__ __forceinline__ static void sstore(char* sm, int T, int i, const RowKPM& r)
+    __device__ __forceinline__ static RowKPM pad(const Cols&) { return RowKPM { ~0u, ~0u, ~0u, 0u }; }
+    __device__ __forceinline__ static void sstore(char* sm, int, int i, const RowKPM& r)
     {
-        reinterpret_cast<uint64_t*>(sm)[i] = r.k;
-        reinterpret_cast<uint32_t*>(sm + 8 * T)[i] = r.p;
-        reinterpret_cast<uint8_t*>(sm + 12 * T)[i] = (uint8_t)r.m;
+        reinterpret_cast<uint4*>(sm)[i] = make_uint4(r.kl, r.kh, r.p, r.m);
     }
-    __device__ __forceinline__ static RowKPM sload(const char* sm, int T, int i)
+    __device__ __forceinline__ static RowKPM sload(const char* sm, int, int i)
     {
-        return RowKPM { reinterpret_cast<const uint64_t*>(sm)[i], reinterpret_cast<const uint32_t*>(sm + 8 * T)[i],
-                        (uint32_t) reinterpret_cast<const uint8_t*>(sm + 12 * T)[i] };
+        const uint4 x = reinterpret_cast<const uint4*>(sm)[i];
+        return RowKPM { x.x, x.y, x.z, x.w };
     }
     __device__ __forceinline__ static uint32_t swap_mask(const RowKPM& a, const RowKPM& b, uint32_t desc, const Cols&)
     {
-        const uint32_t gt = gt_mask3(a.p, lo32(a.k), hi32(a.k), b.p, lo32(b.k), hi32(b.k));
-        const uint32_t lt = gt_mask3(b.p, lo32(b.k), hi32(b.k), a.p, lo32(a.k), hi32(a.k));
+        const uint32_t gt = gt_mask3(a.p, a.kl, a.kh, b.p, b.kl, b.kh);
+        const uint32_t lt = gt_mask3(b.p, b.kl, b.kh, a.p, a.kl, a.kh);
         return desc ? lt : gt;
     }
-    __device__ __forceinline__ static RowKPM select(bool c, const RowKPM& a, const RowKPM& b)
+    __device__ __forceinline__ static void cswap(RowKPM& a, RowKPM& b, uint32_t msk)
     {
-        return RowKPM { sel(c, a.k, b.k), sel(c, a.p, b.p), sel(c, a.m, b.m) };
+        const uint32_t dl = (a.kl ^ b.kl) & msk, dh = (a.kh ^ b.kh) & msk, dp = (a.p ^ b.p) & msk,
+                       dm = (a.m ^ b.m) & msk;
+        a.kl ^= dl;
+        b.kl ^= dl;
+        a.kh ^= dh;
+        b.kh ^= dh;
+        a.p ^= dp;
+        b.p ^= dp;
+        a.m ^= dm;
+        b.m ^= dm;
     }
     __device__ __forceinline__ static bool marked(const RowKPM& r) { return r.m != 0; }
 };
@@ -216,8 +232,12 @@ struct RowRec {
         uint64_t pad[W];
         int mark_bit;
         int mark_inv;
+        int mark_word; // word holding the mark bit (0 unless set)
     };
-    static constexpr int SMEM_BYTES = 8 * W;
+    // smem: words 0 and 1 share a 16-byte slot (W >= 2), word 2 (W == 3) is a
+    // separate 8-byte array; W == 1 uses 8-byte slots
+    static constexpr int SMEM_BYTES = 8 * W + (W == 3 ? 0 : 0);
+    static constexpr int SWZ_BITS = W == 1 ? 4 : 3;
     __device__ __forceinline__ static RowRec load(const Cols& c, size_t g)
     {
         RowRec r;
@@ -242,17 +262,39 @@ struct RowRec {
     }
     __device__ __forceinline__ static void sstore(char* sm, int T, int i, const RowRec& r)
     {
+        if constexpr (W == 1) {
+            reinterpret_cast<uint64_t*>(sm)[i] = r.w[0];
+        } else {
+            reinterpret_cast<ulonglong2*>(sm)[i] = make_ulonglong2(r.w[0], r.w[1]);
 #pragma unroll
-        for (int x = 0; x < W; x++)
-            reinterpret_cast<uint64_t*>(sm + (size_t)8 * T * x)[i] = r.w[x];
+            for (int x = 2; x < W; x++)
+                reinterpret_cast<uint64_t*>(sm + (size_t)16 * T + (size_t)8 * T * (x - 2))[i] = r.w[x];
+        }
     }
     __device__ __forceinline__ static RowRec sload(const char* sm, int T, int i)
     {
         RowRec r;
+        if constexpr (W == 1) {
+            r.w[0] = reinterpret_cast<const uint64_t*>(sm)[i];
+        } else {
+            const ulonglong2 x = reinterpret_cast<const ulonglong2*>(sm)[i];
+            r.w[0] = x.x;
+            r.w[1] = x.y;
 #pragma unroll
-        for (int x = 0; x < W; x++)
-            r.w[x] = reinterpret_cast<const uint64_t*>(sm + (size_t)8 * T * x)[i];
+            for (int y = 2; y < W; y++)
+                r.w[y] = reinterpret_cast<const uint64_t*>(sm + (size_t)16 * T + (size_t)8 * T * (y - 2))[i];
+        }
         return r;
+    }
+    __device__ __forceinline__ static void cswap(RowRec& a, RowRec& b, uint32_t m)
+    {
+        const uint64_t mm = ((uint64_t)m << 32) | m;
+#pragma unroll
+        for (int x = 0; x < W; x++) {
+            const uint64_t d = (a.w[x] ^ b.w[x]) & mm;
+            a.w[x] ^= d;
+            b.w[x] ^= d;
+        }
     }
     __device__ __forceinline__ static uint32_t swap_mask(const RowRec& a, const RowRec& b, uint32_t desc,
                                                          const Cols& c)
@@ -281,7 +323,11 @@ struct RowRec {
     }
     __device__ __forceinline__ static bool marked_c(const RowRec& r, const Cols& c)
     {
-        return (((r.w[0] >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
+        uint64_t w = r.w[0];
+#pragma unroll
+        for (int x = 1; x < W; x++)
+            w = c.mark_word == x ? r.w[x] : w;
+        return (((w >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
     }
 };
 
@@ -309,10 +355,17 @@ struct Tile {
     static constexpr int T = 1 << LOG_T;
     static_assert(LOG_NT >= 5, "at least one warp per CTA");
 
-    // bank-spreading swizzle: XOR bits 5..9 into bits 0..4 (a bijection on
-    // every aligned group of 1024 rows, so it stays inside the tile).  It is
-    // linear over XOR, so swz(a | b) = swz(a) ^ swz(b) for disjoint a, b.
-    __host__ __device__ __forceinline__ static constexpr int swz(int l) { return l ^ ((l >> 5) & 31); }
+    // bank-spreading swizzle of smem slots: XOR SWZ bits taken above the
+    // register window into the low bits, so the lanes of one shared-memory
+    // phase (8 lanes for 16-byte slots, 16 for 8-byte slots) hit distinct
+    // banks in every layout.  The source bits are never modified, so it is a
+    // bijection on the tile; it is linear over XOR, so
+    // swz(a | b) = swz(a) ^ swz(b) for disjoint a, b.
+    template <int SWZ>
+    __host__ __device__ __forceinline__ static constexpr int swz(int l)
+    {
+        return l ^ ((l >> (LOG_E > SWZ ? LOG_E : SWZ)) & ((1 << SWZ) - 1));
+    }
 };
 
 // window start that covers bit p, going down (bitonic) or up (ORCompact)

@@ -246,6 +246,7 @@ extern "C" velo_status velo_filter_groupby(const velo_lineitem* cols, size_t n, 
     rc3.mask[0] = LI_KEYMASK;
     rc3.mark_bit = 63;
     rc3.mark_inv = 1;
+    rc3.mark_word = 0;
 
     // 2. ORCompact over the next_pow2(n) records
     {

@@ -360,6 +360,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     uc.pad[0] = uc.pad[1] = ~0ull;
     uc.mark_bit = 29;
     uc.mark_inv = 0;
+    uc.mark_word = 0;
     // 2. sort the union on (key, tag)
     if (logU > 0) {
         std::vector<NetPass> passes;
@@ -396,6 +397,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     gc.mask[0] = ~0ull;
     gc.mark_bit = 63;
     gc.mark_inv = 1;
+    gc.mark_word = 0;
     k_jseg_summary<<<nts, SEG_THREADS, JSeg::SMEM, st>>>(uc, s.aggs, s.runs);
     k_jseg_carries<<<1, 1024, JoinAgg::V * 1024 * 8 + 2 * 1024 * 4, st>>>(s.aggs, s.runs, nts, s.carry,
                                                                             s.tail_prefix, s.n_groups);
@@ -425,6 +427,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     tc.mask[2] = 0xFFFFFFFF00000000ull;
     tc.mark_bit = 63;
     tc.mark_inv = 1;
+    tc.mark_word = 0;
     const int logT = ilog2_floor(n_top);
     if (logT > 0) {
         std::vector<NetPass> passes;

@@ -85,8 +85,8 @@ inline velo_status launch_count_scan(const typename R::Cols& c, size_t n, int lo
     return VELO_OK;
 }
 
-// (LOG_NT, LOG_E) pairs compiled for the tunable row types; tile 2^11..2^14
-// rows, 256..1024 threads.
+// (LOG_NT, LOG_E) pairs compiled for the tunable row types; tile 2^11..2^13
+// rows, 256..1024 threads (the autotuner's search space).
 #define VELO_FOR_TUNES(X)                                                                                              \
     X(8, 3)                                                                                                            \
     X(9, 2)                                                                                                            \
@@ -96,10 +96,9 @@ inline velo_status launch_count_scan(const typename R::Cols& c, size_t n, int lo
     X(10, 2)                                                                                                           \
     X(8, 5)                                                                                                            \
     X(9, 4)                                                                                                            \
-    X(10, 3)                                                                                                           \
-    X(10, 4)
+    X(10, 3)
 
-// the same grid without 2^14-row tiles (compaction rows + prefix exceed smem)
+// the same grid for compaction rows
 #define VELO_FOR_TUNES_COMPACT(X)                                                                                      \
     X(8, 3)                                                                                                            \
     X(9, 2)                                                                                                            \

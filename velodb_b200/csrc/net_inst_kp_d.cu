@@ -2,4 +2,3 @@
 #include "net_impl.cuh"
 
 VELO_INSTANTIATE_NET(velo::RowKP, 10, 3)
-VELO_INSTANTIATE_NET(velo::RowKP, 10, 4)

@@ -92,7 +92,7 @@ extern "C" velo_status velo_osort_kp(uint64_t* d_keys, uint32_t* d_payload, size
     if (capacity < np)
         return einval("velo_osort_kp: capacity must be >= next_pow2(n)");
     int log_nt, log_e;
-    velo_status rc = resolve_tune(tune, 9, 4, &log_nt, &log_e);
+    velo_status rc = resolve_tune(tune, 8, 4, &log_nt, &log_e);
     if (rc != VELO_OK)
         return rc;
     if (np == 1)

@@ -55,7 +55,7 @@ template <int W, int KW, bool S>
 struct MarkAt<RowRec<W, KW, S>> {
     __device__ __forceinline__ static bool get(const typename RowRec<W, KW, S>::Cols& c, size_t g)
     {
-        return (((__ldcg(c.w[0] + g) >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
+        return (((__ldcg(c.w[c.mark_word] + g) >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
     }
 };
 
@@ -147,24 +147,40 @@ struct Net {
         return (tid & ((1 << s) - 1)) | ((tid >> s) << (s + LOG_E));
     }
 
-    // re-layout the tile from layout `from` to layout `to` through smem; the
-    // slot of register e is swz(tp | e<<s) = swz(tp) ^ swz(e<<s)
+    static constexpr int SWZ = R::SWZ_BITS;
+
+    // smem slots of the E registers in layout s: swz(tp | e<<s) =
+    // swz(tp) ^ swz(e<<s), and swz(e<<s) is the XOR of the basis values
+    // swz(1 << (s+j)) over the set bits j of e (one XOR per register)
+    __device__ __forceinline__ static void slots(int s, int (&slot)[E])
+    {
+        int basis[LOG_E > 0 ? LOG_E : 1];
+#pragma unroll
+        for (int j = 0; j < LOG_E; j++)
+            basis[j] = TL::template swz<SWZ>(1 << (s + j));
+        slot[0] = TL::template swz<SWZ>(tidpart(s));
+#pragma unroll
+        for (int e = 1; e < E; e++) {
+            const int low = e & (-e); // lowest set bit of e
+            const int j = low == 1 ? 0 : low == 2 ? 1 : low == 4 ? 2 : low == 8 ? 3 : 4;
+            slot[e] = slot[e & (e - 1)] ^ basis[j];
+        }
+    }
+
+    // re-layout the tile from layout `from` to layout `to` through smem
     __device__ __forceinline__ static void transpose(R (&v)[E], int from, int to, char* sm)
     {
+        int slot[E];
         __syncthreads();
-        {
-            const int base = TL::swz(tidpart(from));
+        slots(from, slot);
 #pragma unroll
-            for (int e = 0; e < E; e++)
-                R::sstore(sm, T, base ^ TL::swz(e << from), v[e]);
-        }
+        for (int e = 0; e < E; e++)
+            R::sstore(sm, T, slot[e], v[e]);
         __syncthreads();
-        {
-            const int base = TL::swz(tidpart(to));
+        slots(to, slot);
 #pragma unroll
-            for (int e = 0; e < E; e++)
-                v[e] = R::sload(sm, T, base ^ TL::swz(e << to));
-        }
+        for (int e = 0; e < E; e++)
+            v[e] = R::sload(sm, T, slot[e]);
     }
 
     // ---- bitonic compare-exchange on register bit Q -----------------------
@@ -183,11 +199,7 @@ struct Net {
             uint32_t d = dm;
             if constexpr (PER_E)
                 d = ((e >> dbit) & 1) ? ~0u : 0u;
-            const bool sw = R::swap_mask(v[e], v[e2], d, c) != 0;
-            const R a = R::select(sw, v[e2], v[e]);
-            const R b = R::select(sw, v[e], v[e2]);
-            v[e] = a;
-            v[e2] = b;
+            R::cswap(v[e], v[e2], R::swap_mask(v[e], v[e2], d, c));
         }
     }
 
@@ -243,10 +255,7 @@ struct Net {
                 const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
                 sw = sb != (i >= ((off + left) & (half - 1)));
             }
-            const R a = R::select(sw, v[e2], v[e]);
-            const R bb = R::select(sw, v[e], v[e2]);
-            v[e] = a;
-            v[e2] = bb;
+            R::cswap(v[e], v[e2], sw ? ~0u : 0u);
         }
     }
 
@@ -272,10 +281,7 @@ struct Net {
             const uint64_t i = g - blk;
             const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
             const bool sw = sb != (i >= ((off + left) & (half - 1)));
-            const R a = R::select(sw, v[e2], v[e]);
-            const R bb = R::select(sw, v[e], v[e2]);
-            v[e] = a;
-            v[e2] = bb;
+            R::cswap(v[e], v[e2], sw ? ~0u : 0u);
         }
     }
 

@@ -1,0 +1,798 @@
+// Column operators of the reference's command set and their oblivious
+// replacements:
+//   compat (reference semantics, data-dependent addresses as in the
+//   reference):  OP_PERMUTE, OP_SCATTER, OP_GATHER, OP_COMPARE_EQ,
+//                OP_COMPOSE_POSITION_MAP, OP_ENRICH_POSITIONS
+//   oblivious:   position-map shuffle (device PRF + bitonic network),
+//                oblivious gather (union sort + fill + sort back),
+//                PK-FK equi-join producing (build rowid, probe rowid) pairs
+#include "net_impl.cuh"
+
+namespace velo {
+
+static int type_bytes(uint32_t t)
+{
+    switch (t) {
+    case VELO_BOOLEAN:
+    case VELO_TINYINT:
+        return 1;
+    case VELO_SMALLINT:
+        return 2;
+    case VELO_INTEGER:
+    case VELO_FLOAT:
+    case VELO_DATE:
+        return 4;
+    case VELO_BIGINT:
+    case VELO_DOUBLE:
+    case VELO_VARCHAR:
+        return 8;
+    default:
+        return 0;
+    }
+}
+
+static unsigned grid_for(size_t n)
+{
+    const size_t b = (n + 255) / 256;
+    return (unsigned)(b < 148 * 16 ? (b ? b : 1) : 148 * 16);
+}
+
+#define VELO_GRID_STRIDE(i, n)                                                                                         \
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
+
+// ---------------------------------------------------------------------------
+// compat operators (include/cuda/permute.cuh:24-40, gather.cuh:28-45,
+// scatter.cuh:16-81, compare.cuh:25-91, oblivious_shuffle.cuh:10-34)
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__global__ void k_permute(T* out, const T* in, const int64_t* idx, size_t n)
+{
+    VELO_GRID_STRIDE(i, n)
+    out[i] = in[idx[i]];
+}
+
+template <typename T>
+__global__ void k_gather(T* out, const T* in, const int32_t* idx, const uint8_t* mask, size_t n)
+{
+    VELO_GRID_STRIDE(i, n)
+    {
+        if (mask == nullptr || mask[i] != 0)
+            out[idx[i]] = in[i];
+    }
+}
+
+template <typename T>
+__global__ void k_compare_eq(const T* l, const T* r, uint8_t* out, size_t n)
+{
+    VELO_GRID_STRIDE(i, n)
+    out[i] = (l[i] == r[i]) ? 1 : 0;
+}
+
+__global__ void k_fill_u8(uint8_t* out, uint8_t v, size_t n)
+{
+    VELO_GRID_STRIDE(i, n)
+    out[i] = v;
+}
+
+__global__ void k_compose(const uint32_t* old_map, const uint32_t* sigma, uint32_t* new_map, size_t n)
+{
+    VELO_GRID_STRIDE(i, n)
+    new_map[i] = old_map[sigma[i]];
+}
+
+// stable scatter: per-tile kept counts, their scan, then ranks
+constexpr int SC_LT = 11;
+__global__ void __launch_bounds__(256) k_scatter_count(const uint8_t* mask, size_t n, uint32_t* counts)
+{
+    __shared__ uint32_t tmp[33];
+    const size_t base = (size_t)blockIdx.x << SC_LT;
+    uint32_t c = 0;
+    for (int i = threadIdx.x; i < (1 << SC_LT); i += blockDim.x) {
+        const size_t g = base + i;
+        c += (g < n && mask[g] != 0) ? 1u : 0u;
+    }
+    uint32_t total;
+    block_exclusive_scan(c, tmp, &total);
+    if (threadIdx.x == 0)
+        counts[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(256) k_scatter_write(const uint8_t* mask, size_t n, const uint32_t* prefix,
+                                                       int32_t* out_idx)
+{
+    __shared__ uint32_t tmp[33];
+    // each thread owns 8 consecutive rows of the 2048-row tile
+    const size_t base = ((size_t)blockIdx.x << SC_LT) + (size_t)threadIdx.x * 8;
+    uint32_t m[8], c = 0;
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const size_t g = base + r;
+        m[r] = (g < n && mask[g] != 0) ? 1u : 0u;
+        c += m[r];
+    }
+    uint32_t total;
+    uint32_t rank = prefix[blockIdx.x] + block_exclusive_scan(c, tmp, &total);
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        const size_t g = base + r;
+        if (m[r])
+            out_idx[g] = (int32_t)rank;
+        rank += m[r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), counter-based PRF used
+// to draw the shuffle keys on the device
+// ---------------------------------------------------------------------------
+
+__host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo)
+{
+    const uint64_t p = (uint64_t)a * b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+}
+
+__host__ __device__ __forceinline__ uint64_t philox_u64(uint64_t idx, uint64_t counter, uint64_t key)
+{
+    uint32_t c0 = (uint32_t)idx, c1 = (uint32_t)(idx >> 32), c2 = (uint32_t)counter, c3 = (uint32_t)(counter >> 32);
+    uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(0xD2511F53u, c0, hi0, lo0);
+        mulhilo32(0xCD9E8D57u, c2, hi1, lo1);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return ((uint64_t)c1 << 32) | c0;
+}
+
+__global__ void k_shuffle_pack(const uint32_t* map, size_t n, size_t np, uint64_t counter, uint64_t key, uint64_t* k,
+                               uint32_t* p)
+{
+    VELO_GRID_STRIDE(i, np)
+    {
+        k[i] = i < n ? philox_u64(i, counter, key) : ~0ull;
+        p[i] = i < n ? map[i] : ~0u;
+    }
+}
+
+__global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, size_t n)
+{
+    VELO_GRID_STRIDE(i, n)
+    dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// forward fill over a key-sorted record array: every row receives the
+// (key, value) of the last "source" row at or before it (segmented scan in
+// three passes; addresses never depend on the data)
+// ---------------------------------------------------------------------------
+
+struct FillCarry {
+    uint64_t key;
+    uint64_t val;
+    uint32_t has;
+    uint32_t valid;
+};
+
+__device__ __forceinline__ FillCarry fill_combine(const FillCarry& l, const FillCarry& r)
+{
+    return r.has ? r : l;
+}
+
+constexpr int FL_TS = 2048, FL_THREADS = 256, FL_RPT = FL_TS / FL_THREADS;
+
+// Src: static FillCarry src(w0, w1, w2) -- has = row is a source
+//      static void apply(uint64_t& w0, uint64_t& w1, uint64_t& w2, const FillCarry& last)
+template <class F>
+__global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, const uint64_t* w1, const uint64_t* w2,
+                                                         FillCarry* tile_last)
+{
+    __shared__ FillCarry sm[FL_THREADS];
+    __shared__ int idx[FL_THREADS];
+    const size_t base = (size_t)blockIdx.x * FL_TS;
+    FillCarry c { 0, 0, 0, 0 };
+    int last = -1;
+    for (int i = threadIdx.x; i < FL_TS; i += FL_THREADS) {
+        const size_t g = base + i;
+        const FillCarry d = F::src(w0[g], w1[g], w2[g]);
+        c = fill_combine(c, d);
+        last = d.has ? i : last;
+    }
+    sm[threadIdx.x] = c;
+    idx[threadIdx.x] = last;
+    __syncthreads();
+    for (int off = FL_THREADS / 2; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off) {
+            const int x = idx[threadIdx.x], y = idx[threadIdx.x + off];
+            const bool take_y = y > x;
+            sm[threadIdx.x] = take_y ? sm[threadIdx.x + off] : sm[threadIdx.x];
+            idx[threadIdx.x] = take_y ? y : x;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        tile_last[blockIdx.x] = sm[0];
+}
+
+__global__ void __launch_bounds__(1024) k_fill_scan(const FillCarry* tile_last, int ntiles, FillCarry* carry)
+{
+    __shared__ FillCarry sm[1024];
+    const int per = (ntiles + 1023) / 1024;
+    const int t0 = threadIdx.x * per, t1 = min(ntiles, t0 + per);
+    FillCarry c { 0, 0, 0, 0 };
+    for (int t = t0; t < t1; t++)
+        c = fill_combine(c, tile_last[t]);
+    sm[threadIdx.x] = c;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const FillCarry prev = (int)threadIdx.x >= off ? sm[threadIdx.x - off] : FillCarry { 0, 0, 0, 0 };
+        __syncthreads();
+        sm[threadIdx.x] = fill_combine(prev, sm[threadIdx.x]);
+        __syncthreads();
+    }
+    FillCarry run = threadIdx.x > 0 ? sm[threadIdx.x - 1] : FillCarry { 0, 0, 0, 0 };
+    for (int t = t0; t < t1; t++) {
+        carry[t] = run;
+        run = fill_combine(run, tile_last[t]);
+    }
+}
+
+template <class F>
+__global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_t* w1, uint64_t* w2,
+                                                           const FillCarry* carry, unsigned long long* d_stat)
+{
+    __shared__ FillCarry st[FL_THREADS];
+    __shared__ uint32_t tmp[33];
+    const size_t base = (size_t)blockIdx.x * FL_TS + (size_t)threadIdx.x * FL_RPT;
+    uint64_t a[FL_RPT], b[FL_RPT], c[FL_RPT];
+    FillCarry mine { 0, 0, 0, 0 };
+#pragma unroll
+    for (int r = 0; r < FL_RPT; r++) {
+        a[r] = w0[base + r];
+        b[r] = w1[base + r];
+        c[r] = w2[base + r];
+        mine = fill_combine(mine, F::src(a[r], b[r], c[r]));
+    }
+    st[threadIdx.x] = mine;
+    __syncthreads();
+    for (int off = 1; off < FL_THREADS; off <<= 1) {
+        const FillCarry prev = (int)threadIdx.x >= off ? st[threadIdx.x - off] : FillCarry { 0, 0, 0, 0 };
+        __syncthreads();
+        st[threadIdx.x] = fill_combine(prev, st[threadIdx.x]);
+        __syncthreads();
+    }
+    FillCarry run = fill_combine(carry[blockIdx.x], threadIdx.x > 0 ? st[threadIdx.x - 1] : FillCarry { 0, 0, 0, 0 });
+    uint32_t stat = 0;
+#pragma unroll
+    for (int r = 0; r < FL_RPT; r++) {
+        stat += F::dup(a[r], b[r], c[r], run) ? 1u : 0u;
+        run = fill_combine(run, F::src(a[r], b[r], c[r]));
+        F::apply(a[r], b[r], c[r], run);
+        w0[base + r] = a[r];
+        w1[base + r] = b[r];
+        w2[base + r] = c[r];
+    }
+    // one counter update per CTA at a fixed address
+    uint32_t total;
+    block_exclusive_scan(stat, tmp, &total);
+    if (threadIdx.x == 0 && d_stat)
+        atomicAdd(d_stat, (unsigned long long)total);
+}
+
+template <class F>
+static velo_status run_fill(uint64_t* w0, uint64_t* w1, uint64_t* w2, size_t rows, FillCarry* tl, FillCarry* carry,
+                            unsigned long long* d_stat, cudaStream_t st)
+{
+    const int nt = (int)(rows / FL_TS);
+    k_fill_sum<F><<<nt, FL_THREADS, 0, st>>>(w0, w1, w2, tl);
+    k_fill_scan<<<1, 1024, 0, st>>>(tl, nt, carry);
+    k_fill_apply<F><<<nt, FL_THREADS, 0, st>>>(w0, w1, w2, carry, d_stat);
+    VELO_CUDA_TRY(cudaGetLastError(), "fill launch");
+    return VELO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// oblivious gather: out[j] = table[rid[j]]
+// union row layout (3 words):
+//   table row i : w0 = i << 32 | tag 0      w1 = table[i]   w2 = 0
+//   request j   : w0 = rid << 32 | tag 1    w1 = 0          w2 = j
+// sort 1 on (index, tag); fill gives each request the value of its table
+// row; the requests' w0 becomes (0, j), every other row (1, ...); sort 2 on
+// w0 puts the requests first in request order.
+// ---------------------------------------------------------------------------
+
+struct GatherFill {
+    __device__ __forceinline__ static FillCarry src(uint64_t a, uint64_t b, uint64_t)
+    {
+        const bool table = ((a >> 31) & 1ull) == 0 && a != ~0ull;
+        return FillCarry { a >> 32, b, table ? 1u : 0u, 1u };
+    }
+    __device__ __forceinline__ static bool dup(uint64_t, uint64_t, uint64_t, const FillCarry&) { return false; }
+    __device__ __forceinline__ static void apply(uint64_t& a, uint64_t& b, uint64_t& c, const FillCarry& last)
+    {
+        const bool req = ((a >> 31) & 1ull) == 1 && a != ~0ull;
+        const bool hit = req & (last.has != 0) & (last.key == (a >> 32));
+        b = req ? (hit ? last.val : 0ull) : b;
+        a = req ? (c & 0xFFFFFFFFull) : (1ull << 63);
+    }
+};
+
+__global__ void k_ogather_pack(const uint64_t* table, size_t tn, const uint32_t* rids, size_t rn, size_t rows,
+                               uint64_t* w0, uint64_t* w1, uint64_t* w2)
+{
+    VELO_GRID_STRIDE(g, rows)
+    {
+        uint64_t a = ~0ull, b = ~0ull, c = ~0ull;
+        if (g < tn) {
+            a = (uint64_t)g << 32;
+            b = table[g];
+            c = 0;
+        } else if (g < tn + rn) {
+            const size_t j = g - tn;
+            a = ((uint64_t)rids[j] << 32) | (1ull << 31);
+            b = 0;
+            c = j;
+        }
+        w0[g] = a;
+        w1[g] = b;
+        w2[g] = c;
+    }
+}
+
+__global__ void k_ogather_out(const uint64_t* w1, size_t rn, uint64_t* out)
+{
+    VELO_GRID_STRIDE(j, rn)
+    out[j] = w1[j];
+}
+
+// ---------------------------------------------------------------------------
+// oblivious PK-FK join producing rowid pairs
+// union row layout (3 words):
+//   w0 = key (order-preserving u64)
+//   w1 = [63] tag (0 build, 1 probe) | [62] row valid | [61] joined | [60:0] rowid
+//   w2 = build rowid of a joined probe row
+// ---------------------------------------------------------------------------
+
+constexpr uint64_t OJ_TAG = 1ull << 63, OJ_VALID = 1ull << 62, OJ_JOINED = 1ull << 61;
+constexpr uint64_t OJ_ROWID = (1ull << 61) - 1;
+
+struct JoinFill {
+    __device__ __forceinline__ static bool is_pad(uint64_t a, uint64_t b) { return a == ~0ull && b == ~0ull; }
+    __device__ __forceinline__ static FillCarry src(uint64_t a, uint64_t b, uint64_t)
+    {
+        const bool build = (b & OJ_TAG) == 0 && !is_pad(a, b);
+        return FillCarry { a, b & OJ_ROWID, build ? 1u : 0u, (b & OJ_VALID) ? 1u : 0u };
+    }
+    // a build row whose key equals the preceding build row's key
+    __device__ __forceinline__ static bool dup(uint64_t a, uint64_t b, uint64_t, const FillCarry& last)
+    {
+        const bool build = (b & OJ_TAG) == 0 && !is_pad(a, b);
+        return build & (last.has != 0) & (last.key == a);
+    }
+    __device__ __forceinline__ static void apply(uint64_t& a, uint64_t& b, uint64_t& c, const FillCarry& last)
+    {
+        const bool probe = (b & OJ_TAG) != 0 && !is_pad(a, b);
+        const bool joined = probe & ((b & OJ_VALID) != 0) & (last.has != 0) & (last.valid != 0) & (last.key == a);
+        b = (b & ~OJ_JOINED) | (joined ? OJ_JOINED : 0ull);
+        c = joined ? last.val : ~0ull;
+    }
+};
+
+__global__ void k_ojoin_pack(const void* bk, const uint8_t* bm, size_t bn, const void* pk, const uint8_t* pm, size_t pn,
+                             int key64, size_t rows, uint64_t* w0, uint64_t* w1, uint64_t* w2)
+{
+    VELO_GRID_STRIDE(g, rows)
+    {
+        uint64_t a = ~0ull, b = ~0ull, c = ~0ull;
+        if (g < bn + pn) {
+            const bool build = g < bn;
+            const size_t j = build ? g : g - bn;
+            const void* keys = build ? bk : pk;
+            const uint8_t* mask = build ? bm : pm;
+            const uint64_t key = key64 ? ((uint64_t) static_cast<const int64_t*>(keys)[j] ^ 0x8000000000000000ull)
+                                       : (uint64_t)((uint32_t) static_cast<const int32_t*>(keys)[j] ^ 0x80000000u);
+            const bool valid = mask == nullptr || mask[j] != 0;
+            a = key;
+            b = (build ? 0ull : OJ_TAG) | (valid ? OJ_VALID : 0ull) | ((uint64_t)j & OJ_ROWID);
+            c = ~0ull;
+        }
+        w0[g] = a;
+        w1[g] = b;
+        w2[g] = c;
+    }
+}
+
+__global__ void k_ojoin_out(const uint64_t* w1, const uint64_t* w2, size_t pn, int64_t* ob, int64_t* op)
+{
+    VELO_GRID_STRIDE(i, pn)
+    {
+        const uint64_t b = w1[i];
+        const bool j = (b & OJ_JOINED) != 0 && b != ~0ull;
+        ob[i] = j ? (int64_t)w2[i] : -1;
+        op[i] = j ? (int64_t)(b & OJ_ROWID) : -1;
+    }
+}
+
+__global__ void k_zero_u64(unsigned long long* p, int n)
+{
+    if ((int)threadIdx.x < n)
+        p[threadIdx.x] = 0;
+}
+
+__global__ void k_join_counts(const uint64_t* n_joined, const unsigned long long* dups, uint64_t* d_counts)
+{
+    d_counts[0] = *n_joined;
+    d_counts[1] = *dups;
+}
+
+using Rec3 = RowRec<3, 1, false>;
+using Rec3K2 = RowRec<3, 2, false>;
+constexpr int OP_LOG_NT = 8, OP_LOG_E = 4, OP_LT = OP_LOG_NT + OP_LOG_E;
+constexpr int OP_LMAX = OP_LT - 5 < 8 ? OP_LT - 5 : 8;
+
+// scratch of the union-sort operators: 3 words x rows + fill carries + compaction
+static size_t union_rows(size_t n)
+{
+    size_t r = next_pow2(n);
+    const size_t floor_rows = (size_t)1 << OP_LT;
+    return r < floor_rows ? floor_rows : r;
+}
+
+struct UnionScratch {
+    uint64_t* w[3];
+    FillCarry* tl;
+    FillCarry* carry;
+    uint32_t* counts;
+    uint32_t* prefix;
+    uint64_t* n_marked;
+    unsigned long long* stat;
+    size_t bytes;
+};
+
+static UnionScratch union_layout(char* base, size_t rows)
+{
+    UnionScratch s {};
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        char* p = base ? base + off : nullptr;
+        off += align_up(b, 256);
+        return p;
+    };
+    for (int i = 0; i < 3; i++)
+        s.w[i] = reinterpret_cast<uint64_t*>(take(rows * 8));
+    const size_t nft = rows / FL_TS, nct = rows >> OP_LT;
+    s.tl = reinterpret_cast<FillCarry*>(take(nft * sizeof(FillCarry)));
+    s.carry = reinterpret_cast<FillCarry*>(take(nft * sizeof(FillCarry)));
+    s.counts = reinterpret_cast<uint32_t*>(take(nct * 4));
+    s.prefix = reinterpret_cast<uint32_t*>(take((nct + 1) * 4));
+    s.n_marked = reinterpret_cast<uint64_t*>(take(8));
+    s.stat = reinterpret_cast<unsigned long long*>(take(8));
+    s.bytes = off;
+    return s;
+}
+
+} // namespace velo
+
+using namespace velo;
+
+// ---- compat entry points ---------------------------------------------------
+
+extern "C" velo_status velo_permute(void* d_out, const void* d_in, const int64_t* d_indices, size_t n, uint32_t type,
+                                    void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n == 0)
+        return VELO_OK;
+    if (!d_out || !d_in || !d_indices)
+        return einval("velo_permute: null buffer");
+    switch (type_bytes(type)) {
+    case 1:
+        k_permute<uint8_t><<<grid_for(n), 256, 0, st>>>((uint8_t*)d_out, (const uint8_t*)d_in, d_indices, n);
+        break;
+    case 2:
+        k_permute<uint16_t><<<grid_for(n), 256, 0, st>>>((uint16_t*)d_out, (const uint16_t*)d_in, d_indices, n);
+        break;
+    case 4:
+        k_permute<uint32_t><<<grid_for(n), 256, 0, st>>>((uint32_t*)d_out, (const uint32_t*)d_in, d_indices, n);
+        break;
+    case 8:
+        k_permute<uint64_t><<<grid_for(n), 256, 0, st>>>((uint64_t*)d_out, (const uint64_t*)d_in, d_indices, n);
+        break;
+    default:
+        return einval("velo_permute: unsupported type");
+    }
+    VELO_CUDA_TRY(cudaGetLastError(), "permute launch");
+    return VELO_OK;
+}
+
+extern "C" velo_status velo_gather(void* d_out, const void* d_in, const int32_t* d_indices, const uint8_t* d_mask,
+                                   size_t n, uint32_t type, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n == 0)
+        return VELO_OK;
+    if (!d_out || !d_in || !d_indices)
+        return einval("velo_gather: null buffer");
+    switch (type_bytes(type)) {
+    case 1:
+        k_gather<uint8_t><<<grid_for(n), 256, 0, st>>>((uint8_t*)d_out, (const uint8_t*)d_in, d_indices, d_mask, n);
+        break;
+    case 2:
+        k_gather<uint16_t><<<grid_for(n), 256, 0, st>>>((uint16_t*)d_out, (const uint16_t*)d_in, d_indices, d_mask, n);
+        break;
+    case 4:
+        k_gather<uint32_t><<<grid_for(n), 256, 0, st>>>((uint32_t*)d_out, (const uint32_t*)d_in, d_indices, d_mask, n);
+        break;
+    case 8:
+        k_gather<uint64_t><<<grid_for(n), 256, 0, st>>>((uint64_t*)d_out, (const uint64_t*)d_in, d_indices, d_mask, n);
+        break;
+    default:
+        return einval("velo_gather: unsupported type");
+    }
+    VELO_CUDA_TRY(cudaGetLastError(), "gather launch");
+    return VELO_OK;
+}
+
+extern "C" size_t velo_scatter_scratch_bytes(size_t n)
+{
+    const size_t nt = (n + (1 << SC_LT) - 1) >> SC_LT;
+    return align_up((nt ? nt : 1) * 4, 256) + align_up(((nt ? nt : 1) + 1) * 4, 256);
+}
+
+extern "C" velo_status velo_scatter(const uint8_t* d_mask, size_t n, int32_t* d_out_indices, uint64_t* d_count,
+                                    void* d_scratch, size_t scratch_bytes, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_count)
+        return einval("velo_scatter: null count");
+    if (n == 0) {
+        VELO_CUDA_TRY(cudaMemsetAsync(d_count, 0, 8, st), "cudaMemsetAsync");
+        return VELO_OK;
+    }
+    if (!d_mask || !d_out_indices)
+        return einval("velo_scatter: null buffer");
+    if (!d_scratch || scratch_bytes < velo_scatter_scratch_bytes(n)) {
+        set_error("velo_scatter: scratch must hold velo_scatter_scratch_bytes(n) bytes");
+        return VELO_ENOMEM;
+    }
+    const size_t nt = (n + (1 << SC_LT) - 1) >> SC_LT;
+    uint32_t* counts = static_cast<uint32_t*>(d_scratch);
+    uint32_t* prefix = reinterpret_cast<uint32_t*>(static_cast<char*>(d_scratch) + align_up(nt * 4, 256));
+    k_scatter_count<<<(unsigned)nt, 256, 0, st>>>(d_mask, n, counts);
+    k_scan_tiles<<<1, 1024, 0, st>>>(counts, (int)nt, prefix, d_count);
+    k_scatter_write<<<(unsigned)nt, 256, 0, st>>>(d_mask, n, prefix, d_out_indices);
+    VELO_CUDA_TRY(cudaGetLastError(), "scatter launch");
+    return VELO_OK;
+}
+
+extern "C" velo_status velo_compare_eq(const void* d_left, const void* d_right, uint8_t* d_out_mask, size_t n,
+                                       uint32_t type, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n == 0)
+        return VELO_OK;
+    if (!d_left || !d_right || !d_out_mask)
+        return einval("velo_compare_eq: null buffer");
+    const unsigned g = grid_for(n);
+    switch (type) {
+    case VELO_TINYINT:
+        k_compare_eq<int8_t><<<g, 256, 0, st>>>((const int8_t*)d_left, (const int8_t*)d_right, d_out_mask, n);
+        break;
+    case VELO_SMALLINT:
+        k_compare_eq<int16_t><<<g, 256, 0, st>>>((const int16_t*)d_left, (const int16_t*)d_right, d_out_mask, n);
+        break;
+    case VELO_INTEGER:
+    case VELO_DATE:
+        k_compare_eq<int32_t><<<g, 256, 0, st>>>((const int32_t*)d_left, (const int32_t*)d_right, d_out_mask, n);
+        break;
+    case VELO_BIGINT:
+        k_compare_eq<int64_t><<<g, 256, 0, st>>>((const int64_t*)d_left, (const int64_t*)d_right, d_out_mask, n);
+        break;
+    case VELO_FLOAT:
+        k_compare_eq<float><<<g, 256, 0, st>>>((const float*)d_left, (const float*)d_right, d_out_mask, n);
+        break;
+    case VELO_DOUBLE:
+        k_compare_eq<double><<<g, 256, 0, st>>>((const double*)d_left, (const double*)d_right, d_out_mask, n);
+        break;
+    default:
+        // unsupported types compare as all-false, as the reference does
+        k_fill_u8<<<g, 256, 0, st>>>(d_out_mask, 0, n);
+        break;
+    }
+    VELO_CUDA_TRY(cudaGetLastError(), "compare launch");
+    return VELO_OK;
+}
+
+extern "C" velo_status velo_compose_position_map(const uint32_t* d_old, const uint32_t* d_sigma, uint32_t* d_new,
+                                                 size_t n, void* stream)
+{
+    if (n == 0)
+        return VELO_OK;
+    if (!d_old || !d_sigma || !d_new)
+        return einval("velo_compose_position_map: null buffer");
+    k_compose<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d_old, d_sigma, d_new, n);
+    VELO_CUDA_TRY(cudaGetLastError(), "compose launch");
+    return VELO_OK;
+}
+
+extern "C" velo_status velo_enrich_positions(const uint32_t* d_record_ids, const uint32_t* d_map, uint32_t* d_out,
+                                             size_t n, void* stream)
+{
+    if (n == 0)
+        return VELO_OK;
+    if (!d_record_ids || !d_map || !d_out)
+        return einval("velo_enrich_positions: null buffer");
+    // pos[i] = map[rid[i]]: the same gather as a composition
+    k_compose<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d_map, d_record_ids, d_out, n);
+    VELO_CUDA_TRY(cudaGetLastError(), "enrich launch");
+    return VELO_OK;
+}
+
+// ---- oblivious shuffle ---------------------------------------------------------
+
+extern "C" size_t velo_oshuffle_scratch_bytes(size_t n)
+{
+    const size_t np = next_pow2(n);
+    return align_up(np * 8, 256) + align_up(np * 4, 256);
+}
+
+extern "C" velo_status velo_oshuffle_position_map(uint32_t* d_map, size_t n, uint64_t key, uint64_t counter,
+                                                  void* d_scratch, size_t scratch_bytes, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n == 0)
+        return VELO_OK;
+    if (!d_map)
+        return einval("velo_oshuffle_position_map: null map");
+    const size_t np = next_pow2(n);
+    if (np > ((size_t)1 << MAX_LOGN))
+        return einval("velo_oshuffle_position_map: n too large");
+    if (!d_scratch || scratch_bytes < velo_oshuffle_scratch_bytes(n)) {
+        set_error("velo_oshuffle_position_map: scratch must hold velo_oshuffle_scratch_bytes(n) bytes");
+        return VELO_ENOMEM;
+    }
+    uint64_t* k = static_cast<uint64_t*>(d_scratch);
+    uint32_t* p = reinterpret_cast<uint32_t*>(static_cast<char*>(d_scratch) + align_up(np * 8, 256));
+    k_shuffle_pack<<<grid_for(np), 256, 0, st>>>(d_map, n, np, counter, key, k, p);
+    VELO_CUDA_TRY(cudaGetLastError(), "shuffle pack launch");
+    velo_status rc = velo_osort_kp(k, p, np, np, nullptr, stream);
+    if (rc != VELO_OK)
+        return rc;
+    k_copy_u32<<<grid_for(n), 256, 0, st>>>(d_map, p, n);
+    VELO_CUDA_TRY(cudaGetLastError(), "shuffle copy launch");
+    return VELO_OK;
+}
+
+// ---- oblivious gather ----------------------------------------------------------
+
+extern "C" size_t velo_ogather_scratch_bytes(size_t table_n, size_t n_req)
+{
+    return union_layout(nullptr, union_rows(table_n + n_req)).bytes;
+}
+
+extern "C" velo_status velo_ogather_u64(const uint64_t* d_table, size_t table_n, const uint32_t* d_rids, size_t n_req,
+                                        uint64_t* d_out, void* d_scratch, size_t scratch_bytes, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n_req == 0)
+        return VELO_OK;
+    if (!d_table || !d_rids || !d_out)
+        return einval("velo_ogather_u64: null buffer");
+    if (table_n >= 0xFFFFFFFFull || n_req >= 0xFFFFFFFFull)
+        return einval("velo_ogather_u64: sizes must fit 32 bits");
+    const size_t rows = union_rows(table_n + n_req);
+    const int logR = ilog2_floor(rows);
+    if (logR > MAX_LOGN)
+        return einval("velo_ogather_u64: too large");
+    UnionScratch s = union_layout(static_cast<char*>(d_scratch), rows);
+    if (!d_scratch || scratch_bytes < s.bytes) {
+        set_error("velo_ogather_u64: scratch must hold velo_ogather_scratch_bytes() bytes");
+        return VELO_ENOMEM;
+    }
+    k_ogather_pack<<<grid_for(rows), 256, 0, st>>>(d_table, table_n, d_rids, n_req, rows, s.w[0], s.w[1], s.w[2]);
+    VELO_CUDA_TRY(cudaGetLastError(), "ogather pack launch");
+    Rec3::Cols c;
+    for (int i = 0; i < 3; i++) {
+        c.w[i] = s.w[i];
+        c.pad[i] = ~0ull;
+    }
+    c.mask[0] = 0xFFFFFFFF80000000ull;
+    c.mark_bit = 0;
+    c.mark_inv = 0;
+    c.mark_word = 0;
+    std::vector<NetPass> passes;
+    plan_sort(logR, OP_LT, OP_LMAX, passes);
+    velo_status rc = launch_net<Rec3, OP_LOG_NT, OP_LOG_E>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
+    if (rc != VELO_OK)
+        return rc;
+    rc = run_fill<GatherFill>(s.w[0], s.w[1], s.w[2], rows, s.tl, s.carry, nullptr, st);
+    if (rc != VELO_OK)
+        return rc;
+    c.mask[0] = ~0ull;
+    rc = launch_net<Rec3, OP_LOG_NT, OP_LOG_E>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
+    if (rc != VELO_OK)
+        return rc;
+    k_ogather_out<<<grid_for(n_req), 256, 0, st>>>(s.w[1], n_req, d_out);
+    VELO_CUDA_TRY(cudaGetLastError(), "ogather out launch");
+    return VELO_OK;
+}
+
+// ---- oblivious PK-FK join ------------------------------------------------------
+
+extern "C" size_t velo_ojoin_scratch_bytes(size_t build_n, size_t probe_n)
+{
+    return union_layout(nullptr, union_rows(build_n + probe_n)).bytes;
+}
+
+extern "C" velo_status velo_ojoin_pkfk(const void* d_build_keys, const uint8_t* d_build_mask, size_t build_n,
+                                       const void* d_probe_keys, const uint8_t* d_probe_mask, size_t probe_n,
+                                       uint32_t key_type, int64_t* d_out_build_rowid, int64_t* d_out_probe_rowid,
+                                       uint64_t* d_counts, void* d_scratch, size_t scratch_bytes, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_counts)
+        return einval("velo_ojoin_pkfk: null counts");
+    if (key_type != VELO_INTEGER && key_type != VELO_BIGINT)
+        return einval("velo_ojoin_pkfk: join keys must be INTEGER or BIGINT");
+    if (probe_n == 0 || build_n == 0) {
+        VELO_CUDA_TRY(cudaMemsetAsync(d_counts, 0, 16, st), "cudaMemsetAsync");
+        if (probe_n) {
+            VELO_CUDA_TRY(cudaMemsetAsync(d_out_build_rowid, 0xFF, probe_n * 8, st), "cudaMemsetAsync");
+            VELO_CUDA_TRY(cudaMemsetAsync(d_out_probe_rowid, 0xFF, probe_n * 8, st), "cudaMemsetAsync");
+        }
+        return VELO_OK;
+    }
+    if (!d_build_keys || !d_probe_keys || !d_out_build_rowid || !d_out_probe_rowid)
+        return einval("velo_ojoin_pkfk: null buffer");
+    const size_t rows = union_rows(build_n + probe_n);
+    const int logR = ilog2_floor(rows);
+    if (logR > MAX_LOGN)
+        return einval("velo_ojoin_pkfk: too large");
+    UnionScratch s = union_layout(static_cast<char*>(d_scratch), rows);
+    if (!d_scratch || scratch_bytes < s.bytes) {
+        set_error("velo_ojoin_pkfk: scratch must hold velo_ojoin_scratch_bytes() bytes");
+        return VELO_ENOMEM;
+    }
+    k_zero_u64<<<1, 32, 0, st>>>(s.stat, 1);
+    k_ojoin_pack<<<grid_for(rows), 256, 0, st>>>(d_build_keys, d_build_mask, build_n, d_probe_keys, d_probe_mask,
+                                                 probe_n, key_type == VELO_BIGINT, rows, s.w[0], s.w[1], s.w[2]);
+    VELO_CUDA_TRY(cudaGetLastError(), "ojoin pack launch");
+    Rec3K2::Cols c;
+    for (int i = 0; i < 3; i++) {
+        c.w[i] = s.w[i];
+        c.pad[i] = ~0ull;
+    }
+    c.mask[0] = ~0ull;
+    c.mask[1] = OJ_TAG;
+    c.mark_word = 1;
+    c.mark_bit = 61;
+    c.mark_inv = 0;
+    std::vector<NetPass> passes;
+    plan_sort(logR, OP_LT, OP_LMAX, passes);
+    velo_status rc = launch_net<Rec3K2, OP_LOG_NT, OP_LOG_E>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
+    if (rc != VELO_OK)
+        return rc;
+    rc = run_fill<JoinFill>(s.w[0], s.w[1], s.w[2], rows, s.tl, s.carry, s.stat, st);
+    if (rc != VELO_OK)
+        return rc;
+    const int nct = (int)(rows >> OP_LT);
+    k_count_marks<Rec3K2><<<nct, 256, 0, st>>>(c, rows, OP_LT, s.counts);
+    k_scan_tiles<<<1, 1024, 0, st>>>(s.counts, nct, s.prefix, s.n_marked);
+    std::vector<NetPass> cp;
+    plan_compact(logR, OP_LT, OP_LMAX, cp);
+    rc = launch_net<Rec3K2, OP_LOG_NT, OP_LOG_E>(c, NetGeom { rows, logR, 0 }, cp, s.prefix, st);
+    if (rc != VELO_OK)
+        return rc;
+    k_ojoin_out<<<grid_for(probe_n), 256, 0, st>>>(s.w[1], s.w[2], probe_n, d_out_build_rowid, d_out_probe_rowid);
+    k_join_counts<<<1, 1, 0, st>>>(s.n_marked, s.stat, d_counts);
+    VELO_CUDA_TRY(cudaGetLastError(), "ojoin out launch");
+    return VELO_OK;
+}

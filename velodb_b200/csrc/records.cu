@@ -23,6 +23,7 @@ static velo_status rec_sort(uint64_t* const* words, uint64_t mask, size_t n, int
     c.mask[0] = mask;
     c.mark_bit = 0;
     c.mark_inv = 0;
+    c.mark_word = 0;
     std::vector<NetPass> passes;
     NetGeom g { n, logN, 0 };
 #define X(a, b)                                                                                                        \

@@ -218,6 +218,7 @@ static velo_status sort_cols_kw(const ColSpec& s, size_t n, int logN, uint64_t* 
         c.pad[i] = ~0ull; // unused: every row (real or pad) is packed explicitly
     c.mark_bit = 0;
     c.mark_inv = 0;
+    c.mark_word = 0;
     if (np > 1) {
         std::vector<NetPass> passes;
         const int lt = LOG_NT + LOG_E;
