@@ -349,6 +349,103 @@ velo_status velo_join_groupby_topk(const velo_join_tables* tables, const velo_jo
                                    int64_t* d_out, uint64_t* d_counts, void* d_scratch, size_t scratch_bytes,
                                    void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Command queue: the boundary the reference's TaskManager /                */
+/* CommandQueueController expose (include/cuda/task_manager.hpp:12-30,      */
+/* include/cuda/commands.hpp:16-201, src/cuda/commands.cpp:47-91)           */
+/* ------------------------------------------------------------------------ */
+
+/* Opcodes: the reference's OpCode values for the operators it has, new
+ * values for the oblivious operators. */
+typedef enum velo_opcode {
+    VELO_OP_NOP = 0,
+    VELO_OP_SCATTER = 1,
+    VELO_OP_GATHER = 2,
+    VELO_OP_SORT = 3, /* multi-column sort, reference contract (velo_sort_columns) */
+    VELO_OP_PERMUTE = 4,
+    VELO_OP_COMPARE_EQ = 10,
+    VELO_OP_COMPOSE_POSITION_MAP = 11,
+    VELO_OP_ENRICH_POSITIONS = 12,
+    VELO_OP_OSORT_KP = 0x100,
+    VELO_OP_OCOMPACT_KPM = 0x101,
+    VELO_OP_OSORT_RECORDS = 0x102,
+    VELO_OP_OJOIN_PKFK = 0x103,
+    VELO_OP_OGATHER = 0x104,
+    VELO_OP_OSHUFFLE = 0x105,
+    VELO_OP_FILTER_GROUPBY = 0x106,
+    VELO_OP_JOIN_GROUPBY_TOPK = 0x107
+} velo_opcode;
+
+/* A command: device pointers and public sizes only (the same arguments as
+ * the direct entry point of each opcode; scratch buffers are caller-owned). */
+typedef struct velo_cmd {
+    uint32_t opcode;
+    uint32_t flags;
+    union {
+        struct { void* d_out; const void* d_in; const int64_t* d_indices; size_t n; uint32_t type; } permute;
+        struct { const uint8_t* d_mask; size_t n; int32_t* d_out_indices; uint64_t* d_count; void* d_scratch;
+                 size_t scratch_bytes; } scatter;
+        struct { void* d_out; const void* d_in; const int32_t* d_indices; const uint8_t* d_mask; size_t n;
+                 uint32_t type; } gather;
+        struct { void* const* d_cols; const uint32_t* types; const uint8_t* ascending; uint32_t n_cols; size_t n;
+                 size_t capacity; int64_t* d_indices; void* d_scratch; size_t scratch_bytes; } sort;
+        struct { const void* d_left; const void* d_right; uint8_t* d_out_mask; size_t n; uint32_t type; } compare_eq;
+        struct { const uint32_t* d_old; const uint32_t* d_sigma; uint32_t* d_new; size_t n; } compose;
+        struct { const uint32_t* d_record_ids; const uint32_t* d_map; uint32_t* d_out; size_t n; } enrich;
+        struct { uint64_t* d_keys; uint32_t* d_payload; size_t n; size_t capacity; } osort_kp;
+        struct { uint64_t* d_keys; uint32_t* d_payload; uint8_t* d_marks; size_t n; size_t capacity;
+                 uint64_t* d_count; void* d_scratch; size_t scratch_bytes; } ocompact_kpm;
+        struct { uint64_t* const* d_words; uint32_t n_words; uint64_t key_mask; size_t n; size_t capacity; }
+            osort_records;
+        struct { const void* d_build_keys; const uint8_t* d_build_mask; size_t build_n; const void* d_probe_keys;
+                 const uint8_t* d_probe_mask; size_t probe_n; uint32_t key_type; int64_t* d_out_build_rowid;
+                 int64_t* d_out_probe_rowid; uint64_t* d_counts; void* d_scratch; size_t scratch_bytes; } ojoin;
+        struct { const uint64_t* d_table; size_t table_n; const uint32_t* d_rids; size_t n_req; uint64_t* d_out;
+                 void* d_scratch; size_t scratch_bytes; } ogather;
+        struct { uint32_t* d_map; size_t n; uint64_t key; uint64_t counter; void* d_scratch; size_t scratch_bytes; }
+            oshuffle;
+        struct { const velo_lineitem* cols; size_t n; const velo_lineitem_pred* pred; uint32_t group_bound;
+                 int64_t* d_out; uint64_t* d_counts; void* d_scratch; size_t scratch_bytes; } filter_groupby;
+        struct { const velo_join_tables* tables; const velo_join_pred* pred; uint32_t k; int64_t* d_out;
+                 uint64_t* d_counts; void* d_scratch; size_t scratch_bytes; } join_topk;
+    } args;
+} velo_cmd;
+
+typedef struct velo_ctx velo_ctx;
+
+typedef struct velo_config {
+    int32_t device;          /* CUDA device ordinal */
+    uint32_t queue_capacity; /* tickets in flight before submit waits (0 = 1024) */
+} velo_config;
+
+/* Creates a context: a non-blocking stream on `device` and a ring of
+ * completion events (replaces TaskManager::start, which launches a
+ * cooperative persistent kernel that polls a host-mapped ring forever; here
+ * nothing runs while the queue is empty). */
+velo_status velo_init(const velo_config* config, velo_ctx** out);
+/* Waits up to timeout_ms for outstanding commands, then releases the
+ * context.  Never resets the device (the reference calls cudaDeviceReset on
+ * timeout, src/cuda/task_manager.cu:110-119).  VELO_ETIMEDOUT if commands
+ * were still running (the context is released anyway). */
+velo_status velo_shutdown(velo_ctx* ctx, uint32_t timeout_ms);
+/* Enqueues one command; *ticket identifies its completion.  Thread-safe
+ * (the reference's push is single-producer, src/cuda/commands.cpp:47-67). */
+velo_status velo_submit(velo_ctx* ctx, const velo_cmd* cmd, uint64_t* ticket);
+/* Enqueues n commands; the VELO_OP_OSORT_KP / VELO_OP_OCOMPACT_KPM commands
+ * among them run as ONE persistent batched launch (velo_batch_*), the others
+ * in order after it.  tickets[i] completes with the whole submission. */
+velo_status velo_batch_submit(velo_ctx* ctx, const velo_cmd* cmds, size_t n, uint64_t* tickets);
+/* Waits for a ticket, at most timeout_ns (VELO_ETIMEDOUT instead of
+ * spinning forever, cf. src/cuda/commands.cpp:69-91). */
+velo_status velo_wait(velo_ctx* ctx, uint64_t ticket, uint64_t timeout_ns);
+/* Copies the context's last error text into buf (always NUL-terminated). */
+velo_status velo_last_error(velo_ctx* ctx, char* buf, size_t len);
+/* The context's stream (a cudaStream_t) for callers that interleave their
+ * own work. */
+void* velo_ctx_stream(velo_ctx* ctx);
+/* sizeof(velo_cmd), for bindings that lay out command arrays themselves. */
+size_t velo_cmd_size(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,3 +68,17 @@ def test_compact_scratch_size():
     assert 0 < small <= big
     # one u32 count and one u32 prefix per 8192-row tile, 256-byte aligned
     assert big == 2 * ((1 << 10) * 4) + 256
+
+
+def test_queue_init_without_device_fails_cleanly():
+    import torch
+
+    if torch.cuda.is_available():
+        return  # covered by tests/test_queue_gpu.py on a GPU
+    L = velodb_b200.lib()
+    c = C.c_void_p()
+    rc = L.velo_init(C.byref(_lib.VeloConfig(0, 8)), C.byref(c))
+    assert rc == -3 and not c.value  # VELO_ECUDA, no context
+    assert L.velo_shutdown(None, 0) == 0
+    buf = C.create_string_buffer(64)
+    assert L.velo_last_error(None, buf, 64) == 0

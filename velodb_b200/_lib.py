@@ -37,6 +37,14 @@ PROTOS = {
     "velo_ogather_u64": (i32, [vp, sz, vp, sz, vp, vp, sz, vp]),
     "velo_ojoin_scratch_bytes": (sz, [sz, sz]),
     "velo_ojoin_pkfk": (i32, [vp, vp, sz, vp, vp, sz, u32, vp, vp, vp, vp, sz, vp]),
+    "velo_init": (i32, [vp, vp]),
+    "velo_shutdown": (i32, [vp, u32]),
+    "velo_submit": (i32, [vp, vp, vp]),
+    "velo_batch_submit": (i32, [vp, vp, sz, vp]),
+    "velo_wait": (i32, [vp, u64, u64]),
+    "velo_last_error": (i32, [vp, vp, sz]),
+    "velo_ctx_stream": (vp, [vp]),
+    "velo_cmd_size": (sz, []),
     "velo_batch_create": (i32, [vp, sz, vp, vp]),
     "velo_batch_launch": (i32, [vp, vp]),
     "velo_batch_status": (i32, [vp, vp]),
@@ -113,6 +121,34 @@ class VeloJoinPred(C.Structure):
 class VeloBatchItem(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("pad_", C.c_uint32), ("d_keys", C.c_void_p), ("d_payload", C.c_void_p),
                 ("d_marks", C.c_void_p), ("n", C.c_size_t), ("capacity", C.c_size_t), ("d_count", C.c_void_p)]
+
+
+def _args(*fields):
+    return type("Args", (C.Structure,), {"_fields_": [(f"f{i}", t) for i, t in enumerate(fields)]})
+
+
+class VeloCmdArgs(C.Union):
+    _fields_ = [
+        ("permute", _args(vp, vp, vp, sz, u32)),
+        ("compare_eq", _args(vp, vp, vp, sz, u32)),
+        ("osort_kp", _args(vp, vp, sz, sz)),
+        ("ocompact_kpm", _args(vp, vp, vp, sz, sz, vp, vp, sz)),
+        ("ogather", _args(vp, sz, vp, sz, vp, vp, sz)),
+        ("ojoin", _args(vp, vp, sz, vp, vp, sz, u32, vp, vp, vp, vp, sz)),
+    ]
+
+
+class VeloCmd(C.Structure):
+    _fields_ = [("opcode", C.c_uint32), ("flags", C.c_uint32), ("args", VeloCmdArgs)]
+
+
+class VeloConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("queue_capacity", C.c_uint32)]
+
+
+OP = dict(NOP=0, SCATTER=1, GATHER=2, SORT=3, PERMUTE=4, COMPARE_EQ=10, COMPOSE_POSITION_MAP=11, ENRICH_POSITIONS=12,
+          OSORT_KP=0x100, OCOMPACT_KPM=0x101, OSORT_RECORDS=0x102, OJOIN_PKFK=0x103, OGATHER=0x104, OSHUFFLE=0x105,
+          FILTER_GROUPBY=0x106, JOIN_GROUPBY_TOPK=0x107)
 
 
 def tune_ref(tune):
