@@ -446,6 +446,79 @@ void* velo_ctx_stream(velo_ctx* ctx);
 /* sizeof(velo_cmd), for bindings that lay out command arrays themselves. */
 size_t velo_cmd_size(void);
 
+/* ------------------------------------------------------------------------ */
+/* Serving layer: continuous admission of queries over resident tables      */
+/* ------------------------------------------------------------------------ */
+
+/* Device-resident tables the server's queries read (owned by the caller,
+ * resident for the server's lifetime). */
+typedef struct velo_served_tables {
+    velo_lineitem fact;         /* lineitem-shaped columns of the fact table */
+    const int64_t* fact_fk;     /* fact -> dimension key */
+    const int32_t* fact_fk32;   /* the same keys as int32 (two-way join query) */
+    size_t fact_n;
+    const int64_t* dim_key;     /* unique dimension keys */
+    const int32_t* dim_key32;   /* the same keys as int32 */
+    const int32_t* dim_date;
+    size_t dim_n;
+    const int64_t* fact2_fk;    /* second fact table -> fact row id */
+    const int64_t* fact2_price;
+    size_t fact2_n;
+} velo_served_tables;
+
+/* Query shapes: filter + group-by over a fact slice (config-1 shape);
+ * dimension slice JOIN fact slice + group-by + top-10 (config-2 shape);
+ * three-way chain dimension <- fact <- second fact, returning the number of
+ * joined rows and the sum of the second fact table's price. */
+#define VELO_Q_FILTER_GROUPBY 1u
+#define VELO_Q_JOIN_TOPK 2u
+#define VELO_Q_JOIN3 3u
+
+typedef struct velo_query {
+    uint32_t shape;
+    uint32_t pad_;
+    size_t offset, n;         /* fact slice (public size) */
+    size_t dim_offset, dim_n; /* dimension slice (joins) */
+    size_t f2_offset, f2_n;   /* second fact slice (VELO_Q_JOIN3) */
+    velo_lineitem_pred pred;  /* VELO_Q_FILTER_GROUPBY */
+    velo_join_pred jpred;     /* joins */
+} velo_query;
+
+typedef struct velo_query_result {
+    uint64_t qid;
+    int32_t status;
+    uint32_t shape;
+    double submit_ms, start_ms, end_ms; /* host clock, ms since server start */
+    int64_t out[96]; /* FILTER_GROUPBY: 8 x 6 as velo_filter_groupby; JOIN_TOPK: 10 x 3 as
+                        velo_join_groupby_topk; JOIN3: out[0] = sum of second-fact price */
+    uint64_t counts[2];
+} velo_query_result;
+
+typedef struct velo_server_config {
+    int32_t device;
+    uint32_t slots;            /* queries on the device at once (one stream each), 1..64 */
+    uint64_t hbm_budget_bytes; /* arena for all in-flight queries' scratch, allocated once */
+} velo_server_config;
+
+typedef struct velo_server_stats_t {
+    uint64_t admitted, completed, pending, peak_inflight, arena_bytes, peak_arena_bytes;
+} velo_server_stats_t;
+
+typedef struct velo_server velo_server;
+
+/* Starts the request loop.  Queries are admitted in arrival order whenever a
+ * slot is free and their scratch fits in the budget; admitted queries run
+ * concurrently on their own streams.  With slots = 1 the server runs one
+ * query at a time (the plain path). */
+velo_status velo_server_create(const velo_server_config* cfg, const velo_served_tables* tables, velo_server** out);
+/* Thread-safe; returns immediately with the query id. */
+velo_status velo_server_submit(velo_server* srv, const velo_query* q, uint64_t* qid);
+/* Waits (bounded) for a query and collects its result (once per query). */
+velo_status velo_server_wait(velo_server* srv, uint64_t qid, uint64_t timeout_ns, velo_query_result* out);
+velo_status velo_server_stats(velo_server* srv, velo_server_stats_t* out);
+/* Drains (bounded) and stops the loop; VELO_ETIMEDOUT leaves it running. */
+velo_status velo_server_destroy(velo_server* srv, uint32_t timeout_ms);
+
 #ifdef __cplusplus
 }
 #endif

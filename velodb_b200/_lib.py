@@ -45,6 +45,11 @@ PROTOS = {
     "velo_last_error": (i32, [vp, vp, sz]),
     "velo_ctx_stream": (vp, [vp]),
     "velo_cmd_size": (sz, []),
+    "velo_server_create": (i32, [vp, vp, vp]),
+    "velo_server_submit": (i32, [vp, vp, vp]),
+    "velo_server_wait": (i32, [vp, u64, u64, vp]),
+    "velo_server_stats": (i32, [vp, vp]),
+    "velo_server_destroy": (i32, [vp, u32]),
     "velo_batch_create": (i32, [vp, sz, vp, vp]),
     "velo_batch_launch": (i32, [vp, vp]),
     "velo_batch_status": (i32, [vp, vp]),
@@ -149,6 +154,32 @@ class VeloConfig(C.Structure):
 OP = dict(NOP=0, SCATTER=1, GATHER=2, SORT=3, PERMUTE=4, COMPARE_EQ=10, COMPOSE_POSITION_MAP=11, ENRICH_POSITIONS=12,
           OSORT_KP=0x100, OCOMPACT_KPM=0x101, OSORT_RECORDS=0x102, OJOIN_PKFK=0x103, OGATHER=0x104, OSHUFFLE=0x105,
           FILTER_GROUPBY=0x106, JOIN_GROUPBY_TOPK=0x107)
+
+
+class VeloServedTables(C.Structure):
+    _fields_ = [("fact", VeloLineitem), ("fact_fk", vp), ("fact_fk32", vp), ("fact_n", sz), ("dim_key", vp),
+                ("dim_key32", vp), ("dim_date", vp), ("dim_n", sz), ("fact2_fk", vp), ("fact2_price", vp),
+                ("fact2_n", sz)]
+
+
+class VeloQuery(C.Structure):
+    _fields_ = [("shape", C.c_uint32), ("pad_", C.c_uint32), ("offset", sz), ("n", sz), ("dim_offset", sz),
+                ("dim_n", sz), ("f2_offset", sz), ("f2_n", sz), ("pred", VeloLineitemPred), ("jpred", VeloJoinPred)]
+
+
+class VeloQueryResult(C.Structure):
+    _fields_ = [("qid", C.c_uint64), ("status", C.c_int32), ("shape", C.c_uint32), ("submit_ms", C.c_double),
+                ("start_ms", C.c_double), ("end_ms", C.c_double), ("out", C.c_int64 * 96),
+                ("counts", C.c_uint64 * 2)]
+
+
+class VeloServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("slots", C.c_uint32), ("hbm_budget_bytes", C.c_uint64)]
+
+
+class VeloServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("admitted", "completed", "pending", "peak_inflight", "arena_bytes",
+                                          "peak_arena_bytes")]
 
 
 def tune_ref(tune):
