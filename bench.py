@@ -7,7 +7,13 @@ sort on (flag1, flag2) -> segmented int64 sums, output padded to 8 groups).
 One step = one pass of that pipeline over one batch of input.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload groupby|sort]
+                    [--workload groupby|sort|batch|serve]
+
+Workloads: groupby (6,001,215-row filter + group-by, the default), sort
+(plain 2^20-row sort), batch (512 uneven sorts/compactions in one persistent
+launch replayed from a CUDA graph, beside 512 plain launch sequences), serve
+(query stream over resident 60 M / 15 M / 150 M-row tables: served vs plain
+one-at-a-time throughput and p50/p99 latency).
 
 Multi-GPU: one process per GPU (torchrun); the path does not shard, so every
 rank runs an independent replica of the workload ("replicas only") and the
@@ -467,7 +473,10 @@ def cpu_baseline_sort(W, orc):
 
 def run_reference(args, rank):
     """CPU reference arm: the reference's algorithm for the path (the oracle
-    port in the reference's network order) on all host cores, rank 0 only."""
+    port in the reference's network order) on all host cores, rank 0 only.
+    Each step is a bounded sample of the workload: the whole table for
+    groupby and sort, one instance of the 512 for batch, one query of the
+    stream for serve."""
     if rank != 0:
         return
     import oracle as orc
@@ -475,40 +484,195 @@ def run_reference(args, rank):
 
     orc.lib()
     cores = os.cpu_count() or 1
+    unit = "Mrows/s"
     if args.workload == "sort":
         n = 1 << 20
         keys, pay = W.sort_kp(n)
-        fn = lambda: orc.bitonic_kp(keys, pay, n_threads=cores)  # noqa: E731
-        sample, metric_rows = "full 2^20-row sort per step", n
+        steps = [(lambda: orc.bitonic_kp(keys, pay, n_threads=cores), n)]
+        sample, wl = "full 2^20-row sort per step", "plain_sort_2^20"
+    elif args.workload == "batch":
+        insts = W.batch_instances()
+        order = [(i * 97) % len(insts) for i in range(len(insts))]
+
+        def inst_fn(it):
+            if it["kind"] == "sort":
+                return lambda: orc.bitonic_kp(it["keys"], it["pay"], n_threads=cores)
+            rows = np.zeros((it["n"], 16), np.uint8)
+            rows[:, :8] = it["keys"].view(np.uint8).reshape(-1, 8)
+            rows[:, 8:12] = it["pay"].view(np.uint8).reshape(-1, 4)
+            return lambda: orc.ocompact(rows, it["marks"])
+
+        steps = [(inst_fn(insts[i]), insts[i]["n"]) for i in order]
+        sample = "one of the 512 instances per step (stride 97 through the list); sorts on all cores, " \
+                 "compactions single-threaded"
+        wl = "batched_512"
+    elif args.workload == "serve":
+        from velodb_b200 import serving as S
+
+        hs = S.HostSlices(**S.FULL_SCALE)
+        lo, hi = SERVE_DISTS["short"]
+        qs = [q for q in S.query_stream(hs, 4 * (args.steps + args.warmup) + 8, seed=0xB200000000000004,
+                                        lo_log2=lo, hi_log2=hi) if q.shape != S.Q_JOIN3]
+
+        def q_fn(q):
+            if q.shape == S.Q_FILTER_GROUPBY:
+                cols = hs.lineitem(q.offset, q.n)
+                return lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores)
+            dim, fact = hs.join_inputs(q)
+            return lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, 10, n_threads=cores)
+
+        steps = [(q_fn(q), 1) for q in qs]
+        unit = "queries/s"
+        sample = "one query per step from the served stream (sizes 2^10..2^18), filter+group-by and " \
+                 "two-way join shapes (the three-way chain has no oracle pipeline)"
+        wl = "served_stream"
     else:
         # the reference reveals the filtered count and sorts next_pow2(count)
         # rows (src/operator/filter_compaction_operator.cpp:171-178)
         n = W.LINEITEM_ROWS
         cols = W.lineitem(n)
-        fn = lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores)  # noqa: E731
-        sample, metric_rows = "full 6,001,215-row table per step (filtered count revealed)", n
-    for _ in range(args.warmup):
-        fn()
-    ts = []
-    for _ in range(args.steps):
+        steps = [(lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores), n)]
+        sample, wl = "full 6,001,215-row table per step (filtered count revealed)", "filter_groupby"
+    for i in range(args.warmup):
+        steps[i % len(steps)][0]()
+    ts, units = [], 0
+    for i in range(args.steps):
+        fn, u = steps[(args.warmup + i) % len(steps)]
         t0 = time.perf_counter()
         fn()
         ts.append(time.perf_counter() - t0)
-    ms = 1e3 * float(np.mean(ts))
-    value = metric_rows / (ms / 1e3) / 1e6
-    wl = "plain_sort_2^20" if args.workload == "sort" else "filter_groupby"
+        units += u
+    total = float(np.sum(ts))
+    ms = 1e3 * total / args.steps
+    value = units / total / (1e6 if unit == "Mrows/s" else 1.0)
     line = {
-        "impl": "reference", "metric": metric_name(args.workload), "value": value, "unit": "Mrows/s",
+        "impl": "reference", "metric": metric_name(args.workload), "value": value, "unit": unit,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": wl, "rows": metric_rows},
-        "cpu_baseline": {"value": value, "unit": "Mrows/s", "cores": cores, "kind": "port", "sample": sample},
-        "e2e": {"value": value, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": wl},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------
+# served query stream (resident tables, continuous admission)
+# --------------------------------------------------------------------------
+
+SERVE_DISTS = {"short": (10.0, 18.0), "analytic": (14.0, 22.0)}
+SERVE_LOADS = (0.5, 0.9, 1.5, 3.0, 6.0)
+
+
+def _lat(results, t_key="submit_ms"):
+    lat = np.asarray([r.end_ms - getattr(r, t_key) for r in results])
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+
+
+def run_serve(args, world, rank, local):
+    """Config-4 shape: a seeded query stream (50 % filter + group-by, 35 %
+    two-way join + top-10, 15 % three-way chain) over resident tables of
+    60 M / 15 M / 150 M rows, admitted by a 120 GB HBM budget.  The plain
+    path is the same request loop with one slot, each query submitted after
+    the previous one returned; the served path admits up to 16 queries at a
+    time on their own streams.  Latency is submit -> result in host memory on
+    the host clock (the request loop spans many streams, so no single device
+    event brackets it); `value` is the served throughput at saturation."""
+    import torch
+    import torch.distributed as dist
+
+    from velodb_b200 import serving as S
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+    t0 = time.perf_counter()
+    tab = S.ServedTables(**S.FULL_SCALE)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(120 << 30, free - (4 << 30)))
+    nq = max(128, 32 * args.steps)
+    slots = 16
+    out = {}
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    for dname, (lo, hi) in SERVE_DISTS.items():
+        qs = S.query_stream(tab, nq, seed=0xB200000000000004, lo_log2=lo, hi_log2=hi)
+        srv = S.Server(tab, slots=1, budget_bytes=budget)
+        S.run_closed_one_at_a_time(srv, qs[: max(8, args.warmup)])
+        plain_res, plain_s = S.run_closed_one_at_a_time(srv, qs)
+        plain_qps = nq / plain_s
+        plain_loads = {}
+        for f in (0.5, 0.9):
+            r, _ = S.run_open_loop(srv, qs, S.arrivals(nq, f * plain_qps, seed=int(f * 1000)))
+            plain_loads[f"{f}x"] = {"offered_qps": f * plain_qps, **_lat(r)}
+        srv.close()
+        srv = S.Server(tab, slots=slots, budget_bytes=budget)
+        S.run_open_loop(srv, qs[: max(16, args.warmup)], np.zeros(max(16, args.warmup)))
+        sat_res, sat_s = S.run_open_loop(srv, qs, np.zeros(nq))
+        served_qps = nq / sat_s
+        loads = {}
+        for f in SERVE_LOADS:
+            r, s = S.run_open_loop(srv, qs, S.arrivals(nq, f * plain_qps, seed=int(f * 1000)))
+            loads[f"{f}x"] = {"offered_qps": f * plain_qps, "achieved_qps": nq / s, **_lat(r)}
+        st = srv.stats()
+        srv.close()
+        same = all(S.result_key(a) == S.result_key(b) and a.status == 0 and b.status == 0
+                   for a, b in zip(plain_res, sat_res))
+        shapes = {S.SHAPE_NAMES[k]: int(sum(1 for q in qs if q.shape == k)) for k in S.SHAPE_NAMES}
+        out[dname] = {
+            "sizes_log2": [lo, hi], "queries": nq, "mix": shapes,
+            "plain": {"qps": plain_qps, **_lat(plain_res), "under_poisson": plain_loads},
+            "served": {"qps_saturation": served_qps, **_lat(sat_res), "slots": slots,
+                       "peak_inflight": st["peak_inflight"], "peak_arena_bytes": st["peak_arena_bytes"],
+                       "poisson": loads},
+            "speedup_served_vs_plain": served_qps / plain_qps,
+            "results_identical_alone_and_in_mix": bool(same),
+        }
+    clk = clocks.stop()
+    head = out["short"]
+    value = head["served"]["qps_saturation"]
+    if world > 1:
+        t = torch.tensor([1.0 / value], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        value = world / float(t.item())
+    from velodb_b200._lib import VeloQuery, VeloQueryResult
+
+    line = {
+        "metric": metric_name("serve"), "value": value, "unit": "queries/s", "n_gpus": world,
+        "steps": nq, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": "served_stream", "tables_rows": dict(S.FULL_SCALE),
+                   "resident_bytes": int(tab.bytes), "table_build_s": build_s, "hbm_budget_bytes": budget,
+                   "headline_sizes_log2": list(SERVE_DISTS["short"]), "parallelism": f"replicas{world}",
+                   "timing": "host clock, submit -> result in host memory",
+                   "l2": "inputs larger than L2 (resident tables 4.9 GB)"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": C_sizeof(VeloQuery),
+                "d2h_bytes_per_step": C_sizeof(VeloQueryResult),
+                "note": "the served numbers are end to end: a query descriptor in, a result struct out"},
+        "serve": out, "clocks": clk,
+        "gpu_launches": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def C_sizeof(t):
+    import ctypes
+
+    return ctypes.sizeof(t)
+
+
 def metric_name(workload):
+    if workload == "serve":
+        return "served query throughput at saturation (queries/s; p50/p99 vs plain one-at-a-time)"
     if workload == "batch":
         return "batched oblivious sorts+compactions throughput (512 instances, 2^10..2^22 rows)"
     if workload == "sort":
@@ -522,7 +686,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "sort", "batch"])
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "sort", "batch", "serve"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -533,6 +697,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload == "serve":
+        run_serve(args, world, rank, local)
         return
 
     import torch

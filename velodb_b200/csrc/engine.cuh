@@ -101,7 +101,7 @@ __device__ __forceinline__ uint32_t key_gt_mask(const uint64_t* x, const uint64_
 // ---------------------------------------------------------------------------
 // row types: SoA columns in global memory, SoA arrays in shared memory.
 //
-// swap_mask(a, b, desc) is the compare-exchange decision for the pair
+// swap_pred(a, b, desc) is the compare-exchange decision for the pair
 // (a at the lower index, b): ascending swaps iff a > b, descending iff a < b.
 // STRICT types follow the reference exactly on ties (include/cuda/sort.cuh:
 // 31-40: no swap when equal).  Non-strict types are used where the
@@ -116,6 +116,28 @@ __device__ __forceinline__ T sel(bool c, T a, T b)
 {
     return c ? a : b;
 }
+
+// exchange a and b when x (selects, no branch)
+__device__ __forceinline__ void xsel(bool x, uint32_t& a, uint32_t& b)
+{
+    const uint32_t na = x ? b : a, nb = x ? a : b;
+    a = na;
+    b = nb;
+}
+
+__device__ __forceinline__ void xsel(bool x, uint64_t& a, uint64_t& b)
+{
+    const uint64_t na = x ? b : a, nb = x ? a : b;
+    a = na;
+    b = nb;
+}
+
+// how a RowRec compares its key
+enum KeyMode : int {
+    KEY_MASKED = 0, // words 0..KW-1, each AND-ed with Cols::mask (runtime)
+    KEY_FULL = 1,   // words 0..KW-1 as they are
+    KEY_HI32 = 2,   // the high 32 bits of word 0 only (KW == 1)
+};
 
 // (u64 key, u32 payload), ordered lexicographically on both (plain sort rows).
 // Every field is compared, so the sorted output is unique.  Registers hold
@@ -148,20 +170,16 @@ struct RowKP {
         const uint4 x = reinterpret_cast<const uint4*>(sm)[i];
         return RowKP { x.x, x.y, x.z };
     }
-    __device__ __forceinline__ static uint32_t swap_mask(const RowKP& a, const RowKP& b, uint32_t desc, const Cols&)
+    __device__ __forceinline__ static bool swap_pred(const RowKP& a, const RowKP& b, bool desc, const Cols&)
     {
-        return gt_mask3(a.p, a.kl, a.kh, b.p, b.kl, b.kh) ^ desc;
+        return (gt_mask3(a.p, a.kl, a.kh, b.p, b.kl, b.kh) != 0u) != desc;
     }
-    // exchange a and b where m is all ones, in place
-    __device__ __forceinline__ static void cswap(RowKP& a, RowKP& b, uint32_t m)
+    // exchange a and b where m is all ones, in place (two selects a register)
+    __device__ __forceinline__ static void cswap(RowKP& a, RowKP& b, bool x)
     {
-        const uint32_t dl = (a.kl ^ b.kl) & m, dh = (a.kh ^ b.kh) & m, dp = (a.p ^ b.p) & m;
-        a.kl ^= dl;
-        b.kl ^= dl;
-        a.kh ^= dh;
-        b.kh ^= dh;
-        a.p ^= dp;
-        b.p ^= dp;
+        xsel(x, a.kl, b.kl);
+        xsel(x, a.kh, b.kh);
+        xsel(x, a.p, b.p);
     }
     __device__ __forceinline__ static bool marked(const RowKP&) { return false; }
 };
@@ -198,33 +216,29 @@ struct RowKPM {
         const uint4 x = reinterpret_cast<const uint4*>(sm)[i];
         return RowKPM { x.x, x.y, x.z, x.w };
     }
-    __device__ __forceinline__ static uint32_t swap_mask(const RowKPM& a, const RowKPM& b, uint32_t desc, const Cols&)
+    __device__ __forceinline__ static bool swap_pred(const RowKPM& a, const RowKPM& b, bool desc, const Cols&)
     {
         const uint32_t gt = gt_mask3(a.p, a.kl, a.kh, b.p, b.kl, b.kh);
         const uint32_t lt = gt_mask3(b.p, b.kl, b.kh, a.p, a.kl, a.kh);
-        return desc ? lt : gt;
+        return (desc ? lt : gt) != 0u;
     }
-    __device__ __forceinline__ static void cswap(RowKPM& a, RowKPM& b, uint32_t msk)
+    __device__ __forceinline__ static void cswap(RowKPM& a, RowKPM& b, bool x)
     {
-        const uint32_t dl = (a.kl ^ b.kl) & msk, dh = (a.kh ^ b.kh) & msk, dp = (a.p ^ b.p) & msk,
-                       dm = (a.m ^ b.m) & msk;
-        a.kl ^= dl;
-        b.kl ^= dl;
-        a.kh ^= dh;
-        b.kh ^= dh;
-        a.p ^= dp;
-        b.p ^= dp;
-        a.m ^= dm;
-        b.m ^= dm;
+        xsel(x, a.kl, b.kl);
+        xsel(x, a.kh, b.kh);
+        xsel(x, a.p, b.p);
+        xsel(x, a.m, b.m);
     }
     __device__ __forceinline__ static bool marked(const RowKPM& r) { return r.m != 0; }
 };
 
-// W u64 words per row (SoA).  Ordered lexicographically on the first KW words,
-// each AND-ed with a mask; the mark (for compaction) is bit `mark_bit` of word
-// 0, inverted when mark_inv is set (so an "invalid" flag can sort last).
-template <int W, int KW, bool STRICT = true>
+// W u64 words per row (SoA).  Ordered lexicographically on the first KW words
+// as KM says (masked, whole, or the high half of word 0); the mark (for
+// compaction) is bit `mark_bit` of word `mark_word`, inverted when mark_inv is
+// set (so an "invalid" flag can sort last).
+template <int W, int KW, bool STRICT = true, int KM = KEY_MASKED>
 struct RowRec {
+    static_assert(KM != KEY_HI32 || KW == 1, "a 32-bit key lives in word 0");
     uint64_t w[W];
     struct Cols {
         uint64_t* w[W];
@@ -286,31 +300,33 @@ struct RowRec {
         }
         return r;
     }
-    __device__ __forceinline__ static void cswap(RowRec& a, RowRec& b, uint32_t m)
+    __device__ __forceinline__ static void cswap(RowRec& a, RowRec& b, bool x)
     {
-        const uint64_t mm = ((uint64_t)m << 32) | m;
 #pragma unroll
-        for (int x = 0; x < W; x++) {
-            const uint64_t d = (a.w[x] ^ b.w[x]) & mm;
-            a.w[x] ^= d;
-            b.w[x] ^= d;
-        }
+        for (int i = 0; i < W; i++)
+            xsel(x, a.w[i], b.w[i]);
     }
-    __device__ __forceinline__ static uint32_t swap_mask(const RowRec& a, const RowRec& b, uint32_t desc,
-                                                         const Cols& c)
+    __device__ __forceinline__ static bool swap_pred(const RowRec& a, const RowRec& b, bool desc, const Cols& c)
     {
+        if constexpr (KM == KEY_HI32) {
+            const uint32_t x = hi32(a.w[0]), y = hi32(b.w[0]);
+            if constexpr (STRICT)
+                return desc ? (x < y) : (x > y);
+            else
+                return (x > y) != desc;
+        }
         uint64_t ka[KW], kb[KW];
 #pragma unroll
         for (int x = 0; x < KW; x++) {
-            ka[x] = a.w[x] & c.mask[x];
-            kb[x] = b.w[x] & c.mask[x];
+            ka[x] = KM == KEY_FULL ? a.w[x] : (a.w[x] & c.mask[x]);
+            kb[x] = KM == KEY_FULL ? b.w[x] : (b.w[x] & c.mask[x]);
         }
         if constexpr (STRICT) {
             const uint32_t gt = key_gt_mask<KW>(ka, kb);
             const uint32_t lt = key_gt_mask<KW>(kb, ka);
-            return desc ? lt : gt;
+            return (desc ? lt : gt) != 0u;
         } else {
-            return key_gt_mask<KW>(ka, kb) ^ desc;
+            return (key_gt_mask<KW>(ka, kb) != 0u) != desc;
         }
     }
     __device__ __forceinline__ static RowRec select(bool cnd, const RowRec& a, const RowRec& b)
@@ -335,11 +351,12 @@ template <class R>
 struct MarkOf {
     __device__ __forceinline__ static bool get(const R& r, const typename R::Cols&) { return R::marked(r); }
 };
-template <int W, int KW, bool S>
-struct MarkOf<RowRec<W, KW, S>> {
-    __device__ __forceinline__ static bool get(const RowRec<W, KW, S>& r, const typename RowRec<W, KW, S>::Cols& c)
+template <int W, int KW, bool S, int KM>
+struct MarkOf<RowRec<W, KW, S, KM>> {
+    __device__ __forceinline__ static bool get(const RowRec<W, KW, S, KM>& r,
+                                               const typename RowRec<W, KW, S, KM>::Cols& c)
     {
-        return RowRec<W, KW, S>::marked_c(r, c);
+        return RowRec<W, KW, S, KM>::marked_c(r, c);
     }
 };
 

@@ -38,9 +38,10 @@ constexpr int J_LMAX = J_LT - 5 < 8 ? J_LT - 5 : 8;
 struct JoinAgg {
     static constexpr int W = 2;
     static constexpr int V = 2;
+    struct Params {};
     __device__ __forceinline__ static uint64_t key(const uint64_t* w) { return w[0] & (0xFFFFFFFF00000000ull | J_JOINED); }
     __device__ __forceinline__ static bool valid(const uint64_t* w) { return (w[0] & J_JOINED) != 0; }
-    __device__ __forceinline__ static void values(const uint64_t* w, int64_t (&v)[V])
+    __device__ __forceinline__ static void values(const uint64_t* w, int64_t (&v)[V], const Params&)
     {
         const bool ok = valid(w);
         v[0] = ok ? (int64_t)w[1] : 0;
@@ -215,7 +216,7 @@ __global__ void k_topk_out(const uint64_t* t0, const uint64_t* t1, const uint64_
 __global__ void __launch_bounds__(SEG_THREADS) k_jseg_summary(JRec::Cols c, SegTileAgg* aggs, int64_t* runs)
 {
     extern __shared__ __align__(16) char sm[];
-    JSeg::tile_summary(c.w, blockIdx.x, aggs, runs, sm);
+    JSeg::tile_summary(c.w, blockIdx.x, aggs, runs, JoinAgg::Params {}, sm);
 }
 
 __global__ void __launch_bounds__(1024) k_jseg_carries(const SegTileAgg* aggs, const int64_t* runs, int ntiles,
@@ -229,7 +230,7 @@ __global__ void __launch_bounds__(SEG_THREADS) k_jseg_emit_rows(JRec::Cols c, in
                                                                 const int64_t* carry_in, GRec::Cols g)
 {
     extern __shared__ __align__(16) char sm[];
-    JSeg::emit_rows(c.w, blockIdx.x, ntiles, aggs, carry_in, g.w, sm);
+    JSeg::emit_rows(c.w, blockIdx.x, ntiles, aggs, carry_in, g.w, JoinAgg::Params {}, sm);
 }
 
 struct JoinScratch {
@@ -301,7 +302,7 @@ static velo_status join_attrs()
     VELO_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev >= 0 && dev < 64 && done[dev])
         return VELO_OK;
-    VELO_CUDA_TRY(cudaFuncSetAttribute(k_jseg_summary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JSeg::SMEM),
+    VELO_CUDA_TRY(cudaFuncSetAttribute(k_jseg_summary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JSeg::SMEM_IN),
                   "cudaFuncSetAttribute");
     VELO_CUDA_TRY(cudaFuncSetAttribute(k_jseg_emit_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JSeg::SMEM),
                   "cudaFuncSetAttribute");
@@ -398,7 +399,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     gc.mark_bit = 63;
     gc.mark_inv = 1;
     gc.mark_word = 0;
-    k_jseg_summary<<<nts, SEG_THREADS, JSeg::SMEM, st>>>(uc, s.aggs, s.runs);
+    k_jseg_summary<<<nts, SEG_THREADS, JSeg::SMEM_IN, st>>>(uc, s.aggs, s.runs);
     k_jseg_carries<<<1, 1024, JoinAgg::V * 1024 * 8 + 2 * 1024 * 4, st>>>(s.aggs, s.runs, nts, s.carry,
                                                                             s.tail_prefix, s.n_groups);
     k_jseg_emit_rows<<<nts, SEG_THREADS, JSeg::SMEM, st>>>(uc, nts, s.aggs, s.carry, gc);

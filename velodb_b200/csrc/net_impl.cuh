@@ -7,8 +7,13 @@
 
 namespace velo {
 
+// 256-thread CTAs are asked to fit two per SM (at most 128 registers a
+// thread): with one 8-warp CTA per SM the in-tile levels stall on latency.
+template <int LOG_NT>
+constexpr int net_min_blocks() { return LOG_NT <= 8 ? 2 : 1; }
+
 template <class R, int LOG_NT, int LOG_E>
-__global__ void __launch_bounds__(1 << LOG_NT)
+__global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<LOG_NT>())
     k_sort_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];
@@ -16,7 +21,7 @@ __global__ void __launch_bounds__(1 << LOG_NT)
 }
 
 template <class R, int LOG_NT, int LOG_E>
-__global__ void __launch_bounds__(1 << LOG_NT)
+__global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<LOG_NT>())
     k_compact_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];

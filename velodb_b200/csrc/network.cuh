@@ -51,9 +51,9 @@ template <>
 struct MarkAt<RowKPM> {
     __device__ __forceinline__ static bool get(const RowKPM::Cols& c, size_t g) { return __ldcg(c.m + g) != 0; }
 };
-template <int W, int KW, bool S>
-struct MarkAt<RowRec<W, KW, S>> {
-    __device__ __forceinline__ static bool get(const typename RowRec<W, KW, S>::Cols& c, size_t g)
+template <int W, int KW, bool S, int KM>
+struct MarkAt<RowRec<W, KW, S, KM>> {
+    __device__ __forceinline__ static bool get(const typename RowRec<W, KW, S, KM>::Cols& c, size_t g)
     {
         return (((__ldcg(c.w[c.mark_word] + g) >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
     }
@@ -189,17 +189,17 @@ struct Net {
     // the register window (only for phases k < 2^LOG_E), where pair e is
     // descending iff bit `dbit` of e is set.
     template <int Q, bool PER_E>
-    __device__ __forceinline__ static void bitonic_level(R (&v)[E], const Cols& c, uint32_t dm, int dbit)
+    __device__ __forceinline__ static void bitonic_level(R (&v)[E], const Cols& c, bool dm, uint32_t dpat)
     {
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
                 continue;
             const int e2 = e | (1 << Q);
-            uint32_t d = dm;
+            bool d = dm;
             if constexpr (PER_E)
-                d = ((e >> dbit) & 1) ? ~0u : 0u;
-            R::cswap(v[e], v[e2], R::swap_mask(v[e], v[e2], d, c));
+                d = (dpat & (1u << e)) != 0u;
+            R::cswap(v[e], v[e2], R::swap_pred(v[e], v[e2], d, c));
         }
     }
 
@@ -208,16 +208,36 @@ struct Net {
                                                           bool dconst, bool asc_c)
     {
         const bool per_e = !dconst && K >= s && K < s + LOG_E;
-        const uint32_t dm = dconst ? (asc_c ? 0u : ~0u) : ((((tidpart(s) >> K) & 1) != 0) ? ~0u : 0u);
-        const int dbit = K - s;
+        const bool dm = dconst ? !asc_c : (((tidpart(s) >> K) & 1) != 0);
+        // per-register directions: bit e set iff bit K-s of e is set
+        const int kb = K - s;
+        const uint32_t dpat = !per_e ? 0u
+            : kb == 0               ? 0xAAAAAAAAu
+            : kb == 1               ? 0xCCCCCCCCu
+            : kb == 2               ? 0xF0F0F0F0u
+            : kb == 3               ? 0xFF00FF00u
+                                    : 0xFFFF0000u;
+        static_assert(LOG_E <= 5, "direction patterns cover 32 registers");
+        if (b_hi >= s + LOG_E - 1 && b_lo <= s) {
+            // the whole window: straight-line levels, no per-level branch
+            // (a branch per level makes every join re-home the row registers)
+            if (per_e) {
+                auto f = [&](auto qc) { bitonic_level<decltype(qc)::value, true>(v, c, dm, dpat); };
+                QDown<LOG_E - 1>::run(f);
+            } else {
+                auto f = [&](auto qc) { bitonic_level<decltype(qc)::value, false>(v, c, dm, dpat); };
+                QDown<LOG_E - 1>::run(f);
+            }
+            return;
+        }
         auto f = [&](auto qc) {
             constexpr int Q = decltype(qc)::value;
             const int b = s + Q;
             if (b <= b_hi && b >= b_lo) {
                 if (per_e)
-                    bitonic_level<Q, true>(v, c, dm, dbit);
+                    bitonic_level<Q, true>(v, c, dm, dpat);
                 else
-                    bitonic_level<Q, false>(v, c, dm, dbit);
+                    bitonic_level<Q, false>(v, c, dm, dpat);
             }
         };
         QDown<LOG_E - 1>::run(f);
@@ -255,17 +275,21 @@ struct Net {
                 const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
                 sw = sb != (i >= ((off + left) & (half - 1)));
             }
-            R::cswap(v[e], v[e2], sw ? ~0u : 0u);
+            R::cswap(v[e], v[e2], sw);
         }
     }
 
+    // `gpre[m]` holds P at the tile whose bits b_lo..b_hi are m (the CTA's
+    // other tile bits fixed, its bits below b_lo zero): every block start and
+    // block middle of a global level is such a tile boundary.
     template <int Q>
     __device__ __forceinline__ static void compact_level_global(R (&v)[E], const Cols& c, int s, int b,
-                                                                const uint32_t* tile_prefix, int C, int b_lo,
-                                                                size_t cta_bits)
+                                                                const uint32_t* gpre, int C, int b_lo,
+                                                                size_t cta_bits, int L)
     {
         const int tp = tidpart(s);
         const uint64_t half = 1ull << b;
+        const uint32_t mmask = (1u << L) - 1u;
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
@@ -274,14 +298,15 @@ struct Net {
             const int l = tp | (e << s);
             const uint64_t g = (uint64_t)(l & ((1 << C) - 1)) | ((uint64_t)(l >> C) << b_lo) | cta_bits;
             const uint64_t blk = g & ~(2 * half - 1);
-            const uint32_t ps = __ldcg(tile_prefix + (blk >> LT));
-            const uint32_t pm = __ldcg(tile_prefix + ((blk + half) >> LT));
+            const uint32_t mb = (uint32_t)(blk >> b_lo) & mmask;
+            const uint32_t ps = gpre[mb];
+            const uint32_t pm = gpre[mb | (1u << (b - b_lo))];
             const uint64_t left = pm - ps;
             const uint64_t off = ps & (2 * half - 1);
             const uint64_t i = g - blk;
             const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
             const bool sw = sb != (i >= ((off + left) & (half - 1)));
-            R::cswap(v[e], v[e2], sw ? ~0u : 0u);
+            R::cswap(v[e], v[e2], sw);
         }
     }
 
@@ -387,16 +412,32 @@ struct Net {
                         s = ns;
                     }
                     const int hi = (s + LOG_E - 1 < p.K - 1) ? s + LOG_E - 1 : p.K - 1;
-                    auto f = [&](auto qc) {
-                        constexpr int Q = decltype(qc)::value;
-                        const int bb = s + Q;
-                        if (bb >= b && bb <= hi)
-                            compact_level_tile<Q>(v, c, s, bb, p_tile, pre);
-                    };
-                    QUp<0, LOG_E>::run(f);
+                    if (b <= s && hi == s + LOG_E - 1) {
+                        auto f = [&](auto qc) {
+                            constexpr int Q = decltype(qc)::value;
+                            compact_level_tile<Q>(v, c, s, s + Q, p_tile, pre);
+                        };
+                        QUp<0, LOG_E>::run(f);
+                    } else {
+                        auto f = [&](auto qc) {
+                            constexpr int Q = decltype(qc)::value;
+                            const int bb = s + Q;
+                            if (bb >= b && bb <= hi)
+                                compact_level_tile<Q>(v, c, s, bb, p_tile, pre);
+                        };
+                        QUp<0, LOG_E>::run(f);
+                    }
                     b = hi + 1;
                 }
             } else { // P_COMPACT_GLOBAL: local bits C..C+L-1 bottom-up
+                uint32_t* gpre = reinterpret_cast<uint32_t*>(sm + smem_rows());
+                {
+                    const int lo_bits = b_lo - C;
+                    const size_t t_hi = ((size_t)(cta >> lo_bits)) << (p.b_hi + 1 - LT);
+                    for (int m = threadIdx.x; m < (1 << p.L); m += TL::NT)
+                        gpre[m] = __ldcg(tile_prefix + (t_hi | ((size_t)m << (b_lo - LT))));
+                    __syncthreads();
+                }
                 int lb = C;
                 const int top = C + p.L - 1;
                 while (lb <= top) {
@@ -407,13 +448,21 @@ struct Net {
                         s = ns;
                     }
                     const int hi = (s + LOG_E - 1 < top) ? s + LOG_E - 1 : top;
-                    auto f = [&](auto qc) {
-                        constexpr int Q = decltype(qc)::value;
-                        const int lp = s + Q;
-                        if (lp >= lb && lp <= hi)
-                            compact_level_global<Q>(v, c, s, b_lo + (lp - C), tile_prefix, C, b_lo, cta_bits);
-                    };
-                    QUp<0, LOG_E>::run(f);
+                    if (lb <= s && hi == s + LOG_E - 1) {
+                        auto f = [&](auto qc) {
+                            constexpr int Q = decltype(qc)::value;
+                            compact_level_global<Q>(v, c, s, b_lo + (s + Q - C), gpre, C, b_lo, cta_bits, p.L);
+                        };
+                        QUp<0, LOG_E>::run(f);
+                    } else {
+                        auto f = [&](auto qc) {
+                            constexpr int Q = decltype(qc)::value;
+                            const int lp = s + Q;
+                            if (lp >= lb && lp <= hi)
+                                compact_level_global<Q>(v, c, s, b_lo + (lp - C), gpre, C, b_lo, cta_bits, p.L);
+                        };
+                        QUp<0, LOG_E>::run(f);
+                    }
                     lb = hi + 1;
                 }
             }

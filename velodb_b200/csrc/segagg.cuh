@@ -88,18 +88,24 @@ __device__ __forceinline__ int64_t warp_sum_i64(int64_t x)
     return x;
 }
 
-// Agg: static constexpr int W (record words), V (values);
+// Agg: static constexpr int W (record words), V (values); struct Params
+//      (public decoding parameters passed to every pass);
 //      static uint64_t key(const uint64_t* w)      -- run key (includes validity)
 //      static bool valid(const uint64_t* w)
-//      static void values(const uint64_t* w, int64_t (&v)[V])  -- zero when invalid
-//      static int64_t out_key(const uint64_t* w)
+//      static void values(const uint64_t* w, int64_t (&v)[V], const Params&)  -- zero when invalid
+//      static int64_t out_key_from(uint64_t key)
 template <class Agg>
 struct SegAgg {
     static constexpr int W = Agg::W;
     static constexpr int V = Agg::V;
     // the tile area holds the W input words, later the 1+V output words
     static constexpr int TW = W > 1 + V ? W : 1 + V;
+    using Params = typename Agg::Params;
+    // emit_rows stages 1+V output words in the tile area; the other passes
+    // only the W input words (smaller footprint, more CTAs per SM)
     static constexpr size_t SMEM = (size_t)SEG_TS_PAD * TW * 8 + (size_t)V * SEG_THREADS * 8 + SEG_THREADS * 4 + 256;
+    static constexpr size_t SMEM_IN = (size_t)SEG_TS_PAD * W * 8 + (size_t)V * SEG_THREADS * 8 + SEG_THREADS * 4 + 256;
+    static_assert((size_t)SEG_MAX_G * (1 + V) * 8 * 8 <= (size_t)SEG_TS_PAD * W * 8, "emit reduction fits the tile area");
 
     // stage the tile's records in smem (coalesced), then thread t owns rows
     // [t*RPT, t*RPT + RPT)
@@ -122,11 +128,11 @@ struct SegAgg {
 
     // pass A
     __device__ static void tile_summary(uint64_t* const* words, int tile, SegTileAgg* aggs, int64_t* tail_runs,
-                                        char* smem)
+                                        const Params& prm, char* smem)
     {
         uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
-        uint32_t* tmp = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS_PAD * TW * 8);
-        int64_t* red = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * TW * 8 + 256);
+        uint32_t* tmp = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS_PAD * W * 8);
+        int64_t* red = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * W * 8 + 256);
         const size_t base = (size_t)tile * SEG_TS;
         load_tile(words, base, sw);
         uint64_t wl[W];
@@ -146,7 +152,7 @@ struct SegAgg {
             row(sw, nxt, wn);
             const uint64_t k = Agg::key(w);
             int64_t v[V];
-            Agg::values(w, v);
+            Agg::values(w, v, prm);
             const bool in_run = (k == tail_key);
 #pragma unroll
             for (int i = 0; i < V; i++)
@@ -287,11 +293,11 @@ struct SegAgg {
     // pass C
     __device__ static void emit(uint64_t* const* words, int tile, int ntiles, const SegTileAgg* aggs,
                                 const int64_t* carry_in, const uint32_t* tail_prefix, int G, int64_t* tile_out,
-                                char* smem)
+                                const Params& prm, char* smem)
     {
         uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
-        int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * TW * 8);
-        uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS_PAD * TW * 8 + (size_t)V * SEG_THREADS * 8);
+        int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * W * 8);
+        uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS_PAD * W * 8 + (size_t)V * SEG_THREADS * 8);
         const size_t base = (size_t)tile * SEG_TS;
         load_tile(words, base, sw);
         const uint64_t next_head = (tile + 1 < ntiles) ? aggs[tile + 1].head_key : ~0ull;
@@ -318,7 +324,7 @@ struct SegAgg {
                 row(sw, r0 + r, w);
                 const uint64_t k = Agg::key(w);
                 int64_t v[V];
-                Agg::values(w, v);
+                Agg::values(w, v, prm);
                 const bool starts = (r0 + r == 0) ? true : (k != prev_key);
                 start_flag = start_flag | starts;
 #pragma unroll
@@ -426,7 +432,7 @@ struct SegAgg {
     // o1.. = the group's sums, valid only on the group's last row); an
     // ORCompact of the records then yields the groups in key order.
     __device__ static void emit_rows(uint64_t* const* words, int tile, int ntiles, const SegTileAgg* aggs,
-                                     const int64_t* carry_in, uint64_t* const* out, char* smem)
+                                     const int64_t* carry_in, uint64_t* const* out, const Params& prm, char* smem)
     {
         uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
         int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * TW * 8);
@@ -455,7 +461,7 @@ struct SegAgg {
                 row(sw, r0 + r, w);
                 const uint64_t k = Agg::key(w);
                 int64_t v[V];
-                Agg::values(w, v);
+                Agg::values(w, v, prm);
                 const bool starts = (r0 + r == 0) ? true : (k != prev_key);
                 start_flag = start_flag | starts;
 #pragma unroll
@@ -520,17 +526,25 @@ struct SegAgg {
         }
     }
 
-    // pass D: out[j] = sum over tiles of tile_out[tile][j] (one CTA)
+    // pass D: out[q] = sum over tiles of tile_out[tile][q]; CTA q of
+    // G*(1+V) CTAs, SEG_THREADS threads
     __device__ static void finish(const int64_t* tile_out, int ntiles, int G, int64_t* out)
     {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-        for (int q = warp; q < G * (1 + V); q += nw) {
-            int64_t sum = 0;
-            for (int t = lane; t < ntiles; t += 32)
-                sum += tile_out[(size_t)t * G * (1 + V) + q];
-            sum = warp_sum_i64(sum);
-            if (lane == 0)
-                out[q] = sum;
+        __shared__ int64_t part[SEG_THREADS / 32];
+        const int q = blockIdx.x;
+        const int QN = G * (1 + V);
+        int64_t sum = 0;
+        for (int t = threadIdx.x; t < ntiles; t += SEG_THREADS)
+            sum += tile_out[(size_t)t * QN + q];
+        sum = warp_sum_i64(sum);
+        if ((threadIdx.x & 31) == 0)
+            part[threadIdx.x >> 5] = sum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t s = 0;
+            for (int w = 0; w < SEG_THREADS / 32; w++)
+                s += part[w];
+            out[q] = s;
         }
     }
 };

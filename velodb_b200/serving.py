@@ -26,7 +26,7 @@ from ._lib import (VeloJoinPred, VeloLineitem, VeloLineitemPred, VeloQuery, Velo
 Q_FILTER_GROUPBY, Q_JOIN_TOPK, Q_JOIN3 = 1, 2, 3
 SHAPE_NAMES = {Q_FILTER_GROUPBY: "filter_groupby", Q_JOIN_TOPK: "join2_topk", Q_JOIN3: "join3_chain"}
 
-FULL_SCALE = dict(fact=60_000_000, dim=15_000_000, fact2=150_000_000)
+FULL_SCALE = dict(fact_n=60_000_000, dim_n=15_000_000, fact2_n=150_000_000)
 
 
 class ServedTables:
@@ -56,7 +56,33 @@ class ServedTables:
                                 self.dim_n, self.fact2_fk.data_ptr(), self.fact2_price.data_ptr(), self.fact2_n)
 
 
-def query_stream(tables: ServedTables, count: int, seed: int = W.SEED_SERVE, lo_log2: float = 16.0,
+class HostSlices:
+    """Host copies of the slices a query reads, generated from the same
+    seeded streams as ``ServedTables`` without building the whole tables (the
+    dimension keys, a permutation, are generated once in full)."""
+
+    def __init__(self, fact_n: int, dim_n: int, fact2_n: int, seed: int = W.SEED_SERVE):
+        self.fact_n, self.dim_n, self.fact2_n, self.seed = fact_n, dim_n, fact2_n, seed
+        self._dim_key = None
+
+    def dim_key(self):
+        if self._dim_key is None:
+            self._dim_key = (W.permutation(self.seed, self.dim_n, 20) + 1).astype(np.int64)
+        return self._dim_key
+
+    def lineitem(self, o: int, n: int) -> dict:
+        return W.lineitem(n, seed=self.seed, start=o)
+
+    def join_inputs(self, q):
+        s, o, n, do, dn = self.seed, q.offset, q.n, q.dim_offset, q.dim_n
+        dim = dict(key=self.dim_key()[do:do + dn].astype(np.int32),
+                   date=W.uniform_int(s, dn, 22, 0, 2556, np.int32, do))
+        fact = dict(fk=W.uniform_int(s, n, 21, 1, self.dim_n, np.int64, o).astype(np.int32),
+                    price=W.uniform_int(s, n, 1, 90_000, 10_500_000, np.int64, o))
+        return dim, fact
+
+
+def query_stream(tables, count: int, seed: int = W.SEED_SERVE, lo_log2: float = 16.0,
                  hi_log2: float = 22.0):
     """Seeded query mix (50 % filter + group-by, 35 % two-way join, 15 %
     three-way chain) with public slice sizes log-uniform in [2^lo, 2^hi]."""

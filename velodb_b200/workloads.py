@@ -24,11 +24,12 @@ SEED_BATCH = 0xB200000000000003
 SEED_SERVE = 0xB200000000000004
 
 
-def splitmix64(seed: int, n: int, stream: int = 0) -> np.ndarray:
-    """n outputs of the splitmix64 generator started at seed + stream*STEP."""
+def splitmix64(seed: int, n: int, stream: int = 0, start: int = 0) -> np.ndarray:
+    """Outputs start..start+n-1 of the splitmix64 generator started at
+    seed + stream*STEP."""
     with np.errstate(over="ignore"):
         base = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + np.uint64(stream) * STREAM_STEP
-        z = base + (np.arange(1, n + 1, dtype=np.uint64) * GAMMA)
+        z = base + (np.arange(start + 1, start + n + 1, dtype=np.uint64) * GAMMA)
         z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         return z ^ (z >> np.uint64(31))
@@ -44,9 +45,9 @@ def lemire(x: np.ndarray, rng: int) -> np.ndarray:
         return (hi * r + ((lo * r) >> np.uint64(32))) >> np.uint64(32)
 
 
-def uniform_int(seed: int, n: int, stream: int, lo: int, hi: int, dtype) -> np.ndarray:
-    """n integers uniform over [lo, hi] (inclusive)."""
-    return (lemire(splitmix64(seed, n, stream), hi - lo + 1).astype(np.int64) + lo).astype(dtype)
+def uniform_int(seed: int, n: int, stream: int, lo: int, hi: int, dtype, start: int = 0) -> np.ndarray:
+    """n integers uniform over [lo, hi] (inclusive), rows start..start+n-1."""
+    return (lemire(splitmix64(seed, n, stream, start), hi - lo + 1).astype(np.int64) + lo).astype(dtype)
 
 
 def permutation(seed: int, n: int, stream: int) -> np.ndarray:
@@ -68,15 +69,16 @@ LINEITEM_PRED = dict(ship_lo=0, ship_hi=2504, disc_lo=10, disc_hi=10, qty_lo=1, 
 LINEITEM_GROUP_BOUND = 8
 
 
-def lineitem(n: int = LINEITEM_ROWS, seed: int = SEED_LINEITEM) -> dict:
+def lineitem(n: int = LINEITEM_ROWS, seed: int = SEED_LINEITEM, start: int = 0) -> dict:
+    """Rows start..start+n-1 of the lineitem-shaped table of `seed`."""
     return dict(
-        qty=uniform_int(seed, n, 0, 1, 50, np.int32),
-        price=uniform_int(seed, n, 1, 90_000, 10_500_000, np.int64),
-        disc=uniform_int(seed, n, 2, 0, 10, np.int32),
-        tax=uniform_int(seed, n, 3, 0, 8, np.int32),
-        shipdate=uniform_int(seed, n, 4, 0, 2556, np.int32),
-        flag1=uniform_int(seed, n, 5, 0, 2, np.uint8),
-        flag2=uniform_int(seed, n, 6, 0, 1, np.uint8),
+        qty=uniform_int(seed, n, 0, 1, 50, np.int32, start),
+        price=uniform_int(seed, n, 1, 90_000, 10_500_000, np.int64, start),
+        disc=uniform_int(seed, n, 2, 0, 10, np.int32, start),
+        tax=uniform_int(seed, n, 3, 0, 8, np.int32, start),
+        shipdate=uniform_int(seed, n, 4, 0, 2556, np.int32, start),
+        flag1=uniform_int(seed, n, 5, 0, 2, np.uint8, start),
+        flag2=uniform_int(seed, n, 6, 0, 1, np.uint8, start),
     )
 
 
