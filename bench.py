@@ -38,8 +38,10 @@ sys.path.insert(0, ROOT)
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu
-# capture (profiles/), or None when not captured for the workload.
-TRAFFIC = {"groupby": None, "sort": None}
+# capture (profiles/k_sort_pass_groupby_rec2_2p23.md: mean of the tile,
+# global and merge passes; profiles/k_sort_pass_kp_2p20_2p24.md), or None when
+# the workload's launch is too large to capture.
+TRAFFIC = {"groupby": 210.1e6, "sort": 12.65e6, "batch": None}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -150,8 +152,8 @@ class GroupBy:
         self.counts_host = torch.empty(2, dtype=torch.int64).pin_memory()
         self.in_bytes = sum(v.numel() * v.element_size() for v in self.pinned.values())
         self.np_rows = 1 << int(np.ceil(np.log2(self.n)))
-        self.rec_bytes = 24
-        self.flush_l2 = False  # inputs (156 MB) and records (201 MB) exceed the 126 MB L2
+        self.rec_bytes = 16  # 2-word records (the predicate's bands fit the packed layout)
+        self.flush_l2 = False  # inputs (156 MB) and records (134 MB) exceed the 126 MB L2
 
     def step(self):
         self.capi.filter_groupby(self.dev, self.n, self.pred, self.G, scratch=self.scratch, out=self.out,
@@ -189,25 +191,30 @@ class GroupBy:
 
     def dominant(self, device):
         """The dominant kernel is the bitonic pass kernel of the pipeline's
-        sort (about 80 % of the step in the ncu launch list).  It is timed
-        here on the pipeline's own record shape and tile configuration:
-        next_pow2(6,001,215) = 2^23 records of 3 u64 words, 4096-row tiles of
-        256 threads.  Every launch reads and writes every record once, so
-        its algorithmic bytes are 2 x 2^23 x 24 B."""
-        torch, capi = self.torch, self.capi
-        from velodb_b200 import workloads as W
-
-        n = self.np_rows
-        src = [capi.to_dev_u64(W.splitmix64(7, n, i)) for i in range(3)]
-        ws = [x.clone() for x in src]
-        logn = int(np.log2(n))
+        sort stage (about 70 % of the step in the ncu launch list).  Its
+        launches are timed inside the pipeline itself: with stage timing on,
+        velo_filter_groupby records CUDA events on its stream around each
+        stage, and the sort stage's time is divided by its launch count.  The
+        records are 2 words (16 B: the predicate's quantity and discount bands
+        fit the packed layout) over next_pow2(6,001,215) = 2^23 rows, and
+        every launch reads and writes every record once: 2 x 2^23 x 16 B."""
+        capi = self.capi
+        logn = int(np.log2(self.np_rows))
         launches = sort_passes(logn, 12, 7)
-
-        def run():
-            capi.osort_records(ws, n, 0xFFFF800000000000, tune=(12, 256))
-
-        return dominant_timing(torch, run, lambda: [a.copy_(b) for a, b in zip(ws, src)], launches,
-                               2 * n * 24, "k_sort_pass<RowRec<3,1>> (bitonic passes, 2^23 x 24 B records)")
+        capi.set_stage_timing(True)
+        ts = []
+        try:
+            for i in range(6):
+                self.step()
+                st = capi.last_stage_times()
+                if i:
+                    ts.append(st[2])
+        finally:
+            capi.set_stage_timing(False)
+        return {"kernel": "k_sort_pass<RowRec<2,1,false,KEY_HI32>,8,4> (bitonic passes of the sort stage, "
+                          "2^23 x 16 B records)",
+                "launches_per_sort": launches, "avg_launch_us": float(np.mean(ts)) * 1e3 / launches,
+                "bytes_per_launch": int(2 * self.np_rows * 16)}
 
 
 def dominant_timing(torch, run, reset, launches, bytes_per_launch, name, reps=5):
@@ -278,7 +285,9 @@ class Batched:
         with torch.cuda.graph(self.graph, stream=self.stream):
             self.batch.launch(stream=self.stream)
         self.pinned = [(torch.from_numpy(h["keys"].view(np.int64)).pin_memory(),
-                        torch.from_numpy(h["pay"].view(np.int32)).pin_memory()) for h in insts]
+                        torch.from_numpy(h["pay"].view(np.int32)).pin_memory(),
+                        torch.from_numpy(h["marks"]).pin_memory() if h["kind"] == "compact" else None)
+                       for h in insts]
         self.count_host = torch.zeros(len(self.items), dtype=torch.int64).pin_memory()
 
     def step(self):
@@ -292,9 +301,11 @@ class Batched:
                 self.capi.ocompact_kpm(it["keys"], it["pay"], it["marks"], it["n"], tune=self.tune)
 
     def step_e2e(self):
-        for it, (k, p) in zip(self.items, self.pinned):
+        for it, (k, p, m) in zip(self.items, self.pinned):
             it["keys"][: it["n"]].copy_(k, non_blocking=True)
             it["pay"][: it["n"]].copy_(p, non_blocking=True)
+            if m is not None:
+                it["marks"][: it["n"]].copy_(m, non_blocking=True)
         self.step()
         for i, it in enumerate(self.items):
             if "count" in it:
@@ -469,6 +480,33 @@ def cpu_baseline_sort(W, orc):
     dt = (time.perf_counter() - t0) / reps
     return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
             "sample": f"full 2^20-row sort, {reps} runs, OpenMP over all cores"}
+
+
+def cpu_baseline_batch(W, orc):
+    """The oracle on instances of the 512 in a fixed stride order until about
+    10 s of CPU work: sorts on all cores, compactions single-threaded."""
+    cores = os.cpu_count() or 1
+    insts = W.batch_instances()
+    rows, t_tot, used = 0, 0.0, 0
+    for i in range(len(insts)):
+        it = insts[(i * 97) % len(insts)]
+        if it["kind"] == "sort":
+            t0 = time.perf_counter()
+            orc.bitonic_kp(it["keys"], it["pay"], n_threads=cores)
+        else:
+            r = np.zeros((it["n"], 16), np.uint8)
+            r[:, :8] = it["keys"].view(np.uint8).reshape(-1, 8)
+            r[:, 8:12] = it["pay"].view(np.uint8).reshape(-1, 4)
+            t0 = time.perf_counter()
+            orc.ocompact(r, it["marks"])
+        t_tot += time.perf_counter() - t0
+        rows += it["n"]
+        used += 1
+        if t_tot > 10.0:
+            break
+    return {"value": rows / t_tot / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
+            "sample": f"{used} of the 512 instances (stride 97 through the list, {rows} rows); sorts on all "
+                      f"cores, compactions single-threaded"}
 
 
 def run_reference(args, rank):
@@ -795,7 +833,8 @@ def main():
         orc.lib()
         line["checked_against_oracle"] = wl.check(orc)
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = (cpu_baseline_groupby if args.workload == "groupby" else cpu_baseline_sort)(W, orc)
+            line["cpu_baseline"] = {"groupby": cpu_baseline_groupby, "sort": cpu_baseline_sort,
+                                    "batch": cpu_baseline_batch}[args.workload](W, orc)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

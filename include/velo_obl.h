@@ -70,6 +70,20 @@ size_t velo_next_pow2(size_t x);
 /* Text of the last error raised on this host thread ("" if none). */
 const char* velo_last_error_text(void);
 
+/*
+ * Stage timing for profilers (off by default; process-wide switch).  While it
+ * is on, the multi-stage pipelines (velo_filter_groupby,
+ * velo_join_groupby_topk) record a CUDA event on their stream before and
+ * after each stage and synchronize that stream before returning; the stage
+ * durations of the calling thread's last such call are then read with
+ * velo_last_stage_times (ms, in stage order; returns how many were written).
+ *   velo_filter_groupby:    pack, compact, sort, aggregate
+ *   velo_join_groupby_topk: pack, sort, fill, compact, aggregate, top-k
+ * No reference counterpart: a measurement hook of this implementation.
+ */
+void velo_set_stage_timing(int on);
+int velo_last_stage_times(float* ms, int capacity);
+
 /* ------------------------------------------------------------------------ */
 /* Bitonic network sort                                                     */
 /* ------------------------------------------------------------------------ */

@@ -56,3 +56,33 @@ def test_filter_groupby_config1_full(cuda, orc):
     cols = W.lineitem()  # 6,001,215 rows
     check(orc, cols, W.LINEITEM_PRED)
     check(orc, cols, W.LINEITEM_PRED, reveal=True)
+
+
+def test_filter_groupby_wide_bands_use_three_word_records(cuda, orc):
+    # bands too wide for the packed two-word layout: the three-word path
+    cols = W.lineitem(70_000, seed=17)
+    check(orc, cols, dict(ship_lo=0, ship_hi=2000, disc_lo=-(1 << 20), disc_hi=1 << 20, qty_lo=-(2**31),
+                          qty_hi=2**31 - 1))
+
+
+def test_filter_groupby_band_edges_in_packed_layout(cuda, orc):
+    # qty band of 10 bits and disc band of 5 bits (15 packed bits, the limit),
+    # with values at both edges of each band
+    n = 20_000
+    rng = np.random.default_rng(4)
+    cols = W.lineitem(n, seed=23)
+    cols["qty"] = rng.choice(np.array([-7, -7 + 1023, 100], np.int32), n)
+    cols["disc"] = rng.choice(np.array([3, 3 + 31, 10], np.int32), n)
+    check(orc, cols, dict(ship_lo=0, ship_hi=2556, disc_lo=3, disc_hi=34, qty_lo=-7, qty_hi=1016))
+
+
+def test_stage_timing_reports_four_stages(cuda):
+    cols = W.lineitem(100_000, seed=3)
+    d = capi.lineitem_to_device(cols)
+    capi.set_stage_timing(True)
+    try:
+        capi.filter_groupby(d, 100_000, W.LINEITEM_PRED)
+        t = capi.last_stage_times()
+    finally:
+        capi.set_stage_timing(False)
+    assert len(t) == 4 and all(x >= 0 for x in t) and sum(t) > 0

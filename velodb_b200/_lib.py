@@ -17,6 +17,8 @@ vp, sz, u32, u64, i32, i64, u8 = C.c_void_p, C.c_size_t, C.c_uint32, C.c_uint64,
 PROTOS = {
     "velo_next_pow2": (sz, [sz]),
     "velo_last_error_text": (C.c_char_p, []),
+    "velo_set_stage_timing": (None, [i32]),
+    "velo_last_stage_times": (i32, [vp, i32]),
     "velo_osort_kp": (i32, [vp, vp, sz, sz, vp, vp]),
     "velo_sort_columns": (i32, [vp, vp, vp, u32, sz, sz, vp, vp, sz, vp]),
     "velo_sort_scratch_bytes": (sz, [vp, u32, sz]),

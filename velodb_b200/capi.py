@@ -21,6 +21,18 @@ def next_pow2(x: int) -> int:
     return int(lib().velo_next_pow2(x))
 
 
+def set_stage_timing(on: bool) -> None:
+    """Switch the pipelines' per-stage CUDA-event timing (velo_set_stage_timing)."""
+    lib().velo_set_stage_timing(1 if on else 0)
+
+
+def last_stage_times() -> list:
+    """Stage durations (ms) of this thread's last timed pipeline call."""
+    buf = np.zeros(8, dtype=np.float32)
+    n = int(lib().velo_last_stage_times(buf.ctypes.data, 8))
+    return [float(x) for x in buf[:n]]
+
+
 def to_dev_u64(a: np.ndarray, capacity: int | None = None, device="cuda") -> torch.Tensor:
     """Upload a uint64 array into an int64 device tensor of `capacity` rows."""
     cap = len(a) if capacity is None else capacity

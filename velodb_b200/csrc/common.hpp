@@ -53,6 +53,56 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // Largest supported padded size: the mark prefix counts are u32.
 constexpr int MAX_LOGN = 31;
 
+// Stage timing (velo_set_stage_timing): events around the stages of one
+// pipeline call on its stream, results stored for the calling thread.
+bool stage_timing_on();
+void store_stage_times(const float* ms, int n);
+
+class StageTimer {
+public:
+    static constexpr int MAX_STAGES = 8;
+    explicit StageTimer(cudaStream_t st) : st_(st), on_(stage_timing_on())
+    {
+        if (!on_)
+            return;
+        for (int i = 0; i <= MAX_STAGES; i++)
+            if (cudaEventCreate(&ev_[i]) != cudaSuccess)
+                on_ = false;
+        if (on_)
+            cudaEventRecord(ev_[0], st_);
+    }
+    // the stage that started at the previous mark ends here
+    void mark()
+    {
+        if (on_ && n_ < MAX_STAGES)
+            cudaEventRecord(ev_[++n_], st_);
+    }
+    // synchronize on the last event and store the stage durations
+    void finish()
+    {
+        if (!on_ || n_ == 0)
+            return;
+        float ms[MAX_STAGES] = {};
+        if (cudaEventSynchronize(ev_[n_]) == cudaSuccess)
+            for (int i = 0; i < n_; i++)
+                cudaEventElapsedTime(&ms[i], ev_[i], ev_[i + 1]);
+        store_stage_times(ms, n_);
+    }
+    ~StageTimer()
+    {
+        if (on_)
+            for (int i = 0; i <= MAX_STAGES; i++)
+                if (ev_[i])
+                    cudaEventDestroy(ev_[i]);
+    }
+
+private:
+    cudaStream_t st_;
+    bool on_;
+    int n_ = 0;
+    cudaEvent_t ev_[MAX_STAGES + 1] = {};
+};
+
 } // namespace velo
 
 #define VELO_CUDA_TRY(call, what)                                                                                      \

@@ -274,12 +274,14 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
         return rc;
     const size_t np = next_pow2(n);
     const int logN = ilog2_floor(np);
+    StageTimer tm(st);
 
     // 1. predicate + pack (+ per-tile pass counts)
     k_li_pack<W><<<s.ntiles_c, 256, 0, st>>>(c, pred, prm, n, s.n_rec, LI_LT, s.w[0], s.w[1], s.w[2], s.counts);
     const int ntiles_np = logN > LI_LT ? 1 << (logN - LI_LT) : 1;
     k_scan_tiles<<<1, 1024, 0, st>>>(s.counts, ntiles_np, s.prefix, s.d_rows);
     VELO_CUDA_TRY(cudaGetLastError(), "pack launch");
+    tm.mark();
 
     typename Rec::Cols rc3;
     for (int i = 0; i < W; i++) {
@@ -300,6 +302,7 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
         if (rc != VELO_OK)
             return rc;
     }
+    tm.mark();
     // 3. sort by group key: all next_pow2(n) rows, or -- when the caller
     // reveals the filtered count like the reference operator -- only
     // next_pow2(count) rows
@@ -318,6 +321,7 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
         if (rc != VELO_OK)
             return rc;
     }
+    tm.mark();
     // 4. segmented sums with public output bound
     size_t nseg = (size_t)1 << logS;
     if (nseg < (size_t)SEG_TS)
@@ -331,6 +335,8 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
     k_seg_finish<<<group_bound * (1 + LI_V), SEG_THREADS, 0, st>>>(s.tile_out, ntiles_s, (int)group_bound, d_out,
                                                                    s.d_rows, s.n_groups, d_counts);
     VELO_CUDA_TRY(cudaGetLastError(), "group-by launch");
+    tm.mark();
+    tm.finish();
     return VELO_OK;
 }
 

@@ -24,8 +24,10 @@
 
 namespace velo {
 
-// ties (fact rows of one key) are aggregated, their order is irrelevant
-using JRec = RowRec<2, 1, false>;
+// ties (fact rows of one key) are aggregated, their order is irrelevant; the
+// union sorts on the whole of w0, whose bits below the (key, tag) pair only
+// refine that order
+using JRec = RowRec<2, 1, false, KEY_FULL>;
 using GRec = RowRec<3, 1, false>;
 using TRec = RowRec<3, 3, false>;
 constexpr uint64_t J_KEYTAG = 0xFFFFFFFF80000000ull;
@@ -348,12 +350,14 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     const int logR = ilog2_floor(s.n_rec);
     const size_t n_union = t->n_dim + t->n_fact;
     const int logU = ilog2_floor(next_pow2(n_union));
+    StageTimer tm(st);
 
     // 1. pack
     const unsigned blocks = 148 * 8;
     k_join_pack<<<blocks, 256, 0, st>>>(t->dim_key, t->dim_date, t->n_dim, t->fact_fk, t->fact_price, t->n_fact,
                                         pred->date_hi, pred->price_hi, s.n_rec, s.u[0], s.u[1]);
     VELO_CUDA_TRY(cudaGetLastError(), "join pack launch");
+    tm.mark();
     JRec::Cols uc;
     uc.w[0] = s.u[0];
     uc.w[1] = s.u[1];
@@ -370,12 +374,14 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
         if (rc != VELO_OK)
             return rc;
     }
+    tm.mark();
     // 3. forward fill of the dimension side -> joined flag
     const int ntf = (int)(s.n_rec / FILL_TS);
     k_fill_summary<<<ntf, FILL_THREADS, 0, st>>>(s.u[0], s.tile_last);
     k_fill_carries<<<1, 1024, 0, st>>>(s.tile_last, ntf, s.fcarry);
     k_fill_apply<<<ntf, FILL_THREADS, 0, st>>>(s.u[0], s.fcarry);
     VELO_CUDA_TRY(cudaGetLastError(), "join fill launch");
+    tm.mark();
     // 4. ORCompact of the joined fact rows
     {
         const int ntc = logR > J_LT ? 1 << (logR - J_LT) : 1;
@@ -387,6 +393,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
         if (rc != VELO_OK)
             return rc;
     }
+    tm.mark();
     // 5. group-by fk over the joined prefix (already in fk order: the
     // compaction keeps the sorted order of the joined rows)
     const int nts = (int)(s.n_rec / SEG_TS);
@@ -414,6 +421,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
         if (rc != VELO_OK)
             return rc;
     }
+    tm.mark();
     // 6. top-k: sort the first next_pow2(n_dim) group records (the public
     // bound on the number of groups) on (sum desc, fk asc)
     const size_t n_top = s.n_top;
@@ -442,5 +450,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     VELO_CUDA_TRY(cudaGetLastError(), "top-k launch");
     if (kk < k)
         VELO_CUDA_TRY(cudaMemsetAsync(d_out + kk * 3, 0, (k - kk) * 3 * 8, st), "cudaMemsetAsync");
+    tm.mark();
+    tm.finish();
     return VELO_OK;
 }

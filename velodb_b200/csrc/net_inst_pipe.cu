@@ -1,0 +1,13 @@
+// Instantiations of the network passes for the pipeline records: the filter +
+// group-by records (2 or 3 words ordered on the high 32 bits of word 0) and
+// the join union records (2 words ordered on the whole of word 0).
+#include "net_impl.cuh"
+
+using LiRec2 = velo::RowRec<2, 1, false, velo::KEY_HI32>;
+using LiRec3 = velo::RowRec<3, 1, false, velo::KEY_HI32>;
+
+VELO_INSTANTIATE_NET(LiRec2, 8, 4)
+VELO_INSTANTIATE_NET(LiRec3, 8, 4)
+
+using JoinRec = velo::RowRec<2, 1, false, velo::KEY_FULL>;
+VELO_INSTANTIATE_NET(JoinRec, 8, 4)

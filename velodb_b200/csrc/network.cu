@@ -1,6 +1,7 @@
 // Plain-path entry points of the two networks for (u64 key, u32 payload)
 // rows: velo_osort_kp and velo_ocompact_kpm.
 #include <mutex>
+#include <atomic>
 #include <string>
 
 #include "net_host.cuh"
@@ -71,6 +72,29 @@ using namespace velo;
 extern "C" size_t velo_next_pow2(size_t x)
 {
     return next_pow2(x);
+}
+
+static std::atomic<int> g_stage_timing { 0 };
+static thread_local float g_stage_ms[velo::StageTimer::MAX_STAGES];
+static thread_local int g_stage_n = 0;
+
+bool velo::stage_timing_on() { return g_stage_timing.load(std::memory_order_relaxed) != 0; }
+
+void velo::store_stage_times(const float* ms, int n)
+{
+    g_stage_n = n;
+    for (int i = 0; i < n; i++)
+        g_stage_ms[i] = ms[i];
+}
+
+extern "C" void velo_set_stage_timing(int on) { g_stage_timing.store(on ? 1 : 0, std::memory_order_relaxed); }
+
+extern "C" int velo_last_stage_times(float* ms, int capacity)
+{
+    const int n = capacity < g_stage_n ? capacity : g_stage_n;
+    for (int i = 0; ms && i < n; i++)
+        ms[i] = g_stage_ms[i];
+    return ms ? n : g_stage_n;
 }
 
 extern "C" const char* velo_last_error_text(void)
