@@ -193,6 +193,54 @@ velo_status velo_enrich_positions(const uint32_t* d_record_ids, const uint32_t* 
                                   void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Device memory and streams (for host code above the ABI)                   */
+/* ------------------------------------------------------------------------ */
+
+enum { VELO_COPY_H2D = 1, VELO_COPY_D2H = 2, VELO_COPY_D2D = 3 };
+/* Stream-ordered allocation (cudaMallocAsync); VELO_ENOMEM when the device is
+ * full.  bytes == 0 gives NULL. */
+velo_status velo_device_alloc(size_t bytes, void* stream, void** out);
+velo_status velo_device_free(void* p, void* stream);
+/* Stream-ordered copy; kind is VELO_COPY_*. */
+velo_status velo_copy(void* dst, const void* src, size_t bytes, uint32_t kind, void* stream);
+velo_status velo_memset(void* dst, int value, size_t bytes, void* stream);
+velo_status velo_stream_sync(void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Column helpers of the operator layer                                     */
+/* ------------------------------------------------------------------------ */
+
+/* d_mask[i] = (lo <= col[i] <= hi), or AND-ed into d_mask when combine != 0:
+ * the conjunctive range predicates SeqScanOperator pushes down
+ * (src/operator/seq_scan_operator.cpp:38-45), evaluated on the device.
+ * Integer, BOOLEAN and DATE columns; one pass, every row read. */
+velo_status velo_range_mask(const void* d_col, uint32_t type, size_t n, int64_t lo, int64_t hi, uint8_t* d_mask,
+                            uint32_t combine, void* stream);
+/* d_out[i] = start + i (the $_rowid column of a scan). */
+velo_status velo_iota_i64(int64_t* d_out, size_t n, int64_t start, void* stream);
+/* Oblivious in-place compaction of n_cols typed columns (and their validity
+ * bytes, d_valid[c] may be NULL) by d_mask: the rows with mask != 0 move to
+ * [0, *d_count) in input order.  ORCompact over next_pow2(n) rows, two columns
+ * per network run; the exchanges depend only on n.  Replaces OP_SCATTER +
+ * OP_GATHER of FilterCompactionOperator
+ * (src/operator/filter_compaction_operator.cpp:65-184), whose scatter
+ * addresses follow the data. */
+size_t velo_ocompact_columns_scratch_bytes(size_t n);
+velo_status velo_ocompact_columns(void* const* d_cols, const uint32_t* types, uint8_t* const* d_valid,
+                                  uint32_t n_cols, const uint8_t* d_mask, size_t n, uint64_t* d_count,
+                                  void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* Oblivious typed gather of one column with validity (materialization):
+ * out[j] = col[rowid[j]] and out_valid[j] = valid[rowid[j]] for 0 <= rowid[j]
+ * < table_n, else 0 / not valid.  Built on velo_ogather_u64 (one sort-based
+ * gather, two for 8-byte types when out_valid is wanted); the addresses
+ * depend only on table_n and n. */
+size_t velo_ogather_column_scratch_bytes(size_t table_n, size_t n);
+velo_status velo_ogather_column(const void* d_table_col, uint32_t type, const uint8_t* d_table_valid,
+                                size_t table_n, const int64_t* d_rowids, size_t n, void* d_out,
+                                uint8_t* d_out_valid, void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Oblivious shuffle, gather and PK-FK join                                 */
 /* ------------------------------------------------------------------------ */
 

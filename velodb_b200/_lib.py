@@ -18,6 +18,17 @@ PROTOS = {
     "velo_next_pow2": (sz, [sz]),
     "velo_last_error_text": (C.c_char_p, []),
     "velo_set_stage_timing": (None, [i32]),
+    "velo_device_alloc": (i32, [sz, vp, vp]),
+    "velo_device_free": (i32, [vp, vp]),
+    "velo_copy": (i32, [vp, vp, sz, u32, vp]),
+    "velo_memset": (i32, [vp, i32, sz, vp]),
+    "velo_stream_sync": (i32, [vp]),
+    "velo_range_mask": (i32, [vp, u32, sz, i64, i64, vp, u32, vp]),
+    "velo_iota_i64": (i32, [vp, sz, i64, vp]),
+    "velo_ocompact_columns_scratch_bytes": (sz, [sz]),
+    "velo_ocompact_columns": (i32, [vp, vp, vp, u32, vp, sz, vp, vp, sz, vp]),
+    "velo_ogather_column_scratch_bytes": (sz, [sz, sz]),
+    "velo_ogather_column": (i32, [vp, u32, vp, sz, vp, sz, vp, vp, vp, sz, vp]),
     "velo_last_stage_times": (i32, [vp, i32]),
     "velo_osort_kp": (i32, [vp, vp, sz, sz, vp, vp]),
     "velo_sort_columns": (i32, [vp, vp, vp, u32, sz, sz, vp, vp, sz, vp]),

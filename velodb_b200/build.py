@@ -20,6 +20,9 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libvelo_obl.so")
+HOST = os.path.join(PKG, "host")
+OPS_LIB = os.path.join(PKG, "libvelo_operators.so")
+CXX = os.environ.get("VELO_CXX", "g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -65,7 +68,25 @@ def build(verbose: bool = False, extra_flags=None) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_operators(verbose)
     return LIB
+
+
+def build_operators(verbose: bool = False) -> str:
+    """The C++ operator layer (host/*.cpp) as libvelo_operators.so, linked
+    against libvelo_obl.so only (no CUDA headers or runtime of its own)."""
+    srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
+    deps = srcs + [os.path.join(INCLUDE, "velo_operator.hpp"), os.path.join(INCLUDE, "velo_obl.h"), LIB]
+    if os.path.exists(OPS_LIB) and all(os.path.getmtime(d) <= os.path.getmtime(OPS_LIB) for d in deps):
+        return OPS_LIB
+    if verbose:
+        print("compiling: " + ", ".join(os.path.basename(x) for x in srcs), file=sys.stderr)
+    cmd = [CXX, "-std=c++17", "-O2", "-g", "-fPIC", "-shared", "-Wall", "-Wextra", "-I", INCLUDE] + srcs + \
+        ["-L", PKG, "-lvelo_obl", "-Wl,-rpath,$ORIGIN", "-o", OPS_LIB]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"operator layer build failed:\n{r.stdout}\n{r.stderr}")
+    return OPS_LIB
 
 
 if __name__ == "__main__":
