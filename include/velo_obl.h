@@ -207,6 +207,21 @@ velo_status velo_memset(void* dst, int value, size_t bytes, void* stream);
 velo_status velo_stream_sync(void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Address-trace recording (obliviousness tests)                            */
+/* ------------------------------------------------------------------------ */
+
+/* Only the test build libvelo_obl_trace.so (compiled with VELO_TRACE)
+ * records; the product library returns VELO_ENOTSUP and velo_trace_enabled
+ * 0.  Between begin and end, every instrumented global load/store folds
+ * (site, address) into a hash chain per logical thread (slots of them) and
+ * every instrumented kernel logs (kernel id, grid, block, dynamic smem).  No
+ * reference counterpart. */
+int velo_trace_enabled(void);
+velo_status velo_trace_begin(uint64_t slots, uint64_t launch_capacity);
+velo_status velo_trace_end(uint64_t* chain_digest, uint64_t* touched, uint64_t* launches, uint64_t launch_capacity,
+                           uint64_t* n_launches);
+
+/* ------------------------------------------------------------------------ */
 /* Column helpers of the operator layer                                     */
 /* ------------------------------------------------------------------------ */
 

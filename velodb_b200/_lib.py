@@ -18,6 +18,9 @@ PROTOS = {
     "velo_next_pow2": (sz, [sz]),
     "velo_last_error_text": (C.c_char_p, []),
     "velo_set_stage_timing": (None, [i32]),
+    "velo_trace_enabled": (i32, []),
+    "velo_trace_begin": (i32, [u64, u64]),
+    "velo_trace_end": (i32, [vp, vp, vp, u64, vp]),
     "velo_device_alloc": (i32, [sz, vp, vp]),
     "velo_device_free": (i32, [vp, vp]),
     "velo_copy": (i32, [vp, vp, sz, u32, vp]),

@@ -22,6 +22,8 @@ BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libvelo_obl.so")
 HOST = os.path.join(PKG, "host")
 OPS_LIB = os.path.join(PKG, "libvelo_operators.so")
+TRACE_LIB = os.path.join(PKG, "libvelo_obl_trace.so")
+TRACE_BUILD = os.path.join(PKG, "_build_trace")
 CXX = os.environ.get("VELO_CXX", "g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
@@ -42,8 +44,8 @@ def _stale(obj, src, hdr_mtime):
     return os.path.getmtime(src) > m or hdr_mtime > m
 
 
-def _compile(src, extra):
-    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+def _compile(src, extra, build_dir=BUILD):
+    obj = os.path.join(build_dir, os.path.basename(src) + ".o")
     cmd = [NVCC] + ARCH + CFLAGS + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -51,25 +53,36 @@ def _compile(src, extra):
     return obj
 
 
-def build(verbose: bool = False, extra_flags=None) -> str:
-    """Compile stale sources and relink.  Returns the library path."""
-    os.makedirs(BUILD, exist_ok=True)
+def _build_lib(lib, build_dir, extra, link_extra, verbose):
+    os.makedirs(build_dir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     hdr_mtime = max([os.path.getmtime(h) for h in _headers()] + [os.path.getmtime(__file__)])
-    extra = list(extra_flags or [])
-    todo = [s for s in srcs if _stale(os.path.join(BUILD, os.path.basename(s) + ".o"), s, hdr_mtime)]
+    todo = [s for s in srcs if _stale(os.path.join(build_dir, os.path.basename(s) + ".o"), s, hdr_mtime)]
     if verbose and todo:
         print("compiling:", ", ".join(os.path.basename(s) for s in todo), file=sys.stderr)
     with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 4))) as ex:
-        list(ex.map(lambda s: _compile(s, extra), todo))
-    objs = [os.path.join(BUILD, os.path.basename(s) + ".o") for s in srcs]
-    if todo or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs
+        list(ex.map(lambda s: _compile(s, extra, build_dir), todo))
+    objs = [os.path.join(build_dir, os.path.basename(s) + ".o") for s in srcs]
+    if todo or not os.path.exists(lib) or any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
+        cmd = [NVCC] + ARCH + link_extra + ["-shared", "-o", lib] + objs
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return lib
+
+
+def build(verbose: bool = False, extra_flags=None) -> str:
+    """Compile stale sources and relink.  Returns the library path."""
+    _build_lib(LIB, BUILD, list(extra_flags or []), [], verbose)
     build_operators(verbose)
     return LIB
+
+
+def build_trace(verbose: bool = False) -> str:
+    """The address-trace test library libvelo_obl_trace.so: the same sources
+    with -DVELO_TRACE, as relocatable device code so that the trace buffers
+    are one set of device globals for every translation unit."""
+    return _build_lib(TRACE_LIB, TRACE_BUILD, ["-DVELO_TRACE", "-rdc=true"], ["-rdc=true"], verbose)
 
 
 def build_operators(verbose: bool = False) -> str:
@@ -91,3 +104,5 @@ def build_operators(verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(verbose=True))
+    if "--trace" in sys.argv:
+        print(build_trace(verbose=True))

@@ -96,7 +96,8 @@ __device__ __forceinline__ int64_t load_int(const void* p, uint32_t type, size_t
 __global__ void k_range_mask(const void* col, uint32_t type, size_t n, int64_t lo, int64_t hi, uint8_t* mask,
                              int combine)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_range_mask"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x) {
         const int64_t v = load_int(col, type, i);
         const uint8_t in = (v >= lo) & (v <= hi);
         mask[i] = combine ? (uint8_t)(mask[i] & in) : in;
@@ -105,13 +106,15 @@ __global__ void k_range_mask(const void* col, uint32_t type, size_t n, int64_t l
 
 __global__ void k_iota_i64(int64_t* out, size_t n, int64_t start)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    VELO_TRACE_KERNEL(velo_site_hash("k_iota_i64"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x)
         out[i] = start + (int64_t)i;
 }
 
 // per-tile counts of marked rows (rows >= n unmarked)
 __global__ void __launch_bounds__(256) k_mask_tile_counts(const uint8_t* mask, size_t n, int lt, uint32_t* counts)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_mask_tile_counts"));
     __shared__ uint32_t tmp[33];
     const size_t base = (size_t)blockIdx.x << lt;
     uint32_t cnt = 0;
@@ -136,7 +139,8 @@ struct ColPair {
 __global__ void k_pack_pair(ColPair p, const uint8_t* mask, size_t n, size_t np, uint64_t* w0, uint64_t* w1,
                             uint64_t* w2)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < np; i += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_pack_pair"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, np); i += (size_t)gridDim.x * blockDim.x) {
         uint64_t a = 0, b = 0, m = 0;
         if (i < n) {
             a = p.ba ? load_bits(p.a, p.ba, i) : 0;
@@ -160,7 +164,8 @@ struct ColPairOut {
 
 __global__ void k_unpack_pair(ColPairOut p, size_t n, const uint64_t* w0, const uint64_t* w1, const uint64_t* w2)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_unpack_pair"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x) {
         const uint64_t m = w2[i];
         if (p.ba)
             store_bits(p.a, p.ba, i, w0[i]);
@@ -315,7 +320,8 @@ namespace velo {
 // in bit 32; 8-byte values are widened alone (validity gathered separately)
 __global__ void k_widen_col(const void* col, int bytes, const uint8_t* valid, size_t n, uint64_t* out)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_widen_col"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x) {
         const uint64_t v = load_bits(col, bytes, i);
         const uint64_t ok = valid ? (valid[i] != 0) : 1;
         out[i] = bytes < 8 ? (v | (ok << 32)) : v;
@@ -324,14 +330,16 @@ __global__ void k_widen_col(const void* col, int bytes, const uint8_t* valid, si
 
 __global__ void k_widen_valid(const uint8_t* valid, size_t n, uint64_t* out)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    VELO_TRACE_KERNEL(velo_site_hash("k_widen_valid"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x)
         out[i] = valid ? (valid[i] != 0) : 1;
 }
 
 // row ids -> u32 request ids; negative or >= table_n requests no row
 __global__ void k_rowids_u32(const int64_t* rid, size_t n, size_t table_n, uint32_t* out)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_rowids_u32"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x) {
         const int64_t r = rid[i];
         out[i] = (r >= 0 && (uint64_t)r < table_n) ? (uint32_t)r : 0xFFFFFFFFu;
     }
@@ -339,7 +347,8 @@ __global__ void k_rowids_u32(const int64_t* rid, size_t n, size_t table_n, uint3
 
 __global__ void k_narrow_col(const uint64_t* w, size_t n, int bytes, void* out, uint8_t* out_valid)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_narrow_col"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x) {
         const uint64_t x = w[i];
         store_bits(out, bytes, i, bytes < 8 ? (x & 0xFFFFFFFFull) : x);
         if (bytes < 8 && out_valid)
@@ -349,7 +358,8 @@ __global__ void k_narrow_col(const uint64_t* w, size_t n, int bytes, void* out, 
 
 __global__ void k_narrow_valid(const uint64_t* w, size_t n, uint8_t* out_valid)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    VELO_TRACE_KERNEL(velo_site_hash("k_narrow_valid"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x)
         out_valid[i] = (uint8_t)(w[i] & 1);
 }
 

@@ -25,6 +25,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "trace.cuh"
 #include "velo_obl.h"
 
 namespace velo {
@@ -152,11 +153,13 @@ struct RowKP {
     static constexpr int SWZ_BITS = 3;
     __device__ __forceinline__ static RowKP load(const Cols& c, size_t g)
     {
+        VELO_TRACE_AT(TS_ROW_LOAD, c.k + g);
         const uint64_t k = __ldcg(c.k + g);
         return RowKP { lo32(k), hi32(k), __ldcg(c.p + g) };
     }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowKP& r)
     {
+        VELO_TRACE_AT(TS_ROW_STORE, c.k + g);
         c.k[g] = ((uint64_t)r.kh << 32) | r.kl;
         c.p[g] = r.p;
     }
@@ -197,11 +200,13 @@ struct RowKPM {
     static constexpr int SWZ_BITS = 3;
     __device__ __forceinline__ static RowKPM load(const Cols& c, size_t g)
     {
+        VELO_TRACE_AT(TS_ROW_LOAD, c.k + g);
         const uint64_t k = __ldcg(c.k + g);
         return RowKPM { lo32(k), hi32(k), __ldcg(c.p + g), (uint32_t)__ldcg(c.m + g) };
     }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowKPM& r)
     {
+        VELO_TRACE_AT(TS_ROW_STORE, c.k + g);
         c.k[g] = ((uint64_t)r.kh << 32) | r.kl;
         c.p[g] = r.p;
         c.m[g] = (uint8_t)r.m;
@@ -254,6 +259,7 @@ struct RowRec {
     static constexpr int SWZ_BITS = W == 1 ? 4 : 3;
     __device__ __forceinline__ static RowRec load(const Cols& c, size_t g)
     {
+        VELO_TRACE_AT(TS_ROW_LOAD, c.w[0] + g);
         RowRec r;
 #pragma unroll
         for (int i = 0; i < W; i++)
@@ -262,6 +268,7 @@ struct RowRec {
     }
     __device__ __forceinline__ static void store(const Cols& c, size_t g, const RowRec& r)
     {
+        VELO_TRACE_AT(TS_ROW_STORE, c.w[0] + g);
 #pragma unroll
         for (int i = 0; i < W; i++)
             c.w[i][g] = r.w[i];

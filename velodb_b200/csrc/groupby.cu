@@ -103,6 +103,7 @@ __global__ void __launch_bounds__(256) k_li_pack(LiCols c, velo_lineitem_pred p,
                                                  size_t n_rec, int lt, uint64_t* w0, uint64_t* w1, uint64_t* w2,
                                                  uint32_t* counts)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_li_pack"));
     __shared__ uint32_t tmp[33];
     const size_t base = (size_t)blockIdx.x << lt;
     const int T = 1 << lt;
@@ -111,8 +112,10 @@ __global__ void __launch_bounds__(256) k_li_pack(LiCols c, velo_lineitem_pred p,
         const size_t g = base + i;
         if (g >= n_rec)
             break;
+        VELO_TRACE_AT(TS_LI_OUT, w0 + g);
         uint64_t r0 = ~0ull, r1 = ~0ull, r2 = ~0ull;
         if (g < n) {
+            VELO_TRACE_AT(TS_LI_IN, c.qty + g);
             const int32_t q = c.qty[g], d = c.disc[g], t = c.tax[g], s = c.ship[g];
             const int64_t pr = c.price[g];
             const uint8_t a = c.f1[g], b = c.f2[g];
@@ -145,6 +148,7 @@ template <int W>
 __global__ void __launch_bounds__(SEG_THREADS) k_seg_summary(typename LiTypes<W>::Rec::Cols c, SegTileAgg* aggs,
                                                              int64_t* runs, LiParams prm)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_seg_summary"));
     extern __shared__ __align__(16) char sm[];
     LiTypes<W>::Seg::tile_summary(c.w, blockIdx.x, aggs, runs, prm, sm);
 }
@@ -153,6 +157,7 @@ template <int W>
 __global__ void __launch_bounds__(1024) k_seg_carries(const SegTileAgg* aggs, const int64_t* runs, int ntiles,
                                                       int64_t* carry_in, uint32_t* tail_prefix, uint64_t* n_groups)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_seg_carries"));
     extern __shared__ __align__(16) char sm[];
     LiTypes<W>::Seg::carries(aggs, runs, ntiles, carry_in, tail_prefix, n_groups, sm);
 }
@@ -163,6 +168,7 @@ __global__ void __launch_bounds__(SEG_THREADS) k_seg_emit(typename LiTypes<W>::R
                                                           const uint32_t* tail_prefix, int G, int64_t* tile_out,
                                                           LiParams prm)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_seg_emit"));
     extern __shared__ __align__(16) char sm[];
     LiTypes<W>::Seg::emit(c.w, blockIdx.x, ntiles, aggs, carry_in, tail_prefix, G, tile_out, prm, sm);
 }
@@ -172,6 +178,7 @@ __global__ void __launch_bounds__(SEG_THREADS) k_seg_finish(const int64_t* tile_
                                                             const uint64_t* d_rows, const uint64_t* n_groups,
                                                             uint64_t* d_counts)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_seg_finish"));
     LiTypes<3>::Seg::finish(tile_out, ntiles, G, out);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         d_counts[0] = *d_rows;

@@ -58,7 +58,8 @@ __global__ void __launch_bounds__(256) k_join_pack(const int32_t* dk, const int3
                                                    const int64_t* fp, size_t nf, int32_t date_hi, int64_t price_hi,
                                                    size_t n_rec, uint64_t* w0, uint64_t* w1)
 {
-    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < n_rec; g += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_join_pack"));
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(g, n_rec); g += (size_t)gridDim.x * blockDim.x) {
         uint64_t a = ~0ull, b = ~0ull;
         if (g < nd) {
             const uint64_t key = (uint32_t)dk[g] ^ 0x80000000u;
@@ -98,6 +99,7 @@ constexpr int FILL_TS = 2048, FILL_THREADS = 256, FILL_RPT = FILL_TS / FILL_THRE
 
 __global__ void __launch_bounds__(FILL_THREADS) k_fill_summary(const uint64_t* w0, DimCarry* tile_last)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_summary"));
     // the tile's last dimension row: every thread keeps the last one of its
     // stride (rows are visited in increasing order), then a max-index
     // reduction picks the overall last
@@ -107,6 +109,7 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_summary(const uint64_t* w
     DimCarry c { 0, 0, 0 };
     int last = -1;
     for (int i = threadIdx.x; i < FILL_TS; i += FILL_THREADS) {
+        VELO_TRACE_AT(TS_FILL, w0 + base + i);
         const DimCarry d = dim_of(w0[base + i]);
         c = dim_combine(c, d);
         last = d.has ? i : last;
@@ -130,12 +133,15 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_summary(const uint64_t* w
 // exclusive "last dimension row" scan over tiles; one CTA of 1024 threads
 __global__ void __launch_bounds__(1024) k_fill_carries(const DimCarry* tile_last, int ntiles, DimCarry* carry)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_carries"));
     __shared__ DimCarry sm[1024];
     const int per = (ntiles + 1023) / 1024;
     const int t0 = threadIdx.x * per, t1 = min(ntiles, t0 + per);
     DimCarry c { 0, 0, 0 };
-    for (int t = t0; t < t1; t++)
+    for (int t = t0; t < t1; t++) {
+        VELO_TRACE_AT(TS_FILL, tile_last + t);
         c = dim_combine(c, tile_last[t]);
+    }
     sm[threadIdx.x] = c;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {
@@ -153,11 +159,14 @@ __global__ void __launch_bounds__(1024) k_fill_carries(const DimCarry* tile_last
 
 __global__ void __launch_bounds__(FILL_THREADS) k_fill_apply(uint64_t* w0, const DimCarry* carry)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_apply"));
     __shared__ uint64_t sw[FILL_TS];
     __shared__ DimCarry st[FILL_THREADS];
     const size_t base = (size_t)blockIdx.x * FILL_TS;
-    for (int i = threadIdx.x; i < FILL_TS; i += FILL_THREADS)
+    for (int i = threadIdx.x; i < FILL_TS; i += FILL_THREADS) {
+        VELO_TRACE_AT(TS_FILL, w0 + base + i);
         sw[i] = w0[base + i];
+    }
     __syncthreads();
     const int r0 = threadIdx.x * FILL_RPT;
     DimCarry mine { 0, 0, 0 };
@@ -182,8 +191,10 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_apply(uint64_t* w0, const
         sw[r0 + r] = (a & ~J_JOINED) | (joined ? J_JOINED : 0ull);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < FILL_TS; i += FILL_THREADS)
+    for (int i = threadIdx.x; i < FILL_TS; i += FILL_THREADS) {
+        VELO_TRACE_AT(TS_FILL, w0 + base + i);
         w0[base + i] = sw[i];
+    }
 }
 
 // ---- group records -> top-k sort records ------------------------------------
@@ -192,7 +203,8 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_apply(uint64_t* w0, const
 __global__ void k_topk_pack(const uint64_t* g0, const uint64_t* g1, const uint64_t* g2, size_t n, uint64_t* t0,
                             uint64_t* t1, uint64_t* t2)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_topk_pack"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x) {
         const uint64_t a = g0[i];
         t0[i] = a & (1ull << 63);
         t1[i] = ~(g1[i] ^ 0x8000000000000000ull);
@@ -203,7 +215,9 @@ __global__ void k_topk_pack(const uint64_t* g0, const uint64_t* g1, const uint64
 __global__ void k_topk_out(const uint64_t* t0, const uint64_t* t1, const uint64_t* t2, size_t k, int64_t* out,
                            const uint64_t* n_groups, const uint64_t* n_joined, uint64_t* d_counts)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_topk_out"));
     for (size_t i = threadIdx.x; i < k; i += blockDim.x) {
+        VELO_TRACE_AT(TS_TOPK, t0 + i);
         const bool ok = (t0[i] >> 63) == 0;
         out[i * 3 + 0] = ok ? (int64_t)(int32_t)((uint32_t)(t2[i] >> 32) ^ 0x80000000u) : 0;
         out[i * 3 + 1] = ok ? (int64_t)(~t1[i] ^ 0x8000000000000000ull) : 0;
@@ -217,6 +231,7 @@ __global__ void k_topk_out(const uint64_t* t0, const uint64_t* t1, const uint64_
 
 __global__ void __launch_bounds__(SEG_THREADS) k_jseg_summary(JRec::Cols c, SegTileAgg* aggs, int64_t* runs)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_jseg_summary"));
     extern __shared__ __align__(16) char sm[];
     JSeg::tile_summary(c.w, blockIdx.x, aggs, runs, JoinAgg::Params {}, sm);
 }
@@ -224,6 +239,7 @@ __global__ void __launch_bounds__(SEG_THREADS) k_jseg_summary(JRec::Cols c, SegT
 __global__ void __launch_bounds__(1024) k_jseg_carries(const SegTileAgg* aggs, const int64_t* runs, int ntiles,
                                                        int64_t* carry_in, uint32_t* tail_prefix, uint64_t* n_groups)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_jseg_carries"));
     extern __shared__ __align__(16) char sm[];
     JSeg::carries(aggs, runs, ntiles, carry_in, tail_prefix, n_groups, sm);
 }
@@ -231,6 +247,7 @@ __global__ void __launch_bounds__(1024) k_jseg_carries(const SegTileAgg* aggs, c
 __global__ void __launch_bounds__(SEG_THREADS) k_jseg_emit_rows(JRec::Cols c, int ntiles, const SegTileAgg* aggs,
                                                                 const int64_t* carry_in, GRec::Cols g)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_jseg_emit_rows"));
     extern __shared__ __align__(16) char sm[];
     JSeg::emit_rows(c.w, blockIdx.x, ntiles, aggs, carry_in, g.w, JoinAgg::Params {}, sm);
 }

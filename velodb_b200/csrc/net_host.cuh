@@ -14,6 +14,7 @@ template <class R>
 __global__ void __launch_bounds__(256) k_count_marks(typename R::Cols c, size_t n, int LT, uint32_t* counts)
 {
     __shared__ uint32_t tmp[33];
+    VELO_TRACE_KERNEL(TS_K_COUNT_MARKS);
     count_tile<R>(c, n, LT, blockIdx.x, counts, tmp);
 }
 
@@ -60,7 +61,12 @@ inline velo_status ensure_smem(Kern kern, size_t bytes, int (&done)[64])
     VELO_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
     if (dev >= 0 && dev < 64 && done[dev])
         return VELO_OK;
-    VELO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+    // static shared memory counts against the same per-CTA limit
+    cudaFuncAttributes fa {};
+    VELO_CUDA_TRY(cudaFuncGetAttributes(&fa, kern), "cudaFuncGetAttributes");
+    const size_t room = MAX_SMEM_BYTES > fa.sharedSizeBytes ? MAX_SMEM_BYTES - fa.sharedSizeBytes : 0;
+    VELO_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(bytes < room ? bytes : room)),
                   "cudaFuncSetAttribute");
     if (dev >= 0 && dev < 64)
         done[dev] = 1;

@@ -17,6 +17,7 @@ __global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<LOG_NT>())
     k_sort_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];
+    VELO_TRACE_KERNEL(TS_K_SORT_PASS);
     Net<R, LOG_NT, LOG_E>::template run<true>(c, g, p, tile_prefix, blockIdx.x, sm);
 }
 
@@ -25,6 +26,7 @@ __global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<LOG_NT>())
     k_compact_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];
+    VELO_TRACE_KERNEL(TS_K_COMPACT_PASS);
     Net<R, LOG_NT, LOG_E>::template run<false>(c, g, p, tile_prefix, blockIdx.x, sm);
 }
 

@@ -18,6 +18,7 @@ void set_error(const std::string& msg)
 __global__ void k_scan_tiles(const uint32_t* counts, int ntiles, uint32_t* prefix, uint64_t* d_count)
 {
     __shared__ uint32_t tmp[33];
+    VELO_TRACE_KERNEL(TS_K_SCAN_TILES);
     scan_tiles(counts, ntiles, prefix, d_count, tmp);
 }
 

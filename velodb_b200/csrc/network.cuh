@@ -49,12 +49,17 @@ struct MarkAt<RowKP> {
 };
 template <>
 struct MarkAt<RowKPM> {
-    __device__ __forceinline__ static bool get(const RowKPM::Cols& c, size_t g) { return __ldcg(c.m + g) != 0; }
+    __device__ __forceinline__ static bool get(const RowKPM::Cols& c, size_t g)
+    {
+        VELO_TRACE_AT(TS_MARK_LOAD, c.m + g);
+        return __ldcg(c.m + g) != 0;
+    }
 };
 template <int W, int KW, bool S, int KM>
 struct MarkAt<RowRec<W, KW, S, KM>> {
     __device__ __forceinline__ static bool get(const typename RowRec<W, KW, S, KM>::Cols& c, size_t g)
     {
+        VELO_TRACE_AT(TS_MARK_LOAD, c.w[c.mark_word] + g);
         return (((__ldcg(c.w[c.mark_word] + g) >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
     }
 };
@@ -403,6 +408,7 @@ struct Net {
                 for (int e = 0; e < E; e++)
                     pre[tp0 | e] = base + m[e];
                 __syncthreads();
+                VELO_TRACE_AT(TS_TILE_PREFIX, tile_prefix + cta);
                 const uint32_t p_tile = __ldcg(tile_prefix + cta);
                 int b = 0;
                 while (b < p.K) {
@@ -434,8 +440,10 @@ struct Net {
                 {
                     const int lo_bits = b_lo - C;
                     const size_t t_hi = ((size_t)(cta >> lo_bits)) << (p.b_hi + 1 - LT);
-                    for (int m = threadIdx.x; m < (1 << p.L); m += TL::NT)
+                    for (int m = threadIdx.x; m < (1 << p.L); m += TL::NT) {
+                        VELO_TRACE_AT(TS_TILE_PREFIX, tile_prefix + (t_hi | ((size_t)m << (b_lo - LT))));
                         gpre[m] = __ldcg(tile_prefix + (t_hi | ((size_t)m << (b_lo - LT))));
+                    }
                     __syncthreads();
                 }
                 int lb = C;
@@ -500,8 +508,10 @@ __device__ __forceinline__ void count_tile(const typename R::Cols& c, size_t n, 
     }
     uint32_t total;
     block_exclusive_scan(cnt, tmp, &total);
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
+        VELO_TRACE_AT(TS_TILE_COUNT, counts + cta);
         counts[cta] = total;
+    }
 }
 
 // exclusive scan of the tile counts into prefix[0..ntiles]; one CTA
@@ -511,6 +521,8 @@ __device__ __forceinline__ void scan_tiles(const uint32_t* counts, int ntiles, u
     uint32_t carry = 0;
     for (int base = 0; base < ntiles; base += blockDim.x) {
         const int i = base + threadIdx.x;
+        if (i < ntiles)
+            VELO_TRACE_AT(TS_SCAN, counts + i);
         const uint32_t x = i < ntiles ? __ldcg(counts + i) : 0u;
         uint32_t total;
         const uint32_t ex = block_exclusive_scan(x, tmp, &total);

@@ -38,7 +38,8 @@ static unsigned grid_for(size_t n)
 }
 
 #define VELO_GRID_STRIDE(i, n)                                                                                         \
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, (n));                          \
+         i += (size_t)gridDim.x * blockDim.x)
 
 // ---------------------------------------------------------------------------
 // compat operators (include/cuda/permute.cuh:24-40, gather.cuh:28-45,
@@ -156,6 +157,7 @@ __host__ __device__ __forceinline__ uint64_t philox_u64(uint64_t idx, uint64_t c
 __global__ void k_shuffle_pack(const uint32_t* map, size_t n, size_t np, uint64_t counter, uint64_t key, uint64_t* k,
                                uint32_t* p)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_shuffle_pack"));
     VELO_GRID_STRIDE(i, np)
     {
         k[i] = i < n ? philox_u64(i, counter, key) : ~0ull;
@@ -165,6 +167,7 @@ __global__ void k_shuffle_pack(const uint32_t* map, size_t n, size_t np, uint64_
 
 __global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, size_t n)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_copy_u32"));
     VELO_GRID_STRIDE(i, n)
     dst[i] = src[i];
 }
@@ -195,6 +198,7 @@ template <class F>
 __global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, const uint64_t* w1, const uint64_t* w2,
                                                          FillCarry* tile_last)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_sum"));
     __shared__ FillCarry sm[FL_THREADS];
     __shared__ int idx[FL_THREADS];
     const size_t base = (size_t)blockIdx.x * FL_TS;
@@ -202,6 +206,7 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, con
     int last = -1;
     for (int i = threadIdx.x; i < FL_TS; i += FL_THREADS) {
         const size_t g = base + i;
+        VELO_TRACE_AT(TS_FILL, w0 + g);
         const FillCarry d = F::src(w0[g], w1[g], w2[g]);
         c = fill_combine(c, d);
         last = d.has ? i : last;
@@ -218,18 +223,23 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, con
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
+        VELO_TRACE_AT(TS_FILL, tile_last + blockIdx.x);
         tile_last[blockIdx.x] = sm[0];
+    }
 }
 
 __global__ void __launch_bounds__(1024) k_fill_scan(const FillCarry* tile_last, int ntiles, FillCarry* carry)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_scan"));
     __shared__ FillCarry sm[1024];
     const int per = (ntiles + 1023) / 1024;
     const int t0 = threadIdx.x * per, t1 = min(ntiles, t0 + per);
     FillCarry c { 0, 0, 0, 0 };
-    for (int t = t0; t < t1; t++)
+    for (int t = t0; t < t1; t++) {
+        VELO_TRACE_AT(TS_FILL, tile_last + t);
         c = fill_combine(c, tile_last[t]);
+    }
     sm[threadIdx.x] = c;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {
@@ -249,6 +259,7 @@ template <class F>
 __global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_t* w1, uint64_t* w2,
                                                            const FillCarry* carry, unsigned long long* d_stat)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_apply"));
     __shared__ FillCarry st[FL_THREADS];
     __shared__ uint32_t tmp[33];
     const size_t base = (size_t)blockIdx.x * FL_TS + (size_t)threadIdx.x * FL_RPT;
@@ -256,6 +267,7 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_
     FillCarry mine { 0, 0, 0, 0 };
 #pragma unroll
     for (int r = 0; r < FL_RPT; r++) {
+        VELO_TRACE_AT(TS_FILL, w0 + base + r);
         a[r] = w0[base + r];
         b[r] = w1[base + r];
         c[r] = w2[base + r];
@@ -276,6 +288,7 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_
         stat += F::dup(a[r], b[r], c[r], run) ? 1u : 0u;
         run = fill_combine(run, F::src(a[r], b[r], c[r]));
         F::apply(a[r], b[r], c[r], run);
+        VELO_TRACE_AT(TS_FILL, w0 + base + r);
         w0[base + r] = a[r];
         w1[base + r] = b[r];
         w2[base + r] = c[r];
@@ -328,6 +341,7 @@ struct GatherFill {
 __global__ void k_ogather_pack(const uint64_t* table, size_t tn, const uint32_t* rids, size_t rn, size_t rows,
                                uint64_t* w0, uint64_t* w1, uint64_t* w2)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_ogather_pack"));
     VELO_GRID_STRIDE(g, rows)
     {
         uint64_t a = ~0ull, b = ~0ull, c = ~0ull;
@@ -349,6 +363,7 @@ __global__ void k_ogather_pack(const uint64_t* table, size_t tn, const uint32_t*
 
 __global__ void k_ogather_out(const uint64_t* w1, size_t rn, uint64_t* out)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_ogather_out"));
     VELO_GRID_STRIDE(j, rn)
     out[j] = w1[j];
 }
@@ -389,6 +404,7 @@ struct JoinFill {
 __global__ void k_ojoin_pack(const void* bk, const uint8_t* bm, size_t bn, const void* pk, const uint8_t* pm, size_t pn,
                              int key64, size_t rows, uint64_t* w0, uint64_t* w1, uint64_t* w2)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_ojoin_pack"));
     VELO_GRID_STRIDE(g, rows)
     {
         uint64_t a = ~0ull, b = ~0ull, c = ~0ull;
@@ -412,6 +428,7 @@ __global__ void k_ojoin_pack(const void* bk, const uint8_t* bm, size_t bn, const
 
 __global__ void k_ojoin_out(const uint64_t* w1, const uint64_t* w2, size_t pn, int64_t* ob, int64_t* op)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_ojoin_out"));
     VELO_GRID_STRIDE(i, pn)
     {
         const uint64_t b = w1[i];
@@ -423,12 +440,14 @@ __global__ void k_ojoin_out(const uint64_t* w1, const uint64_t* w2, size_t pn, i
 
 __global__ void k_zero_u64(unsigned long long* p, int n)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_zero_u64"));
     if ((int)threadIdx.x < n)
         p[threadIdx.x] = 0;
 }
 
 __global__ void k_join_counts(const uint64_t* n_joined, const unsigned long long* dups, uint64_t* d_counts)
 {
+    VELO_TRACE_KERNEL(velo_site_hash("k_join_counts"));
     d_counts[0] = *n_joined;
     d_counts[1] = *dups;
 }

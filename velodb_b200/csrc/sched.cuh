@@ -119,6 +119,7 @@ struct Sched {
             const int step = s_step;
             if (step < 0)
                 return;
+            VELO_TRACE_WORK(s_item);
             const SchedStep st = a.steps[step];
             const int tile = (int)(s_item - st.item_begin);
             const SchedInst in = a.insts[st.inst];
@@ -158,6 +159,7 @@ template <int LOG_NT, int LOG_E>
 __global__ void __launch_bounds__(1 << LOG_NT) k_sched(SchedArgs a)
 {
     extern __shared__ __align__(16) char sm[];
+    VELO_TRACE_KERNEL(TS_K_SCHED);
     Sched<LOG_NT, LOG_E>::run(a, sm);
 }
 

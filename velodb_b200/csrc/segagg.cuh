@@ -21,6 +21,8 @@
 
 #include <cstdint>
 
+#include "trace.cuh"
+
 namespace velo {
 
 constexpr int SEG_TS = 2048;     // rows per tile
@@ -112,6 +114,7 @@ struct SegAgg {
     __device__ static void load_tile(uint64_t* const* words, size_t base, uint64_t* sw)
     {
         for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
+            VELO_TRACE_AT(TS_SEG_LOAD, words[0] + base + i);
 #pragma unroll
             for (int x = 0; x < W; x++)
                 sw[x * SEG_TS_PAD + seg_slot(i)] = words[x][base + i];
@@ -179,6 +182,7 @@ struct SegAgg {
             a.tails = t_all;
             a.tail_valid = Agg::valid(wl) ? 1u : 0u;
             a.pad_ = 0;
+            VELO_TRACE_AT(TS_SEG_META, aggs + tile);
             aggs[tile] = a;
 #pragma unroll
             for (int i = 0; i < V; i++) {
@@ -208,6 +212,7 @@ struct SegAgg {
             acc[i] = 0;
         uint32_t tcount = 0;
         for (int t = t0; t < t1; t++) {
+            VELO_TRACE_AT(TS_SEG_META, aggs + t);
             const SegTileAgg a = aggs[t];
             const bool cont = (t > 0) && (aggs[t - 1].tail_key == a.head_key) && a.uniform;
             if (!cont) {
@@ -273,6 +278,7 @@ struct SegAgg {
         }
         // replay my chunk producing carry_in and tail_prefix per tile
         for (int t = t0; t < t1; t++) {
+            VELO_TRACE_AT(TS_SEG_META, carry_in + (size_t)t * V);
             const SegTileAgg a = aggs[t];
             const bool joins = (t > 0) && (aggs[t - 1].tail_key == a.head_key);
 #pragma unroll
@@ -420,6 +426,7 @@ struct SegAgg {
         }
         __syncthreads();
         for (int q = threadIdx.x; q < G * (1 + V); q += SEG_THREADS) {
+            VELO_TRACE_AT(TS_SEG_OUT, tile_out + (size_t)tile * G * (1 + V) + q);
             int64_t sum = 0;
             for (int w = 0; w < SEG_THREADS / 32; w++)
                 sum += red[q * 8 + w];
@@ -520,6 +527,7 @@ struct SegAgg {
         }
         __syncthreads();
         for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
+            VELO_TRACE_AT(TS_SEG_OUT, out[0] + base + i);
 #pragma unroll
             for (int x = 0; x <= V; x++)
                 out[x][base + i] = so[(size_t)x * SEG_TS_PAD + seg_slot(i)];
@@ -534,8 +542,10 @@ struct SegAgg {
         const int q = blockIdx.x;
         const int QN = G * (1 + V);
         int64_t sum = 0;
-        for (int t = threadIdx.x; t < ntiles; t += SEG_THREADS)
+        for (int t = threadIdx.x; t < ntiles; t += SEG_THREADS) {
+            VELO_TRACE_AT(TS_SEG_OUT, tile_out + (size_t)t * QN + q);
             sum += tile_out[(size_t)t * QN + q];
+        }
         sum = warp_sum_i64(sum);
         if ((threadIdx.x & 31) == 0)
             part[threadIdx.x >> 5] = sum;

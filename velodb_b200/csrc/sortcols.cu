@@ -143,7 +143,8 @@ __device__ __forceinline__ void store_raw(const ColSpec& s, int c, size_t g, uin
 template <int KW>
 __global__ void k_pack_cols(ColSpec s, size_t n, size_t np, uint64_t* words)
 {
-    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < np; g += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_pack_cols"));
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(g, np); g += (size_t)gridDim.x * blockDim.x) {
         uint64_t w[KW];
 #pragma unroll
         for (int i = 0; i < KW; i++)
@@ -174,7 +175,8 @@ __global__ void k_pack_cols(ColSpec s, size_t n, size_t np, uint64_t* words)
 template <int KW>
 __global__ void k_unpack_cols(ColSpec s, size_t np, const uint64_t* words, int64_t* indices)
 {
-    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < np; g += (size_t)gridDim.x * blockDim.x) {
+    VELO_TRACE_KERNEL(velo_site_hash("k_unpack_cols"));
+    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(g, np); g += (size_t)gridDim.x * blockDim.x) {
         uint64_t w[KW];
 #pragma unroll
         for (int i = 0; i < KW; i++)
