@@ -133,6 +133,38 @@ __device__ __forceinline__ void xsel(bool x, uint64_t& a, uint64_t& b)
     b = nb;
 }
 
+// The same exchange on the integer multiply-add (FMA) pipe: with s = 1 to
+// swap (mm = -s), d = b - a, a' = a + d*s, b' = b + d*mm, all mod 2^32.  The
+// in-tile levels are bound by the integer ALU pipe (two selects a register);
+// doing part of each row's registers here lets both pipes work.  `neg` is -1
+// known only at run time, so the subtraction stays a multiply-add too.
+struct MadSwap {
+    uint32_t s, mm, neg;
+    __device__ __forceinline__ explicit MadSwap(bool x)
+    {
+        neg = (uint32_t)(-(int)(blockDim.x != 0u));
+        // an opaque copy: knowing mm is 0 or -1, the compiler would turn the
+        // multiply-adds back into selects on the ALU pipe
+        const uint32_t m0 = x ? 0xFFFFFFFFu : 0u;
+        asm("mov.b32 %0, %1;" : "=r"(mm) : "r"(m0));
+        s = mm * neg;
+    }
+    __device__ __forceinline__ void operator()(uint32_t& a, uint32_t& b) const
+    {
+        const uint32_t d = a * neg + b;
+        a = d * s + a;
+        b = d * mm + b;
+    }
+    __device__ __forceinline__ void operator()(uint64_t& a, uint64_t& b) const
+    {
+        uint32_t al = lo32(a), ah = hi32(a), bl = lo32(b), bh = hi32(b);
+        (*this)(al, bl);
+        (*this)(ah, bh);
+        a = ((uint64_t)ah << 32) | al;
+        b = ((uint64_t)bh << 32) | bl;
+    }
+};
+
 // how a RowRec compares its key
 enum KeyMode : int {
     KEY_MASKED = 0, // words 0..KW-1, each AND-ed with Cols::mask (runtime)
@@ -177,11 +209,13 @@ struct RowKP {
     {
         return (gt_mask3(a.p, a.kl, a.kh, b.p, b.kl, b.kh) != 0u) != desc;
     }
-    // exchange a and b where m is all ones, in place (two selects a register)
+    // exchange a and b when x, in place: key halves on the multiply-add
+    // pipe, payload by selects
     __device__ __forceinline__ static void cswap(RowKP& a, RowKP& b, bool x)
     {
-        xsel(x, a.kl, b.kl);
-        xsel(x, a.kh, b.kh);
+        const MadSwap m(x);
+        m(a.kl, b.kl);
+        m(a.kh, b.kh);
         xsel(x, a.p, b.p);
     }
     __device__ __forceinline__ static bool marked(const RowKP&) { return false; }
@@ -229,9 +263,10 @@ struct RowKPM {
     }
     __device__ __forceinline__ static void cswap(RowKPM& a, RowKPM& b, bool x)
     {
-        xsel(x, a.kl, b.kl);
-        xsel(x, a.kh, b.kh);
-        xsel(x, a.p, b.p);
+        const MadSwap mad(x);
+        mad(a.kl, b.kl);
+        mad(a.kh, b.kh);
+        mad(a.p, b.p);
         xsel(x, a.m, b.m);
     }
     __device__ __forceinline__ static bool marked(const RowKPM& r) { return r.m != 0; }
@@ -307,11 +342,26 @@ struct RowRec {
         }
         return r;
     }
+    // about half of the registers on the multiply-add pipe, the rest by
+    // selects (W = 1: the high half only)
     __device__ __forceinline__ static void cswap(RowRec& a, RowRec& b, bool x)
     {
+        const MadSwap mad(x);
+        if constexpr (W == 1) {
+            uint32_t al = lo32(a.w[0]), ah = hi32(a.w[0]), bl = lo32(b.w[0]), bh = hi32(b.w[0]);
+            xsel(x, al, bl);
+            mad(ah, bh);
+            a.w[0] = ((uint64_t)ah << 32) | al;
+            b.w[0] = ((uint64_t)bh << 32) | bl;
+        } else {
 #pragma unroll
-        for (int i = 0; i < W; i++)
-            xsel(x, a.w[i], b.w[i]);
+            for (int i = 0; i < W; i++) {
+                if (2 * i < W)
+                    mad(a.w[i], b.w[i]);
+                else
+                    xsel(x, a.w[i], b.w[i]);
+            }
+        }
     }
     __device__ __forceinline__ static bool swap_pred(const RowRec& a, const RowRec& b, bool desc, const Cols& c)
     {
