@@ -674,10 +674,7 @@ def run_serve(args, world, rank, local):
     clk = clocks.stop()
     head = out["short"]
     value = head["served"]["qps_saturation"]
-    if world > 1:
-        t = torch.tensor([1.0 / value], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        value = world / float(t.item())
+    value, _ = aggregate_throughput(1.0, 1e3 / value, world, device, scale=1.0)
     from velodb_b200._lib import VeloQuery, VeloQueryResult
 
     line = {
@@ -706,6 +703,24 @@ def C_sizeof(t):
     import ctypes
 
     return ctypes.sizeof(t)
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """The slowest rank's value (every rank takes part; identity at N = 1)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_throughput(units_per_rank: float, ms: float, world: int, device=None, scale: float = 1e6) -> tuple:
+    """Whole-job throughput: all ranks' units over the slowest rank's time."""
+    ms_max = max_over_ranks(ms, world, device)
+    return world * units_per_rank / (ms_max / 1e3) / scale, ms_max
 
 
 def metric_name(workload):
@@ -769,25 +784,16 @@ def main():
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
-    ms = float(np.mean(ts))
-    if world > 1:
-        t = torch.tensor([ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     rows_per_step = wl.n
-    value = world * rows_per_step / (ms / 1e3) / 1e6
+    value, ms = aggregate_throughput(rows_per_step, float(np.mean(ts)), world, device)
 
     # end to end through the public API with host buffers
     for _ in range(2):
         wl.step_e2e()
     torch.cuda.synchronize()
     te = time_steps(torch, wl.step_e2e, max(3, args.steps // 2))
-    ems = float(np.mean(te))
-    if world > 1:
-        t = torch.tensor([ems], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
-    e2e = {"value": world * rows_per_step / (ems / 1e3) / 1e6, "unit": "Mrows/s",
+    e2e_value, ems = aggregate_throughput(rows_per_step, float(np.mean(te)), world, device)
+    e2e = {"value": e2e_value, "unit": "Mrows/s",
            "h2d_bytes_per_step": int(wl.in_bytes), "d2h_bytes_per_step": int(wl.d2h_bytes()), "ms_per_step": ems}
 
     if hasattr(wl, "step_plain"):
