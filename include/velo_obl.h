@@ -231,6 +231,9 @@ velo_status velo_trace_end(uint64_t* chain_digest, uint64_t* touched, uint64_t* 
  * Integer, BOOLEAN and DATE columns; one pass, every row read. */
 velo_status velo_range_mask(const void* d_col, uint32_t type, size_t n, int64_t lo, int64_t hi, uint8_t* d_mask,
                             uint32_t combine, void* stream);
+/* d_out[i] = the integer, BOOLEAN or DATE value col[i] as int64 (operands of
+ * SUM in velo_ogroupby). */
+velo_status velo_widen_i64(const void* d_col, uint32_t type, size_t n, int64_t* d_out, void* stream);
 /* d_out[i] = start + i (the $_rowid column of a scan). */
 velo_status velo_iota_i64(int64_t* d_out, size_t n, int64_t start, void* stream);
 /* Oblivious in-place compaction of n_cols typed columns (and their validity
@@ -254,6 +257,24 @@ size_t velo_ogather_column_scratch_bytes(size_t table_n, size_t n);
 velo_status velo_ogather_column(const void* d_table_col, uint32_t type, const uint8_t* d_table_valid,
                                 size_t table_n, const int64_t* d_rowids, size_t n, void* d_out,
                                 uint8_t* d_out_valid, void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* Oblivious GROUP BY key with SUM / COUNT: one or two aggregates a call
+ * (n_sums int64 columns summed mod 2^64, plus COUNT when with_count; n_sums +
+ * with_count is 1 or 2).  Rows with mask == 0 (NULL = all rows) are left out.
+ * Keys: VELO_INTEGER, or VELO_BIGINT in [-2^62, 2^62) (other BIGINT keys are
+ * left out and counted).  Writes the first group_bound groups in key order --
+ * d_out_keys[j], d_out_sums[s][j], d_out_counts[j] -- and zeros past the
+ * number of groups; d_counts (2 u64) = (groups, rows left out for their key).
+ * Sort, segmented sums and ORCompact of one record per group; every address
+ * depends only on n and group_bound.  The reference engine declares an
+ * aggregate plan node (include/planner/abstract_plan_node.hpp:31) without an
+ * operator; the algorithm is obliviator/operator_2/enclave/
+ * scalable_oblivious_join.c:105-262. */
+size_t velo_ogroupby_scratch_bytes(size_t n);
+velo_status velo_ogroupby(const void* d_keys, uint32_t key_type, const int64_t* const* d_sums, uint32_t n_sums,
+                          uint32_t with_count, const uint8_t* d_mask, size_t n, size_t group_bound,
+                          int64_t* d_out_keys, int64_t* const* d_out_sums, int64_t* d_out_counts,
+                          uint64_t* d_counts, void* d_scratch, size_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Oblivious shuffle, gather and PK-FK join                                 */

@@ -14,6 +14,9 @@
 //   HashJoinOperator         include/operator/hash_join_operator.hpp
 //   MaterializationOperator  include/operator/materialization_operator.hpp
 //   LimitOperator            include/operator/limit_operator.hpp
+//   AggregateOperator        the aggregate node the reference plans name
+//                            (include/planner/abstract_plan_node.hpp:31) but
+//                            do not implement
 // Errors inside an operator throw ExecutionError (the reference's
 // VELODB_THROW / CHECKED_CALL_THROW); a child's failed Result is returned
 // unchanged.  Special columns keep the reference's names: "$_rowid" (BIGINT)
@@ -328,6 +331,32 @@ public:
 
 private:
     std::vector<ColumnMapping> mappings_;
+};
+
+enum class AggKind { SUM, COUNT };
+
+struct AggregateSpec {
+    AggKind kind;
+    size_t column; // input column summed (ignored for COUNT)
+};
+
+// GROUP BY one integer key column (INTEGER or BIGINT; BIGINT keys in
+// [-2^62, 2^62)) with SUM / COUNT aggregates, oblivious (velo_ogroupby).
+// Rows whose "$_mask" is 0 are left out when the input has that column.
+// Output: the key as BIGINT, then one BIGINT per aggregate, the groups in key
+// order, at most group_bound of them (0 = the number of input rows, i.e. no
+// bound).  SUM columns may be any integer type (summed as int64 mod 2^64).
+class AggregateOperator : public UnaryOperator {
+public:
+    AggregateOperator(ExecutionContext& context, Schema output_schema, std::unique_ptr<AbstractOperator> child,
+                      size_t group_column, std::vector<AggregateSpec> aggregates, size_t group_bound = 0);
+    Result<RowBatch> next() override;
+
+private:
+    size_t group_column_;
+    std::vector<AggregateSpec> aggregates_;
+    size_t group_bound_;
+    bool done_ = false;
 };
 
 class LimitOperator : public UnaryOperator {

@@ -16,6 +16,7 @@
 #include "velo_operator.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -579,6 +580,71 @@ static void test_plan_scan_filter_sort_limit(ExecutionContext& ctx)
         EXPECT(gb[i] == -rows[i].first && gid[i] == rows[i].second);
 }
 
+// ---- aggregate ------------------------------------------------------------------------------
+
+static void test_aggregate_sum_count_with_mask(ExecutionContext& ctx)
+{
+    std::vector<int32_t> a;
+    std::vector<int64_t> b;
+    std::vector<uint32_t> d;
+    Table t = make_table(ctx, 60000, 31, a, b, d);
+    // GROUP BY a with SUM(b), COUNT(*), SUM(d) over the rows the scan's
+    // predicate keeps ($_mask), three aggregates (two calls underneath)
+    auto scan = std::make_unique<SeqScanOperator>(ctx, t, scan_schema(),
+                                                  std::vector<RangePredicate> { { 2, 0, 1999 } });
+    Schema os = schema_of({ { "a", VELO_BIGINT }, { "sum_b", VELO_BIGINT }, { "cnt", VELO_BIGINT },
+                            { "sum_d", VELO_BIGINT } });
+    AggregateOperator op(ctx, os, std::move(scan), 0,
+                         { { AggKind::SUM, 1 }, { AggKind::COUNT, 0 }, { AggKind::SUM, 2 } });
+    auto out = drain(op);
+    std::map<int32_t, std::array<int64_t, 3>> e;
+    for (size_t i = 0; i < a.size(); i++)
+        if (d[i] <= 1999) {
+            auto& x = e[a[i]];
+            x[0] += b[i];
+            x[1] += 1;
+            x[2] += d[i];
+        }
+    auto gk = col_host<int64_t>(ctx, out, 0);
+    auto s0 = col_host<int64_t>(ctx, out, 1);
+    auto c = col_host<int64_t>(ctx, out, 2);
+    auto s1 = col_host<int64_t>(ctx, out, 3);
+    EXPECT(gk.size() == e.size());
+    size_t i = 0;
+    for (auto& kv : e) {
+        EXPECT(gk[i] == kv.first && s0[i] == kv.second[0] && c[i] == kv.second[1] && s1[i] == kv.second[2]);
+        i++;
+    }
+}
+
+static void test_aggregate_bound_and_bigint_keys(ExecutionContext& ctx)
+{
+    std::vector<int64_t> k(5000), v(5000);
+    std::mt19937_64 rng(6);
+    for (size_t i = 0; i < k.size(); i++) {
+        k[i] = (int64_t)(rng() % 400) - 200;
+        v[i] = (int64_t)(rng() % 1000);
+    }
+    Schema s = schema_of({ { "k", VELO_BIGINT }, { "v", VELO_BIGINT } });
+    RowBatch rb;
+    rb.addColumn(Column::fromHost(ctx, VELO_BIGINT, k));
+    rb.addColumn(Column::fromHost(ctx, VELO_BIGINT, v));
+    std::vector<RowBatch> in;
+    in.push_back(std::move(rb));
+    AggregateOperator op(ctx, schema_of({ { "k", VELO_BIGINT }, { "s", VELO_BIGINT } }),
+                         std::make_unique<BatchSource>(ctx, s, std::move(in)), 0, { { AggKind::SUM, 1 } }, 10);
+    auto out = drain(op);
+    std::map<int64_t, int64_t> e;
+    for (size_t i = 0; i < k.size(); i++)
+        e[k[i]] += v[i];
+    auto gk = col_host<int64_t>(ctx, out, 0);
+    auto gs = col_host<int64_t>(ctx, out, 1);
+    EXPECT(gk.size() == 10);
+    auto it = e.begin();
+    for (size_t i = 0; i < 10; i++, ++it)
+        EXPECT(gk[i] == it->first && gs[i] == it->second);
+}
+
 // ------------------------------------------------------------------------------------------
 
 struct TestCase {
@@ -605,6 +671,8 @@ int main(int argc, char** argv)
         { "materialization", test_materialization },
         { "limit_offset", test_limit_offset },
         { "plan_scan_filter_sort_limit", test_plan_scan_filter_sort_limit },
+        { "aggregate_sum_count_with_mask", test_aggregate_sum_count_with_mask },
+        { "aggregate_bound_and_bigint_keys", test_aggregate_bound_and_bigint_keys },
     };
     if (argc > 1 && std::strcmp(argv[1], "--list") == 0) {
         for (auto& t : tests)

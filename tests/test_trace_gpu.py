@@ -322,3 +322,37 @@ def test_column_compaction_trace_is_data_independent(T):
         return f
 
     assert_same_trace([trace_of(T, run(x, d)) for x, d in ((1, 0.0), (2, 0.5), (3, 1.0))])
+
+
+def test_ogroupby_trace_is_data_independent(T):
+    n = 60_001
+    keys = torch.empty(n, dtype=torch.int32, device="cuda")
+    vals = torch.empty(n, dtype=torch.int64, device="cuda")
+    mask = torch.empty(n, dtype=torch.uint8, device="cuda")
+    bound = 1000
+    ok = torch.empty(bound, dtype=torch.int64, device="cuda")
+    os_ = torch.empty(bound, dtype=torch.int64, device="cuda")
+    oc = torch.empty(bound, dtype=torch.int64, device="cuda")
+    cnt = torch.empty(2, dtype=torch.int64, device="cuda")
+    sb = T.velo_ogroupby_scratch_bytes(n)
+    s = torch.empty(sb, dtype=torch.uint8, device="cuda")
+    sums = (C.c_void_p * 2)(vals.data_ptr(), None)
+    outs = (C.c_void_p * 2)(os_.data_ptr(), None)
+
+    def run(k, dens):
+        def f():
+            rng = np.random.default_rng(int(dens * 100))
+            dev_copy(keys, k)
+            dev_copy(vals, rng.integers(0, 1000, n).astype(np.int64))
+            dev_copy(mask, (rng.random(n) < dens).astype(np.uint8))
+            torch.cuda.synchronize()
+            assert T.velo_ogroupby(keys.data_ptr(), 4, sums, 1, 1, mask.data_ptr(), n, bound, ok.data_ptr(), outs,
+                                   oc.data_ptr(), cnt.data_ptr(), s.data_ptr(), sb, None) == 0, \
+                T.velo_last_error_text()
+        return f
+
+    rng = np.random.default_rng(0)
+    cases = [(rng.integers(0, 50, n).astype(np.int32), 0.5),      # few groups
+             (np.arange(n, dtype=np.int32), 1.0),                  # every row its own group
+             (np.zeros(n, np.int32), 0.0)]                         # one key, nothing selected
+    assert_same_trace([trace_of(T, run(k, d)) for k, d in cases])

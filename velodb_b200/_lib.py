@@ -21,6 +21,9 @@ PROTOS = {
     "velo_trace_enabled": (i32, []),
     "velo_trace_begin": (i32, [u64, u64]),
     "velo_trace_end": (i32, [vp, vp, vp, u64, vp]),
+    "velo_widen_i64": (i32, [vp, u32, sz, vp, vp]),
+    "velo_ogroupby_scratch_bytes": (sz, [sz]),
+    "velo_ogroupby": (i32, [vp, u32, vp, u32, u32, vp, sz, sz, vp, vp, vp, vp, vp, sz, vp]),
     "velo_device_alloc": (i32, [sz, vp, vp]),
     "velo_device_free": (i32, [vp, vp]),
     "velo_copy": (i32, [vp, vp, sz, u32, vp]),

@@ -333,3 +333,29 @@ def ojoin_pkfk(build_keys, build_mask, probe_keys, probe_mask, key_type, stream=
                                 pn, key_type, ob.data_ptr(), op.data_ptr(), cnt.data_ptr(), sc.data_ptr(), sc.numel(),
                                 _stream(stream)), "velo_ojoin_pkfk")
     return ob, op, cnt
+
+
+def ogroupby(keys: torch.Tensor, key_type: int, n: int, sums=(), with_count: bool = True, mask=None,
+             group_bound: int | None = None, stream=None):
+    """Oblivious GROUP BY key with SUM/COUNT (velo_ogroupby).  keys: int32
+    (key_type 4) or int64 (5) device tensor; sums: up to two int64 device
+    tensors (one when with_count).  Returns (out_keys, [out_sums], out_counts
+    or None, counts[2] = (groups, rows left out for their key)) as device
+    tensors of group_bound rows (default n)."""
+    import ctypes as C
+
+    dev = keys.device
+    bound = n if group_bound is None else group_bound
+    out_keys = torch.empty(max(bound, 1), dtype=torch.int64, device=dev)
+    out_sums = [torch.empty(max(bound, 1), dtype=torch.int64, device=dev) for _ in sums]
+    out_counts = torch.empty(max(bound, 1), dtype=torch.int64, device=dev) if with_count else None
+    counts = torch.empty(2, dtype=torch.int64, device=dev)
+    nb = int(lib().velo_ogroupby_scratch_bytes(n))
+    scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device=dev)
+    sp = (C.c_void_p * 2)(*[s.data_ptr() for s in sums], *([None] * (2 - len(sums))))
+    op = (C.c_void_p * 2)(*[s.data_ptr() for s in out_sums], *([None] * (2 - len(sums))))
+    check(lib().velo_ogroupby(keys.data_ptr(), key_type, sp, len(sums), 1 if with_count else 0,
+                              mask.data_ptr() if mask is not None else None, n, bound, out_keys.data_ptr(), op,
+                              out_counts.data_ptr() if out_counts is not None else None, counts.data_ptr(),
+                              scratch.data_ptr(), scratch.numel(), _stream(stream)), "velo_ogroupby")
+    return out_keys, out_sums, out_counts, counts

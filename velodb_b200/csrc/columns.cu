@@ -434,3 +434,30 @@ extern "C" velo_status velo_ogather_column(const void* d_table_col, uint32_t typ
     }
     return VELO_OK;
 }
+
+// ---------------------------------------------------------------------------
+// integer column -> int64 (operands of SUM)
+// ---------------------------------------------------------------------------
+
+namespace velo {
+__global__ void k_widen_i64(const void* col, uint32_t type, size_t n, int64_t* out)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_widen_i64"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n);
+         i += (size_t)gridDim.x * blockDim.x)
+        out[i] = load_int(col, type, i);
+}
+} // namespace velo
+
+extern "C" velo_status velo_widen_i64(const void* d_col, uint32_t type, size_t n, int64_t* d_out, void* stream)
+{
+    if (n == 0)
+        return VELO_OK;
+    if (!d_col || !d_out)
+        return einval("velo_widen_i64: null argument");
+    if (type == VELO_FLOAT || type == VELO_DOUBLE || type == VELO_VARCHAR || type_bytes(type) == 0)
+        return einval("velo_widen_i64: integer, BOOLEAN or DATE column expected");
+    k_widen_i64<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d_col, type, n, d_out);
+    VELO_CUDA_TRY(cudaGetLastError(), "widen launch");
+    return VELO_OK;
+}

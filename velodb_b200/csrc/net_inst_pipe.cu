@@ -11,3 +11,9 @@ VELO_INSTANTIATE_NET(LiRec3, 8, 4)
 
 using JoinRec = velo::RowRec<2, 1, false, velo::KEY_FULL>;
 VELO_INSTANTIATE_NET(JoinRec, 8, 4)
+
+// generic group-by records (velo_ogroupby): key word plus 0 or 2 sum words
+using GbRec1 = velo::RowRec<1, 1, false, velo::KEY_FULL>;
+using GbRec3 = velo::RowRec<3, 1, false, velo::KEY_FULL>;
+VELO_INSTANTIATE_NET(GbRec1, 8, 4)
+VELO_INSTANTIATE_NET(GbRec3, 8, 4)

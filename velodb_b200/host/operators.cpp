@@ -628,6 +628,105 @@ Result<RowBatch> MaterializationOperator::next()
     return Result<RowBatch>::success(std::move(out));
 }
 
+// ---- aggregate ----------------------------------------------------------------
+
+AggregateOperator::AggregateOperator(ExecutionContext& context, Schema output_schema,
+                                     std::unique_ptr<AbstractOperator> child, size_t group_column,
+                                     std::vector<AggregateSpec> aggregates, size_t group_bound)
+    : UnaryOperator(context, std::move(output_schema), std::move(child))
+    , group_column_(group_column)
+    , aggregates_(std::move(aggregates))
+    , group_bound_(group_bound)
+{
+    if (aggregates_.empty())
+        throw ExecutionError("AggregateOperator: at least one aggregate");
+    if (output_schema_.getColumnCount() != 1 + aggregates_.size())
+        throw ExecutionError("AggregateOperator: output schema must be the key and one column per aggregate");
+}
+
+Result<RowBatch> AggregateOperator::next()
+{
+    if (done_)
+        return Result<RowBatch>::success(RowBatch());
+    done_ = true;
+    RowBatch in = collectBatches(*child_);
+    const size_t n = in.getRowCount();
+    if (n == 0)
+        return Result<RowBatch>::success(RowBatch());
+    if (group_column_ >= in.getColumnCount())
+        return Result<RowBatch>::failure("AggregateOperator: group column out of range");
+    const Column& key = in.getColumn(group_column_);
+    if (key.getType() != VELO_INTEGER && key.getType() != VELO_BIGINT)
+        return Result<RowBatch>::failure("AggregateOperator: the group key must be INTEGER or BIGINT");
+    const size_t bound = group_bound_ ? std::min(group_bound_, n) : n;
+    // "$_mask" of the input, when there is one
+    const uint8_t* mask = nullptr;
+    for (size_t c = 0; c < in.getColumnCount() && c < child_->getOutputSchema().getColumnCount(); c++) {
+        const std::string& nm = child_->getOutputSchema().getColumnInfo(c).name;
+        if (nm == "$_mask" || (nm.size() > 7 && nm.compare(nm.size() - 7, 7, ".$_mask") == 0))
+            mask = static_cast<const uint8_t*>(in.getColumn(c).rawData());
+    }
+    // SUM operands as int64 columns
+    std::vector<std::shared_ptr<void>> wide(aggregates_.size());
+    for (size_t a = 0; a < aggregates_.size(); a++) {
+        if (aggregates_[a].kind != AggKind::SUM)
+            continue;
+        if (aggregates_[a].column >= in.getColumnCount())
+            return Result<RowBatch>::failure("AggregateOperator: SUM column out of range");
+        const Column& c = in.getColumn(aggregates_[a].column);
+        wide[a] = device_alloc(context_, n * 8);
+        check(velo_widen_i64(c.rawData(), c.getType(), n, static_cast<int64_t*>(wide[a].get()), context_.stream()),
+              "AggregateOperator");
+    }
+    std::vector<Column> out;
+    out.emplace_back(context_, VELO_BIGINT, bound);
+    for (size_t a = 0; a < aggregates_.size(); a++)
+        out.emplace_back(context_, VELO_BIGINT, bound);
+    const size_t sb = velo_ogroupby_scratch_bytes(n);
+    std::shared_ptr<void> scratch = device_alloc(context_, sb);
+    std::shared_ptr<void> counts = device_alloc(context_, 16);
+    std::shared_ptr<void> keys_tmp = device_alloc(context_, bound * 8);
+    // one or two aggregates per call: the groups (and their order) are the
+    // same in every call, so the key column is written by the first call only
+    size_t a = 0;
+    bool first = true;
+    while (a < aggregates_.size()) {
+        std::vector<size_t> take;
+        bool with_count = false;
+        std::vector<const int64_t*> sums;
+        std::vector<int64_t*> outs;
+        int64_t* out_count = nullptr;
+        while (a < aggregates_.size() && take.size() < 2) {
+            if (aggregates_[a].kind == AggKind::COUNT) {
+                if (with_count)
+                    break; // a second COUNT goes to the next call
+                with_count = true;
+                out_count = static_cast<int64_t*>(out[1 + a].rawData());
+            } else {
+                sums.push_back(static_cast<const int64_t*>(wide[a].get()));
+                outs.push_back(static_cast<int64_t*>(out[1 + a].rawData()));
+            }
+            take.push_back(a);
+            a++;
+        }
+        int64_t* keys_out = first ? static_cast<int64_t*>(out[0].rawData()) : static_cast<int64_t*>(keys_tmp.get());
+        check(velo_ogroupby(key.rawData(), key.getType(), sums.data(), (uint32_t)sums.size(), with_count ? 1u : 0u,
+                            mask, n, bound, keys_out, outs.data(), out_count, static_cast<uint64_t*>(counts.get()),
+                            scratch.get(), sb, context_.stream()),
+              "AggregateOperator");
+        first = false;
+    }
+    uint64_t hc[2] = { 0, 0 };
+    check(velo_copy(hc, counts.get(), 16, VELO_COPY_D2H, context_.stream()), "AggregateOperator");
+    context_.sync();
+    const size_t rows = std::min<size_t>((size_t)hc[0], bound);
+    RowBatch batch(std::move(out));
+    batch.setRowCount(rows);
+    if (rows == 0)
+        return Result<RowBatch>::success(RowBatch());
+    return Result<RowBatch>::success(std::move(batch));
+}
+
 // ---- limit -----------------------------------------------------------------
 
 LimitOperator::LimitOperator(ExecutionContext& context, Schema output_schema, std::unique_ptr<AbstractOperator> child,
