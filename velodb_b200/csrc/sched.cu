@@ -33,6 +33,7 @@ struct velo_batch {
     void* dmem = nullptr;               // steps | insts | done | next | status | compaction scratch
     velo::SchedStep* d_steps = nullptr;
     velo::SchedInst* d_insts = nullptr;
+    uint32_t* d_item_step = nullptr;
     uint32_t* d_done = nullptr;
     unsigned long long* d_next = nullptr;
     int* d_status = nullptr;
@@ -121,17 +122,27 @@ static velo_status batch_plan(velo_batch* b, const velo_batch_item* items, size_
         }
     }
     b->total_items = item;
-    // device memory: steps | insts | compaction scratch | done | next | status
+    if (b->steps.size() > 0xFFFFFFFFull)
+        return einval("velo_batch_create: too many steps");
+    // step of every item, so a claim costs one load
+    std::vector<uint32_t> item_step((size_t)item);
+    for (size_t s = 0; s < b->steps.size(); s++)
+        for (uint32_t t = 0; t < b->steps[s].ntiles; t++)
+            item_step[(size_t)b->steps[s].item_begin + t] = (uint32_t)s;
+    // device memory: steps | insts | item steps | compaction scratch | done | next | status
     const size_t steps_b = align_up(b->steps.size() * sizeof(SchedStep) + 1, 256);
+    const size_t items_b = align_up(item_step.size() * 4 + 1, 256);
     const size_t insts_b = align_up(b->insts.size() * sizeof(SchedInst) + 1, 256);
     const size_t scr_b = align_up(scratch_u32 * 4 + 256 * n_items + 1, 256);
     const size_t done_b = align_up(n_items * 4 + 1, 256);
     b->counter_bytes = done_b + 256;
-    VELO_CUDA_TRY(cudaMalloc(&b->dmem, steps_b + insts_b + scr_b + b->counter_bytes), "cudaMalloc(batch)");
+    VELO_CUDA_TRY(cudaMalloc(&b->dmem, steps_b + insts_b + items_b + scr_b + b->counter_bytes),
+                  "cudaMalloc(batch)");
     char* base = static_cast<char*>(b->dmem);
     b->d_steps = reinterpret_cast<SchedStep*>(base);
     b->d_insts = reinterpret_cast<SchedInst*>(base + steps_b);
-    char* scr = base + steps_b + insts_b;
+    b->d_item_step = reinterpret_cast<uint32_t*>(base + steps_b + insts_b);
+    char* scr = base + steps_b + insts_b + items_b;
     b->d_done = reinterpret_cast<uint32_t*>(scr + scr_b);
     b->d_next = reinterpret_cast<unsigned long long*>(scr + scr_b + done_b);
     b->d_status = reinterpret_cast<int*>(scr + scr_b + done_b + 64);
@@ -151,6 +162,9 @@ static velo_status batch_plan(velo_batch* b, const velo_batch_item* items, size_
     VELO_CUDA_TRY(cudaMemcpy(b->d_insts, b->insts.data(), b->insts.size() * sizeof(SchedInst),
                              cudaMemcpyHostToDevice),
                   "cudaMemcpy(insts)");
+    if (!item_step.empty())
+        VELO_CUDA_TRY(cudaMemcpy(b->d_item_step, item_step.data(), item_step.size() * 4, cudaMemcpyHostToDevice),
+                      "cudaMemcpy(item steps)");
     return VELO_OK;
 }
 
@@ -207,6 +221,7 @@ extern "C" velo_status velo_batch_launch(velo_batch* b, void* stream)
     SchedArgs a;
     a.steps = b->d_steps;
     a.insts = b->d_insts;
+    a.item_step = b->d_item_step;
     a.done = b->d_done;
     a.next_item = b->d_next;
     a.status = b->d_status;

@@ -55,6 +55,7 @@ struct SchedInst {
 struct SchedArgs {
     const SchedStep* steps;
     const SchedInst* insts;
+    const uint32_t* item_step; // step of every item (built with the plan)
     uint32_t* done;
     unsigned long long* next_item;
     int* status;
@@ -78,28 +79,28 @@ struct Sched {
     static constexpr size_t SMEM = NS::smem_bytes_sort() > NC::smem_bytes_compact() ? NS::smem_bytes_sort()
                                                                                        : NC::smem_bytes_compact();
 
+    // Thread 0 claims the next item while the CTA still works on the current
+    // one, so the claim, the step lookup and the dependency poll overlap the
+    // tile work of the item before.  A CTA holds at most one claimed item
+    // besides the one it runs; the smallest unfinished claimed item is always
+    // one that a CTA runs, so the launch cannot deadlock.
     __device__ static void run(const SchedArgs& a, char* sm)
     {
-        __shared__ unsigned long long s_item;
-        __shared__ int s_step;
+        __shared__ unsigned long long s_item, s_next;
+        __shared__ SchedStep s_st;
+        __shared__ SchedInst s_in;
         __shared__ uint32_t s_tmp[33];
+        if (threadIdx.x == 0)
+            s_next = atomicAdd(a.next_item, 1ull);
         for (;;) {
             if (threadIdx.x == 0) {
-                const unsigned long long x = atomicAdd(a.next_item, 1ull);
+                const unsigned long long x = s_next;
                 s_item = x;
-                int step = -1;
                 if (x < a.total_items) {
-                    // last step whose first item is <= x
-                    int lo = 0, hi = a.nsteps - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (a.steps[mid].item_begin <= x)
-                            lo = mid;
-                        else
-                            hi = mid - 1;
-                    }
-                    step = lo;
-                    const SchedStep st = a.steps[step];
+                    s_next = atomicAdd(a.next_item, 1ull);
+                    const SchedStep st = a.steps[__ldg(a.item_step + x)];
+                    s_st = st;
+                    s_in = a.insts[st.inst];
                     // bounded wait for the instance's previous passes
                     const uint64_t t0 = globaltimer_ns();
                     uint32_t spins = 0;
@@ -113,16 +114,15 @@ struct Sched {
                     }
                     __threadfence();
                 }
-                s_step = step;
             }
             __syncthreads();
-            const int step = s_step;
-            if (step < 0)
+            const unsigned long long item = s_item;
+            if (item >= a.total_items)
                 return;
-            VELO_TRACE_WORK(s_item);
-            const SchedStep st = a.steps[step];
-            const int tile = (int)(s_item - st.item_begin);
-            const SchedInst in = a.insts[st.inst];
+            const SchedStep st = s_st;
+            const SchedInst in = s_in;
+            VELO_TRACE_WORK(item);
+            const int tile = (int)(item - st.item_begin);
             NetGeom g { in.n, in.logN, 0 };
             switch (st.kind) {
             case STEP_SORT_PASS: {
@@ -146,11 +146,14 @@ struct Sched {
             default:
                 break;
             }
-            // every thread's stores are ordered before the completion count
-            __threadfence();
+            // the CTA's stores, then one gpu-scope fence and the completion
+            // count (bar.sync orders every thread's stores before thread 0's
+            // fence, which releases them with the count)
             __syncthreads();
-            if (threadIdx.x == 0)
+            if (threadIdx.x == 0) {
+                __threadfence();
                 atomicAdd(a.done + st.inst, 1u);
+            }
         }
     }
 };
