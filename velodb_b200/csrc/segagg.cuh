@@ -25,8 +25,8 @@
 
 namespace velo {
 
-constexpr int SEG_TS = 2048;     // rows per tile
-constexpr int SEG_THREADS = 256; // 8 contiguous rows per thread
+constexpr int SEG_TS = 1024;     // rows per tile
+constexpr int SEG_THREADS = 256; // 4 contiguous rows per thread
 constexpr int SEG_RPT = SEG_TS / SEG_THREADS;
 constexpr int SEG_MAX_G = 16;
 // smem row slot with one pad word per 8 rows, so the 8 contiguous rows of each
