@@ -7,10 +7,10 @@ sort on (flag1, flag2) -> segmented int64 sums, output padded to 8 groups).
 One step = one pass of that pipeline over one batch of input.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload groupby|sort|batch|serve]
+                    [--workload groupby|sort|batch|serve|join]
 
 Workloads: groupby (6,001,215-row filter + group-by, the default), sort
-(plain 2^20-row sort), batch (512 uneven sorts/compactions in one persistent
+(plain 2^20-row sort), join (1.5 M x 6 M-row PK-FK join + group-by + top-10), batch (512 uneven sorts/compactions in one persistent
 launch replayed from a CUDA graph, beside 512 plain launch sequences), serve
 (query stream over resident 60 M / 15 M / 150 M-row tables: served vs plain
 one-at-a-time throughput and p50/p99 latency).
@@ -236,9 +236,102 @@ def dominant_timing(torch, run, reset, launches, bytes_per_launch, name, reps=5)
             "bytes_per_launch": int(bytes_per_launch)}
 
 
+class JoinTopK:
+    """Config-2 shape: oblivious PK-FK join of a 1,500,000-row dimension
+    table and a 6,000,000-row fact table (~50 % filters on each side),
+    group-by fk over the joined rows, top-10 groups by sum(price).  Throughput
+    counts the 7.5 M input rows."""
+    name = "join_groupby_top10"
+
+    def __init__(self, torch, capi, W, device):
+        self.torch, self.capi = torch, capi
+        dim, fact = W.join_tables()
+        self.host = (dim, fact)
+        self.nd, self.nf = len(dim["key"]), len(fact["fk"])
+        self.n = self.nd + self.nf
+        self.pred = W.JOIN_PRED
+        self.k = W.JOIN_TOPK
+        self.pinned = {"dim_key": torch.from_numpy(dim["key"]).pin_memory(),
+                       "dim_date": torch.from_numpy(dim["date"]).pin_memory(),
+                       "fact_fk": torch.from_numpy(fact["fk"]).pin_memory(),
+                       "fact_price": torch.from_numpy(fact["price"]).pin_memory()}
+        self.dev = {k: v.to(device) for k, v in self.pinned.items()}
+        self.scratch = torch.empty(capi.join_groupby_topk_scratch_bytes(self.nd, self.nf), dtype=torch.uint8,
+                                   device=device)
+        self.out = torch.empty((self.k, 3), dtype=torch.int64, device=device)
+        self.counts = torch.empty(2, dtype=torch.int64, device=device)
+        self.out_host = torch.empty((self.k, 3), dtype=torch.int64).pin_memory()
+        self.counts_host = torch.empty(2, dtype=torch.int64).pin_memory()
+        self.in_bytes = sum(v.numel() * v.element_size() for v in self.pinned.values())
+        self.np_rows = 1 << int(np.ceil(np.log2(self.n)))
+        self.rec_bytes = 16
+        self.flush_l2 = False  # inputs (60 MB) plus union records (268 MB) exceed the 126 MB L2
+
+    def step(self):
+        self.capi.join_groupby_topk(self.dev, self.pred, self.k, scratch=self.scratch, out=self.out,
+                                    counts=self.counts)
+
+    def step_e2e(self):
+        for key in self.dev:
+            self.dev[key].copy_(self.pinned[key], non_blocking=True)
+        self.step()
+        self.out_host.copy_(self.out, non_blocking=True)
+        self.counts_host.copy_(self.counts, non_blocking=True)
+
+    def d2h_bytes(self):
+        return self.out.numel() * 8 + self.counts.numel() * 8
+
+    def launches(self):
+        u = int(np.log2(self.np_rows))
+        top = int(np.log2(1 << int(np.ceil(np.log2(self.nd)))))
+        return (1 + sort_passes(u, 12, 7) + 3 + 2 + compact_passes(u, 12, 7) + 3 + 2 + compact_passes(u, 12, 7)
+                + 1 + sort_passes(top, 12, 7) + 1)
+
+    def rdm_bytes(self):
+        """The algorithmic-bytes model of the join pipeline: union sort
+        (24 B), compaction to the fact bound, sort by fk (16 B), compaction of
+        the group heads, top-k sort over the dimension bound (16 B), plus one
+        streaming read and write of the union for the fill and the scan."""
+        u = self.np_rows
+        d = 1 << int(np.ceil(np.log2(self.nd)))
+        return (2 * u * 24 * rdm_psort(u) + self.nf * 5 + 2 * u * 24 * rdm_pcomp(u) + 2 * u * 16 * rdm_psort(u)
+                + 2 * u * 24 * rdm_pcomp(u) + 2 * d * 16 * rdm_psort(d) + 2 * 2 * u * 24)
+
+    def check(self, orc):
+        dim, fact = self.host
+        g, ofk, osum, ocnt = orc.join_groupby_topk(dim, fact, self.pred, self.k)
+        out = self.out.cpu().numpy()
+        cnt = self.counts.cpu().numpy()
+        m = min(g, self.k)
+        return bool(int(cnt[1]) == g and np.array_equal(out[:m, 0], ofk) and np.array_equal(out[:m, 1], osum)
+                    and np.array_equal(out[:m, 2], ocnt))
+
+    def dominant(self, device):
+        """The dominant kernel is the bitonic pass kernel of the union sort
+        (next_pow2(7.5 M) = 2^23 records of 2 words, 4096-row tiles), timed
+        live through the pipeline's stage timer (stage 2 = the union sort)."""
+        capi = self.capi
+        launches = sort_passes(int(np.log2(self.np_rows)), 12, 7)
+        capi.set_stage_timing(True)
+        ts = []
+        try:
+            for i in range(6):
+                self.step()
+                st = capi.last_stage_times()
+                if i:
+                    ts.append(st[1])
+        finally:
+            capi.set_stage_timing(False)
+        return {"kernel": "k_sort_pass<RowRec<2,1,false,KEY_FULL>,8,4> (union sort, 2^23 x 16 B records)",
+                "launches_per_sort": launches, "avg_launch_us": float(np.mean(ts)) * 1e3 / launches,
+                "bytes_per_launch": int(2 * self.np_rows * 16)}
+
+
 def make_workload(name, torch, capi, W, device):
     if name == "groupby":
         return GroupBy(torch, capi, W, device)
+    if name == "join":
+        return JoinTopK(torch, capi, W, device)
     if name == "sort":
         return SortKP(torch, capi, W, device)
     if name == "batch":
@@ -482,6 +575,22 @@ def cpu_baseline_sort(W, orc):
             "sample": f"full 2^20-row sort, {reps} runs, OpenMP over all cores"}
 
 
+def cpu_baseline_join(W, orc):
+    cores = os.cpu_count() or 1
+    dim, fact = W.join_tables()
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        orc.join_groupby_topk(dim, fact, W.JOIN_PRED, W.JOIN_TOPK, n_threads=cores)
+        reps += 1
+        if time.perf_counter() - t0 > 10.0 or reps >= 20:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    n = len(dim["key"]) + len(fact["fk"])
+    return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
+            "sample": f"full 1.5 M + 6 M-row join, {reps} runs, OpenMP over all cores"}
+
+
 def cpu_baseline_batch(W, orc):
     """The oracle on instances of the 512 in a fixed stride order until about
     10 s of CPU work: sorts on all cores, compactions single-threaded."""
@@ -544,6 +653,11 @@ def run_reference(args, rank):
         sample = "one of the 512 instances per step (stride 97 through the list); sorts on all cores, " \
                  "compactions single-threaded"
         wl = "batched_512"
+    elif args.workload == "join":
+        dim, fact = W.join_tables()
+        steps = [(lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, W.JOIN_TOPK, n_threads=cores),
+                  len(dim["key"]) + len(fact["fk"]))]
+        sample, wl = "full 1.5 M + 6 M-row join per step", "join_groupby_top10"
     elif args.workload == "serve":
         from velodb_b200 import serving as S
 
@@ -724,6 +838,8 @@ def aggregate_throughput(units_per_rank: float, ms: float, world: int, device=No
 
 
 def metric_name(workload):
+    if workload == "join":
+        return "oblivious PK-FK join + group-by + top-10 input throughput (1.5 M dim + 6 M fact rows)"
     if workload == "serve":
         return "served query throughput at saturation (queries/s; p50/p99 vs plain one-at-a-time)"
     if workload == "batch":
@@ -739,7 +855,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "sort", "batch", "serve"])
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "sort", "batch", "serve", "join"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -840,7 +956,7 @@ def main():
         line["checked_against_oracle"] = wl.check(orc)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = {"groupby": cpu_baseline_groupby, "sort": cpu_baseline_sort,
-                                    "batch": cpu_baseline_batch}[args.workload](W, orc)
+                                    "batch": cpu_baseline_batch, "join": cpu_baseline_join}[args.workload](W, orc)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

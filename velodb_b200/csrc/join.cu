@@ -15,7 +15,10 @@
 //   5. group    segmented sums of price per fk over the joined prefix; every
 //               row writes a group record, ORCompact moves the groups to the
 //               front (public bound: the dimension size)
-//   6. top-k    bitonic sort of the groups on (sum desc, fk asc), first k
+//   6. top-k    groups ordered on (sum desc, fk asc): for k <= 16 every
+//               4096-row tile is sorted in one in-tile pass, its best 16
+//               rows are gathered and only those candidates are fully
+//               sorted; otherwise a full bitonic sort; first k
 // Record layout of the union (2 u64 words):
 //   w0 = [63:32] key ^ 0x80000000 | [31] tag (0 dim, 1 fact) | [30] row passes
 //        its side's filter | [29] joined (set by fill) ; w1 = price (fact rows)
@@ -35,6 +38,7 @@ constexpr uint64_t J_JOINED = 1ull << 29;
 constexpr int J_LOG_NT = 8, J_LOG_E = 4; // 4096-row tiles
 constexpr int J_LT = J_LOG_NT + J_LOG_E;
 constexpr int J_LMAX = J_LT - 5 < 8 ? J_LT - 5 : 8;
+constexpr int J_TOPK_CAND = 16; // candidates kept per sorted tile (k <= 16 takes the tile path)
 
 // group-by over the joined prefix: run key = (fk, joined), values = (sum price, count)
 struct JoinAgg {
@@ -209,6 +213,25 @@ __global__ void k_topk_pack(const uint64_t* g0, const uint64_t* g1, const uint64
         t0[i] = a & (1ull << 63);
         t1[i] = ~(g1[i] ^ 0x8000000000000000ull);
         t2[i] = ((a & 0xFFFFFFFFull) << 32) | (g2[i] & 0xFFFFFFFFull);
+    }
+}
+
+// the best `c` rows of every sorted tile of 2^lt rows: tiles with bit lt of
+// their first row clear were sorted ascending (best first), the others
+// descending (best last); row positions depend only on the tile index
+__global__ void k_topk_candidates(const uint64_t* t0, const uint64_t* t1, const uint64_t* t2, int lt, int c,
+                                  size_t ntiles, uint64_t* c0, uint64_t* c1, uint64_t* c2)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_topk_candidates"));
+    const size_t total = ntiles * (size_t)c;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, total);
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t tile = i / (size_t)c, r = i % (size_t)c;
+        const size_t base = tile << lt;
+        const size_t src = (tile & 1) ? base + ((size_t)1 << lt) - 1 - r : base + r;
+        c0[i] = t0[src];
+        c1[i] = t1[src];
+        c2[i] = t2[src];
     }
 }
 
@@ -455,7 +478,35 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     tc.mark_inv = 1;
     tc.mark_word = 0;
     const int logT = ilog2_floor(n_top);
-    if (logT > 0) {
+    const uint64_t* w0 = s.t[0];
+    const uint64_t* w1 = s.t[1];
+    const uint64_t* w2 = s.t[2];
+    if (logT > J_LT && k <= J_TOPK_CAND) {
+        // top-k without a full sort: the in-tile pass sorts every tile of
+        // 2^J_LT rows, the best J_TOPK_CAND rows of each tile are gathered
+        // (the overall best k lie among them), and the candidates are sorted
+        std::vector<NetPass> passes { NetPass { P_SORT_TILE, J_LT, 0, 0 } };
+        rc = launch_net<TRec, J_LOG_NT, J_LOG_E>(tc, NetGeom { n_top, logT, 0 }, passes, nullptr, st);
+        if (rc != VELO_OK)
+            return rc;
+        const size_t ntiles = n_top >> J_LT;
+        const size_t nc = ntiles * J_TOPK_CAND;
+        k_topk_candidates<<<148 * 4, 256, 0, st>>>(s.t[0], s.t[1], s.t[2], J_LT, J_TOPK_CAND, ntiles, s.g[0],
+                                                    s.g[1], s.g[2]);
+        VELO_CUDA_TRY(cudaGetLastError(), "top-k candidates launch");
+        TRec::Cols cc = tc;
+        for (int i = 0; i < 3; i++)
+            cc.w[i] = s.g[i];
+        const int logC = ilog2_floor(nc);
+        passes.clear();
+        plan_sort(logC, J_LT, J_LMAX, passes);
+        rc = launch_net<TRec, J_LOG_NT, J_LOG_E>(cc, NetGeom { nc, logC, 0 }, passes, nullptr, st);
+        if (rc != VELO_OK)
+            return rc;
+        w0 = s.g[0];
+        w1 = s.g[1];
+        w2 = s.g[2];
+    } else if (logT > 0) {
         std::vector<NetPass> passes;
         plan_sort(logT, J_LT, J_LMAX, passes);
         rc = launch_net<TRec, J_LOG_NT, J_LOG_E>(tc, NetGeom { n_top, logT, 0 }, passes, nullptr, st);
@@ -463,7 +514,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
             return rc;
     }
     const size_t kk = k < n_top ? k : n_top;
-    k_topk_out<<<1, 256, 0, st>>>(s.t[0], s.t[1], s.t[2], kk, d_out, s.n_groups, s.n_joined, d_counts);
+    k_topk_out<<<1, 256, 0, st>>>(w0, w1, w2, kk, d_out, s.n_groups, s.n_joined, d_counts);
     VELO_CUDA_TRY(cudaGetLastError(), "top-k launch");
     if (kk < k)
         VELO_CUDA_TRY(cudaMemsetAsync(d_out + kk * 3, 0, (k - kk) * 3 * 8, st), "cudaMemsetAsync");
