@@ -12,11 +12,21 @@ namespace velo {
 template <int LOG_NT>
 constexpr int net_min_blocks() { return LOG_NT <= 8 ? 2 : 1; }
 
+// Passes of one sequence are launched with programmatic stream serialization:
+// the next pass may be launched while this one drains, and waits here until
+// this pass has completed and its stores are visible, before any global access.
+__device__ __forceinline__ void net_pass_prologue()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 template <class R, int LOG_NT, int LOG_E>
 __global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<LOG_NT>())
     k_sort_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];
+    net_pass_prologue();
     VELO_TRACE_KERNEL(TS_K_SORT_PASS);
     Net<R, LOG_NT, LOG_E>::template run<true>(c, g, p, tile_prefix, blockIdx.x, sm);
 }
@@ -26,6 +36,7 @@ __global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<LOG_NT>())
     k_compact_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];
+    net_pass_prologue();
     VELO_TRACE_KERNEL(TS_K_COMPACT_PASS);
     Net<R, LOG_NT, LOG_E>::template run<false>(c, g, p, tile_prefix, blockIdx.x, sm);
 }
@@ -48,9 +59,21 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
         return rc;
     const int lt = N::LT;
     const size_t grid = g.logN > lt ? ((size_t)1 << (g.logN - lt)) : 1;
-    for (const NetPass& p : passes)
-        kern<<<(unsigned)grid, 1 << LOG_NT, smem, st>>>(c, g, p, tile_prefix);
-    VELO_CUDA_TRY(cudaGetLastError(), "network pass launch");
+    // the first pass follows whatever ran before it; the later ones overlap
+    // their launch with the tail of the previous pass
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    for (size_t i = 0; i < passes.size(); i++) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(1u << LOG_NT);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = i > 0 ? 1 : 0;
+        VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, c, g, passes[i], tile_prefix), "network pass launch");
+    }
     return VELO_OK;
 }
 
