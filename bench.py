@@ -57,6 +57,11 @@ def hbm_peak():
 # pass-count model (mirrors plan_sort / plan_compact of the library)
 # --------------------------------------------------------------------------
 
+# levels fused per global pass: plain (u64, u32) sorts keep 32 contiguous rows
+# per warp (lmax = lt - 5); the pipelines' 8-byte records use 16 (lt - 4)
+PIPE_LMAX = 8
+
+
 def sort_passes(logn: int, lt: int, lmax: int) -> int:
     p = 1
     for k in range(lt + 1, logn + 1):
@@ -171,7 +176,7 @@ class GroupBy:
 
     def launches(self):
         logn = int(np.log2(self.np_rows))
-        return 2 + compact_passes(logn, 12, 7) + sort_passes(logn, 12, 7) + 4
+        return 2 + compact_passes(logn, 12, PIPE_LMAX) + sort_passes(logn, 12, PIPE_LMAX) + 4
 
     def rdm_bytes(self):
         npr = self.np_rows
@@ -200,7 +205,7 @@ class GroupBy:
         every launch reads and writes every record once: 2 x 2^23 x 16 B."""
         capi = self.capi
         logn = int(np.log2(self.np_rows))
-        launches = sort_passes(logn, 12, 7)
+        launches = sort_passes(logn, 12, PIPE_LMAX)
         capi.set_stage_timing(True)
         ts = []
         try:
@@ -284,8 +289,12 @@ class JoinTopK:
     def launches(self):
         u = int(np.log2(self.np_rows))
         top = int(np.log2(1 << int(np.ceil(np.log2(self.nd)))))
-        return (1 + sort_passes(u, 12, 7) + 3 + 2 + compact_passes(u, 12, 7) + 3 + 2 + compact_passes(u, 12, 7)
-                + 1 + sort_passes(top, 12, 7) + 1)
+        # pack, union sort, fill, count+scan, compaction, aggregation, count+scan,
+        # group compaction, top-k pack, tile pass, candidates, candidate sort, out
+        cand = int(np.log2((1 << max(0, top - 12)) * 16)) if top > 12 else 0
+        topk = (1 + 1 + sort_passes(cand, 12, PIPE_LMAX)) if top > 12 else sort_passes(top, 12, PIPE_LMAX)
+        return (1 + sort_passes(u, 12, PIPE_LMAX) + 3 + 2 + compact_passes(u, 12, PIPE_LMAX) + 3 + 2
+                + compact_passes(u, 12, PIPE_LMAX) + 1 + topk + 1)
 
     def rdm_bytes(self):
         """The algorithmic-bytes model of the join pipeline: union sort
@@ -311,7 +320,7 @@ class JoinTopK:
         (next_pow2(7.5 M) = 2^23 records of 2 words, 4096-row tiles), timed
         live through the pipeline's stage timer (stage 2 = the union sort)."""
         capi = self.capi
-        launches = sort_passes(int(np.log2(self.np_rows)), 12, 7)
+        launches = sort_passes(int(np.log2(self.np_rows)), 12, PIPE_LMAX)
         capi.set_stage_timing(True)
         ts = []
         try:

@@ -23,7 +23,8 @@ namespace velo {
 
 constexpr int GB_LOG_NT = 8, GB_LOG_E = 4;
 constexpr int GB_LT = GB_LOG_NT + GB_LOG_E;
-constexpr int GB_LMAX = GB_LT - 5 < 8 ? GB_LT - 5 : 8;
+// up to 8 fused global levels: 16 contiguous rows of 8-byte words fill a line
+constexpr int GB_LMAX = GB_LT - 4 < 8 ? GB_LT - 4 : 8;
 constexpr uint64_t GB_EXCL = 1ull << 63;
 constexpr int64_t GB_BIG = (int64_t)1 << 62;
 

@@ -35,6 +35,9 @@ constexpr uint64_t LI_KEYMASK = 0xFFFF800000000000ull;
 constexpr int LI_LOG_NT = 8, LI_LOG_E = 4; // 4096-row tiles for sort and compaction
 constexpr int LI_LT = LI_LOG_NT + LI_LOG_E;
 constexpr int LI_FIELD_BITS = 15;
+// global passes fuse up to 8 levels: 16 contiguous rows of 8-byte words are a
+// whole 128-byte line, so 2^4-row segments keep the loads coalesced
+constexpr int LI_LMAX = LI_LT - 4 < 8 ? LI_LT - 4 : 8;
 
 // decoding parameters of the two-word layout (public: from the predicate)
 struct LiParams {
@@ -303,7 +306,7 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
     // 2. ORCompact over the next_pow2(n) records
     {
         std::vector<NetPass> passes;
-        plan_compact(logN, LI_LT, LI_LT - 5 < 8 ? LI_LT - 5 : 8, passes);
+        plan_compact(logN, LI_LT, LI_LMAX, passes);
         NetGeom g { np, logN, 0 };
         rc = launch_net<Rec, LI_LOG_NT, LI_LOG_E>(rc3, g, passes, s.prefix, st);
         if (rc != VELO_OK)
@@ -322,7 +325,7 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
     }
     if (logS > 0) {
         std::vector<NetPass> passes;
-        plan_sort(logS, LI_LT, LI_LT - 5 < 8 ? LI_LT - 5 : 8, passes);
+        plan_sort(logS, LI_LT, LI_LMAX, passes);
         NetGeom g { (size_t)1 << logS, logS, 0 };
         rc = launch_net<Rec, LI_LOG_NT, LI_LOG_E>(rc3, g, passes, nullptr, st);
         if (rc != VELO_OK)

@@ -37,7 +37,8 @@ constexpr uint64_t J_KEYTAG = 0xFFFFFFFF80000000ull;
 constexpr uint64_t J_JOINED = 1ull << 29;
 constexpr int J_LOG_NT = 8, J_LOG_E = 4; // 4096-row tiles
 constexpr int J_LT = J_LOG_NT + J_LOG_E;
-constexpr int J_LMAX = J_LT - 5 < 8 ? J_LT - 5 : 8;
+// up to 8 fused global levels: 16 contiguous rows of 8-byte words fill a line
+constexpr int J_LMAX = J_LT - 4 < 8 ? J_LT - 4 : 8;
 constexpr int J_TOPK_CAND = 16; // candidates kept per sorted tile (k <= 16 takes the tile path)
 
 // group-by over the joined prefix: run key = (fk, joined), values = (sum price, count)
