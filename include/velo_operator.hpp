@@ -372,6 +372,32 @@ private:
     size_t skipped_count_ = 0;
 };
 
+// The result of a query: the root operator's schema and every batch it
+// produced (device-resident).
+struct QueryResult {
+    Schema schema;
+    std::vector<RowBatch> batches;
+    size_t rows = 0;
+    size_t getRowCount() const { return rows; }
+};
+
+// Drives an operator tree to the end of its stream, as the reference's
+// ExecutionEngine::executePlan does (src/execution/execution_engine.cpp:
+// 118-142).  SQL parsing and planning (executeQuery(sql)) are not part of this
+// build: plans arrive as operator trees.
+class ExecutionEngine {
+public:
+    explicit ExecutionEngine(ExecutionContext& context) : context_(context) { }
+    Result<QueryResult> executePlan(std::unique_ptr<AbstractOperator> root);
+    size_t getLastExecutionRowCount() const { return last_rows_; }
+    double getLastExecutionTimeMs() const { return last_ms_; }
+
+private:
+    ExecutionContext& context_;
+    size_t last_rows_ = 0;
+    double last_ms_ = 0.0;
+};
+
 // ---- template members --------------------------------------------------
 
 template <class T>

@@ -645,6 +645,42 @@ static void test_aggregate_bound_and_bigint_keys(ExecutionContext& ctx)
         EXPECT(gk[i] == it->first && gs[i] == it->second);
 }
 
+static void test_execution_engine_runs_a_plan(ExecutionContext& ctx)
+{
+    std::vector<int32_t> a;
+    std::vector<int64_t> b;
+    std::vector<uint32_t> d;
+    Table t = make_table(ctx, 20000, 55, a, b, d);
+    // SELECT a, SUM(b), COUNT(*) FROM t WHERE d <= 999 GROUP BY a
+    auto scan = std::make_unique<SeqScanOperator>(ctx, t, scan_schema(),
+                                                  std::vector<RangePredicate> { { 2, 0, 999 } });
+    auto filt = std::make_unique<FilterCompactionOperator>(ctx, scan_schema(), std::move(scan));
+    auto agg = std::make_unique<AggregateOperator>(
+        ctx, schema_of({ { "a", VELO_BIGINT }, { "s", VELO_BIGINT }, { "c", VELO_BIGINT } }), std::move(filt), 0,
+        std::vector<AggregateSpec> { { AggKind::SUM, 1 }, { AggKind::COUNT, 0 } });
+    ExecutionEngine engine(ctx);
+    auto r = engine.executePlan(std::move(agg));
+    EXPECT((bool)r);
+    QueryResult& q = r.value();
+    std::map<int32_t, std::pair<int64_t, int64_t>> e;
+    for (size_t i = 0; i < a.size(); i++)
+        if (d[i] <= 999) {
+            e[a[i]].first += b[i];
+            e[a[i]].second += 1;
+        }
+    EXPECT(q.getRowCount() == e.size() && engine.getLastExecutionRowCount() == e.size());
+    EXPECT(q.schema.getColumnCount() == 3 && engine.getLastExecutionTimeMs() > 0.0);
+    auto gk = col_host<int64_t>(ctx, q.batches, 0);
+    auto gs = col_host<int64_t>(ctx, q.batches, 1);
+    auto gc = col_host<int64_t>(ctx, q.batches, 2);
+    size_t i = 0;
+    for (auto& kv : e) {
+        EXPECT(gk[i] == kv.first && gs[i] == kv.second.first && gc[i] == kv.second.second);
+        i++;
+    }
+    EXPECT(!engine.executePlan(nullptr));
+}
+
 // ------------------------------------------------------------------------------------------
 
 struct TestCase {
@@ -673,6 +709,7 @@ int main(int argc, char** argv)
         { "plan_scan_filter_sort_limit", test_plan_scan_filter_sort_limit },
         { "aggregate_sum_count_with_mask", test_aggregate_sum_count_with_mask },
         { "aggregate_bound_and_bigint_keys", test_aggregate_bound_and_bigint_keys },
+        { "execution_engine_runs_a_plan", test_execution_engine_runs_a_plan },
     };
     if (argc > 1 && std::strcmp(argv[1], "--list") == 0) {
         for (auto& t : tests)

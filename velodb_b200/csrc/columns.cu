@@ -19,8 +19,7 @@
 namespace velo {
 
 using ColRec = RowRec<3, 1, false>;
-constexpr int COL_LOG_NT = 8, COL_LOG_E = 4;
-constexpr int COL_LT = COL_LOG_NT + COL_LOG_E;
+constexpr int COL_LT = 12; // 4096-row tiles (CTA shape per record width: Tile12)
 
 static int type_bytes(uint32_t t)
 {
@@ -301,7 +300,7 @@ extern "C" velo_status velo_ocompact_columns(void* const* d_cols, const uint32_t
         }
         k_pack_pair<<<grid_for(s.np), 256, 0, st>>>(in, s.mask, n, s.np, s.w[0], s.w[1], s.w[2]);
         VELO_CUDA_TRY(cudaGetLastError(), "column pack launch");
-        velo_status rc2 = launch_net<ColRec, COL_LOG_NT, COL_LOG_E>(rc, NetGeom { s.np, logN, 0 }, passes, s.prefix, st);
+        velo_status rc2 = launch_net12<ColRec>(rc, NetGeom { s.np, logN, 0 }, passes, s.prefix, st);
         if (rc2 != VELO_OK)
             return rc2;
         k_unpack_pair<<<grid_for(n), 256, 0, st>>>(out, n, s.w[0], s.w[1], s.w[2]);

@@ -279,6 +279,8 @@ struct RowKPM {
 template <int W, int KW, bool STRICT = true, int KM = KEY_MASKED>
 struct RowRec {
     static_assert(KM != KEY_HI32 || KW == 1, "a 32-bit key lives in word 0");
+    static constexpr int WORDS = W;
+    static constexpr int KEY_WORDS = KW;
     uint64_t w[W];
     struct Cols {
         uint64_t* w[W];
@@ -396,11 +398,15 @@ struct RowRec {
     }
     __device__ __forceinline__ static bool marked_c(const RowRec& r, const Cols& c)
     {
-        uint64_t w = r.w[0];
+        // AND with a per-word mask rather than selecting the word: a select
+        // chain over the words is turned into a dynamically indexed load, which
+        // sends the whole register tile to local memory
+        const uint64_t bit = 1ull << c.mark_bit;
+        uint64_t w = 0;
 #pragma unroll
-        for (int x = 1; x < W; x++)
-            w = c.mark_word == x ? r.w[x] : w;
-        return (((w >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
+        for (int x = 0; x < W; x++)
+            w |= r.w[x] & (c.mark_word == x ? bit : 0ull);
+        return (w != 0) != (c.mark_inv != 0);
     }
 };
 

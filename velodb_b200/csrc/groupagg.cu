@@ -21,8 +21,7 @@
 
 namespace velo {
 
-constexpr int GB_LOG_NT = 8, GB_LOG_E = 4;
-constexpr int GB_LT = GB_LOG_NT + GB_LOG_E;
+constexpr int GB_LT = 12; // 4096-row tiles (CTA shape per record width: Tile12)
 // up to 8 fused global levels: 16 contiguous rows of 8-byte words fill a line
 constexpr int GB_LMAX = GB_LT - 4 < 8 ? GB_LT - 4 : 8;
 constexpr uint64_t GB_EXCL = 1ull << 63;
@@ -269,7 +268,7 @@ static velo_status gb_run(const GbScratch& s, const GbIn& in, size_t n, size_t b
     rc.mark_word = 0;
     std::vector<NetPass> passes;
     plan_sort(logN, GB_LT, GB_LMAX, passes);
-    velo_status rc2 = launch_net<typename T::Rec, GB_LOG_NT, GB_LOG_E>(rc, NetGeom { np, logN, 0 }, passes, nullptr, st);
+    velo_status rc2 = launch_net12<typename T::Rec>(rc, NetGeom { np, logN, 0 }, passes, nullptr, st);
     if (rc2 != VELO_OK)
         return rc2;
 
@@ -294,7 +293,7 @@ static velo_status gb_run(const GbScratch& s, const GbIn& in, size_t n, size_t b
     k_scan_tiles<<<1, 1024, 0, st>>>(s.counts, ntc, s.prefix, s.n_grp_rows);
     passes.clear();
     plan_compact(logN, GB_LT, GB_LMAX, passes);
-    rc2 = launch_net<typename T::Grp, GB_LOG_NT, GB_LOG_E>(gc, NetGeom { np, logN, 0 }, passes, s.prefix, st);
+    rc2 = launch_net12<typename T::Grp>(gc, NetGeom { np, logN, 0 }, passes, s.prefix, st);
     if (rc2 != VELO_OK)
         return rc2;
     k_gb_out<NS, CNT><<<gb_grid(bound), 256, 0, st>>>(s.g[0], s.g[1], s.g[2], bound, in.key_type, out, s.n_groups,

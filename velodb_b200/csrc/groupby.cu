@@ -32,8 +32,7 @@
 namespace velo {
 
 constexpr uint64_t LI_KEYMASK = 0xFFFF800000000000ull;
-constexpr int LI_LOG_NT = 8, LI_LOG_E = 4; // 4096-row tiles for sort and compaction
-constexpr int LI_LT = LI_LOG_NT + LI_LOG_E;
+constexpr int LI_LT = 12; // 4096-row tiles for sort and compaction (CTA shape: Tile12)
 constexpr int LI_FIELD_BITS = 15;
 // global passes fuse up to 8 levels: 16 contiguous rows of 8-byte words are a
 // whole 128-byte line, so 2^4-row segments keep the loads coalesced
@@ -308,7 +307,7 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
         std::vector<NetPass> passes;
         plan_compact(logN, LI_LT, LI_LMAX, passes);
         NetGeom g { np, logN, 0 };
-        rc = launch_net<Rec, LI_LOG_NT, LI_LOG_E>(rc3, g, passes, s.prefix, st);
+        rc = launch_net12<Rec>(rc3, g, passes, s.prefix, st);
         if (rc != VELO_OK)
             return rc;
     }
@@ -327,7 +326,7 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
         std::vector<NetPass> passes;
         plan_sort(logS, LI_LT, LI_LMAX, passes);
         NetGeom g { (size_t)1 << logS, logS, 0 };
-        rc = launch_net<Rec, LI_LOG_NT, LI_LOG_E>(rc3, g, passes, nullptr, st);
+        rc = launch_net12<Rec>(rc3, g, passes, nullptr, st);
         if (rc != VELO_OK)
             return rc;
     }

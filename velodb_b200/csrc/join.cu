@@ -35,8 +35,7 @@ using GRec = RowRec<3, 1, false>;
 using TRec = RowRec<3, 3, false>;
 constexpr uint64_t J_KEYTAG = 0xFFFFFFFF80000000ull;
 constexpr uint64_t J_JOINED = 1ull << 29;
-constexpr int J_LOG_NT = 8, J_LOG_E = 4; // 4096-row tiles
-constexpr int J_LT = J_LOG_NT + J_LOG_E;
+constexpr int J_LT = 12; // 4096-row tiles (CTA shape per record width: Tile12)
 // up to 8 fused global levels: 16 contiguous rows of 8-byte words fill a line
 constexpr int J_LMAX = J_LT - 4 < 8 ? J_LT - 4 : 8;
 constexpr int J_TOPK_CAND = 16; // candidates kept per sorted tile (k <= 16 takes the tile path)
@@ -411,7 +410,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     if (logU > 0) {
         std::vector<NetPass> passes;
         plan_sort(logU, J_LT, J_LMAX, passes);
-        rc = launch_net<JRec, J_LOG_NT, J_LOG_E>(uc, NetGeom { (size_t)1 << logU, logU, 0 }, passes, nullptr, st);
+        rc = launch_net12<JRec>(uc, NetGeom { (size_t)1 << logU, logU, 0 }, passes, nullptr, st);
         if (rc != VELO_OK)
             return rc;
     }
@@ -430,7 +429,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
         k_scan_tiles<<<1, 1024, 0, st>>>(s.counts, ntc, s.prefix, s.n_joined);
         std::vector<NetPass> passes;
         plan_compact(logR, J_LT, J_LMAX, passes);
-        rc = launch_net<JRec, J_LOG_NT, J_LOG_E>(uc, NetGeom { s.n_rec, logR, 0 }, passes, s.prefix, st);
+        rc = launch_net12<JRec>(uc, NetGeom { s.n_rec, logR, 0 }, passes, s.prefix, st);
         if (rc != VELO_OK)
             return rc;
     }
@@ -458,7 +457,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
         k_scan_tiles<<<1, 1024, 0, st>>>(s.gcounts, ntc, s.gprefix, s.n_grp_rows);
         std::vector<NetPass> passes;
         plan_compact(logR, J_LT, J_LMAX, passes);
-        rc = launch_net<GRec, J_LOG_NT, J_LOG_E>(gc, NetGeom { s.n_rec, logR, 0 }, passes, s.gprefix, st);
+        rc = launch_net12<GRec>(gc, NetGeom { s.n_rec, logR, 0 }, passes, s.gprefix, st);
         if (rc != VELO_OK)
             return rc;
     }
@@ -487,7 +486,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
         // 2^J_LT rows, the best J_TOPK_CAND rows of each tile are gathered
         // (the overall best k lie among them), and the candidates are sorted
         std::vector<NetPass> passes { NetPass { P_SORT_TILE, J_LT, 0, 0 } };
-        rc = launch_net<TRec, J_LOG_NT, J_LOG_E>(tc, NetGeom { n_top, logT, 0 }, passes, nullptr, st);
+        rc = launch_net12<TRec>(tc, NetGeom { n_top, logT, 0 }, passes, nullptr, st);
         if (rc != VELO_OK)
             return rc;
         const size_t ntiles = n_top >> J_LT;
@@ -501,7 +500,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
         const int logC = ilog2_floor(nc);
         passes.clear();
         plan_sort(logC, J_LT, J_LMAX, passes);
-        rc = launch_net<TRec, J_LOG_NT, J_LOG_E>(cc, NetGeom { nc, logC, 0 }, passes, nullptr, st);
+        rc = launch_net12<TRec>(cc, NetGeom { nc, logC, 0 }, passes, nullptr, st);
         if (rc != VELO_OK)
             return rc;
         w0 = s.g[0];
@@ -510,7 +509,7 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     } else if (logT > 0) {
         std::vector<NetPass> passes;
         plan_sort(logT, J_LT, J_LMAX, passes);
-        rc = launch_net<TRec, J_LOG_NT, J_LOG_E>(tc, NetGeom { n_top, logT, 0 }, passes, nullptr, st);
+        rc = launch_net12<TRec>(tc, NetGeom { n_top, logT, 0 }, passes, nullptr, st);
         if (rc != VELO_OK)
             return rc;
     }

@@ -80,6 +80,28 @@ template <class R, int LOG_NT, int LOG_E>
 velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::vector<NetPass>& passes,
                        const uint32_t* tile_prefix, cudaStream_t st);
 
+// CTA shape of a 4096-row tile (LT = 12) for a RowRec type: 256 threads with
+// 16 rows each, or 512 threads with 8 rows each where the W x 16 row words do
+// not fit under the 128-register cap of two 256-thread CTAs per SM.  3-word
+// sorts with one or two key words keep 16 rows (no spills, and fewer
+// transposes: measured faster than 8 rows); 3-word sorts with three key words,
+// wider sorts and every 3-word compaction spill at 16 rows.
+template <class R>
+struct Tile12 {
+    static constexpr bool WIDE_SORT = R::WORDS >= 4 || (R::WORDS == 3 && R::KEY_WORDS == 3);
+    static constexpr bool WIDE_COMPACT = R::WORDS >= 3;
+};
+
+template <class R>
+inline velo_status launch_net12(const typename R::Cols& c, const NetGeom& g, const std::vector<NetPass>& passes,
+                                const uint32_t* tile_prefix, cudaStream_t st)
+{
+    const bool compact = !passes.empty() && (passes[0].kind == P_COMPACT_TILE || passes[0].kind == P_COMPACT_GLOBAL);
+    if (compact ? Tile12<R>::WIDE_COMPACT : Tile12<R>::WIDE_SORT)
+        return launch_net<R, 9, 3>(c, g, passes, tile_prefix, st);
+    return launch_net<R, 8, 4>(c, g, passes, tile_prefix, st);
+}
+
 template <class R>
 inline velo_status launch_count_scan(const typename R::Cols& c, size_t n, int logN, int LT, uint32_t* counts,
                                      uint32_t* prefix, uint64_t* d_count, cudaStream_t st)

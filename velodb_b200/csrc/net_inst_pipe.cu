@@ -8,6 +8,7 @@ using LiRec3 = velo::RowRec<3, 1, false, velo::KEY_HI32>;
 
 VELO_INSTANTIATE_NET(LiRec2, 8, 4)
 VELO_INSTANTIATE_NET(LiRec3, 8, 4)
+VELO_INSTANTIATE_NET(LiRec3, 9, 3)
 
 using JoinRec = velo::RowRec<2, 1, false, velo::KEY_FULL>;
 VELO_INSTANTIATE_NET(JoinRec, 8, 4)
@@ -17,3 +18,4 @@ using GbRec1 = velo::RowRec<1, 1, false, velo::KEY_FULL>;
 using GbRec3 = velo::RowRec<3, 1, false, velo::KEY_FULL>;
 VELO_INSTANTIATE_NET(GbRec1, 8, 4)
 VELO_INSTANTIATE_NET(GbRec3, 8, 4)
+VELO_INSTANTIATE_NET(GbRec3, 9, 3)

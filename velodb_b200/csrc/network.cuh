@@ -59,8 +59,14 @@ template <int W, int KW, bool S, int KM>
 struct MarkAt<RowRec<W, KW, S, KM>> {
     __device__ __forceinline__ static bool get(const typename RowRec<W, KW, S, KM>::Cols& c, size_t g)
     {
-        VELO_TRACE_AT(TS_MARK_LOAD, c.w[c.mark_word] + g);
-        return (((__ldcg(c.w[c.mark_word] + g) >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
+        // select the column pointer with constant indices (indexing the
+        // parameter array with mark_word copies it to local memory)
+        const uint64_t* col = c.w[0];
+#pragma unroll
+        for (int x = 1; x < W; x++)
+            col = c.mark_word == x ? c.w[x] : col;
+        VELO_TRACE_AT(TS_MARK_LOAD, col + g);
+        return (((__ldcg(col + g) >> c.mark_bit) & 1ull) != 0) != (c.mark_inv != 0);
     }
 };
 

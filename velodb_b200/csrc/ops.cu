@@ -454,7 +454,7 @@ __global__ void k_join_counts(const uint64_t* n_joined, const unsigned long long
 
 using Rec3 = RowRec<3, 1, false>;
 using Rec3K2 = RowRec<3, 2, false>;
-constexpr int OP_LOG_NT = 8, OP_LOG_E = 4, OP_LT = OP_LOG_NT + OP_LOG_E;
+constexpr int OP_LT = 12; // 4096-row tiles (CTA shape per record width: Tile12)
 constexpr int OP_LMAX = OP_LT - 5 < 8 ? OP_LT - 5 : 8;
 
 // scratch of the union-sort operators: 3 words x rows + fill carries + compaction
@@ -729,14 +729,14 @@ extern "C" velo_status velo_ogather_u64(const uint64_t* d_table, size_t table_n,
     c.mark_word = 0;
     std::vector<NetPass> passes;
     plan_sort(logR, OP_LT, OP_LMAX, passes);
-    velo_status rc = launch_net<Rec3, OP_LOG_NT, OP_LOG_E>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
+    velo_status rc = launch_net12<Rec3>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
     if (rc != VELO_OK)
         return rc;
     rc = run_fill<GatherFill>(s.w[0], s.w[1], s.w[2], rows, s.tl, s.carry, nullptr, st);
     if (rc != VELO_OK)
         return rc;
     c.mask[0] = ~0ull;
-    rc = launch_net<Rec3, OP_LOG_NT, OP_LOG_E>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
+    rc = launch_net12<Rec3>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
     if (rc != VELO_OK)
         return rc;
     k_ogather_out<<<grid_for(n_req), 256, 0, st>>>(s.w[1], n_req, d_out);
@@ -796,7 +796,7 @@ extern "C" velo_status velo_ojoin_pkfk(const void* d_build_keys, const uint8_t* 
     c.mark_inv = 0;
     std::vector<NetPass> passes;
     plan_sort(logR, OP_LT, OP_LMAX, passes);
-    velo_status rc = launch_net<Rec3K2, OP_LOG_NT, OP_LOG_E>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
+    velo_status rc = launch_net12<Rec3K2>(c, NetGeom { rows, logR, 0 }, passes, nullptr, st);
     if (rc != VELO_OK)
         return rc;
     rc = run_fill<JoinFill>(s.w[0], s.w[1], s.w[2], rows, s.tl, s.carry, s.stat, st);
@@ -807,7 +807,7 @@ extern "C" velo_status velo_ojoin_pkfk(const void* d_build_keys, const uint8_t* 
     k_scan_tiles<<<1, 1024, 0, st>>>(s.counts, nct, s.prefix, s.n_marked);
     std::vector<NetPass> cp;
     plan_compact(logR, OP_LT, OP_LMAX, cp);
-    rc = launch_net<Rec3K2, OP_LOG_NT, OP_LOG_E>(c, NetGeom { rows, logR, 0 }, cp, s.prefix, st);
+    rc = launch_net12<Rec3K2>(c, NetGeom { rows, logR, 0 }, cp, s.prefix, st);
     if (rc != VELO_OK)
         return rc;
     k_ojoin_out<<<grid_for(probe_n), 256, 0, st>>>(s.w[1], s.w[2], probe_n, d_out_build_rowid, d_out_probe_rowid);

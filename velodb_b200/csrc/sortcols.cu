@@ -303,11 +303,13 @@ extern "C" velo_status velo_sort_columns(void* const* d_cols, const uint32_t* ty
         return sort_cols_kw<1, 9, 4>(s, n, logN, words, d_indices, st);
     case 2:
         return sort_cols_kw<2, 9, 4>(s, n, logN, words, d_indices, st);
+    // wider records take fewer rows a thread, so the row words stay in
+    // registers (W x E words under the 128-register cap)
     case 3:
-        return sort_cols_kw<3, 8, 4>(s, n, logN, words, d_indices, st);
+        return sort_cols_kw<3, 9, 3>(s, n, logN, words, d_indices, st);
     case 4:
-        return sort_cols_kw<4, 8, 4>(s, n, logN, words, d_indices, st);
+        return sort_cols_kw<4, 9, 2>(s, n, logN, words, d_indices, st);
     default:
-        return sort_cols_kw<8, 8, 3>(s, n, logN, words, d_indices, st);
+        return sort_cols_kw<8, 9, 2>(s, n, logN, words, d_indices, st);
     }
 }

@@ -8,6 +8,7 @@
 #include "velo_operator.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 
 namespace velo_b200 {
@@ -762,6 +763,31 @@ Result<RowBatch> LimitOperator::next()
         current_count_ += take;
         return Result<RowBatch>::success(b.slice(skip, skip + take));
     }
+}
+
+// ---- execution engine ---------------------------------------------------------
+
+Result<QueryResult> ExecutionEngine::executePlan(std::unique_ptr<AbstractOperator> root)
+{
+    if (!root)
+        return Result<QueryResult>::failure("Cannot execute null plan");
+    const auto t0 = std::chrono::steady_clock::now();
+    QueryResult res;
+    res.schema = root->getOutputSchema();
+    for (;;) {
+        Result<RowBatch> r = root->next();
+        if (!r)
+            return Result<QueryResult>::failure(r.error());
+        RowBatch b = std::move(r).value();
+        if (b.getRowCount() == 0)
+            break;
+        res.rows += b.getRowCount();
+        res.batches.push_back(std::move(b));
+    }
+    context_.sync();
+    last_rows_ = res.rows;
+    last_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return Result<QueryResult>::success(std::move(res));
 }
 
 } // namespace velo_b200
