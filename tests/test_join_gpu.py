@@ -42,6 +42,14 @@ def test_join_ties_and_no_matches(cuda, orc):
     check(orc, dim, fact, dict(date_hi=-1, price_hi=10**12))  # no dimension row passes
 
 
+@pytest.mark.parametrize("k", [1, 15, 16, 17, 100, 1024])
+def test_join_topk_sizes(cuda, orc, k):
+    # candidates a tile keeps: 16 up to k = 16, then next_pow2(k); 1024 keeps whole tiles
+    dim, fact = W.join_tables(5000, 40000, seed=11)
+    check(orc, dim, fact, W.JOIN_PRED, k=k)
+    check(orc, dim, fact, dict(date_hi=10**6, price_hi=10**12), k=k)
+
+
 def test_join_config2_full(cuda, orc):
     dim, fact = W.join_tables()  # 1.5 M x 6 M
     check(orc, dim, fact, W.JOIN_PRED)

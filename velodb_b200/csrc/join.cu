@@ -12,18 +12,19 @@
 //   3. fill     forward fill of the last dimension row (segmented scan): a
 //               fact row joins iff its key's dimension row exists and passes
 //   4. compact  ORCompact of joined fact rows to the front (order kept)
-//   5. group    segmented sums of price per fk over the joined prefix; every
-//               row writes a group record, ORCompact moves the groups to the
-//               front (public bound: the dimension size)
-//   6. top-k    groups ordered on (sum desc, fk asc): for k <= 16 every
-//               4096-row tile is sorted in one in-tile pass, its best 16
-//               rows are gathered and only those candidates are fully
-//               sorted; otherwise a full bitonic sort; first k
+//   5. group    segmented sums of price per fk over the joined prefix: the
+//               last row of each fk run carries the group's (sum, count)
+//   6. top-k    groups ordered on (sum desc, fk asc) by a bitonic top-k
+//               network (topk.cuh): each 1024-row tile of the group-by keeps
+//               its best c = max(16, next_pow2(k)) rows in shared memory,
+//               then rounds over blocks of 4096 candidates keep their best
+//               c, until one sorted run of c is left; first k
 // Record layout of the union (2 u64 words):
 //   w0 = [63:32] key ^ 0x80000000 | [31] tag (0 dim, 1 fact) | [30] row passes
 //        its side's filter | [29] joined (set by fill) ; w1 = price (fact rows)
 #include "net_impl.cuh"
 #include "segagg.cuh"
+#include "topk.cuh"
 
 namespace velo {
 
@@ -31,14 +32,12 @@ namespace velo {
 // union sorts on the whole of w0, whose bits below the (key, tag) pair only
 // refine that order
 using JRec = RowRec<2, 1, false, KEY_FULL>;
-using GRec = RowRec<3, 1, false>;
-using TRec = RowRec<3, 3, false>;
 constexpr uint64_t J_KEYTAG = 0xFFFFFFFF80000000ull;
 constexpr uint64_t J_JOINED = 1ull << 29;
 constexpr int J_LT = 12; // 4096-row tiles (CTA shape per record width: Tile12)
 // up to 8 fused global levels: 16 contiguous rows of 8-byte words fill a line
 constexpr int J_LMAX = J_LT - 4 < 8 ? J_LT - 4 : 8;
-constexpr int J_TOPK_CAND = 16; // candidates kept per sorted tile (k <= 16 takes the tile path)
+constexpr int J_TOPK_MIN = 16; // candidates a group-by tile keeps at least
 
 // group-by over the joined prefix: run key = (fk, joined), values = (sum price, count)
 struct JoinAgg {
@@ -201,50 +200,60 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_apply(uint64_t* w0, const
     }
 }
 
-// ---- group records -> top-k sort records ------------------------------------
-// g0 = [63] not a group | [31:0] fk ^ sign ; g1 = sum price ; g2 = count
-// t0 = [63] not a group ; t1 = ~(sum ^ sign) (sum descending) ; t2 = fk << 32 | count
-__global__ void k_topk_pack(const uint64_t* g0, const uint64_t* g1, const uint64_t* g2, size_t n, uint64_t* t0,
-                            uint64_t* t1, uint64_t* t2)
+// ---- top-k keys of the groups -------------------------------------------------
+// k0 = [63] not a group | [62:0] ts >> 1 ; k1 = [63] ts & 1 | [62:31] fk ^ sign |
+// [30:0] count, with ts = ~(sum ^ sign), so ascending (k0, k1 & TK_M1) is
+// (groups first, sum descending, fk ascending).  A count is below 2^31: the
+// union holds at most 2^31 rows, one of them a dimension row.
+constexpr uint64_t TK_M1 = 0xFFFFFFFF80000000ull;
+constexpr uint64_t SIGN64 = 0x8000000000000000ull;
+constexpr int TK_RED_ROWS = 4096, TK_RED_THREADS = 1024; // candidate blocks of the later rounds
+
+__device__ __forceinline__ void topk_key(uint64_t o0, uint64_t sum, uint64_t cnt, uint64_t& k0, uint64_t& k1)
 {
-    VELO_TRACE_KERNEL(velo_site_hash("k_topk_pack"));
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, n); i += (size_t)gridDim.x * blockDim.x) {
-        const uint64_t a = g0[i];
-        t0[i] = a & (1ull << 63);
-        t1[i] = ~(g1[i] ^ 0x8000000000000000ull);
-        t2[i] = ((a & 0xFFFFFFFFull) << 32) | (g2[i] & 0xFFFFFFFFull);
+    const uint64_t ts = ~(sum ^ SIGN64);
+    k0 = (o0 & SIGN64) | (ts >> 1);
+    k1 = (ts << 63) | ((o0 & 0xFFFFFFFFull) << 31) | (cnt & 0x7FFFFFFFull);
+}
+
+// one round: every block of `rn` candidates (runs of c, each ascending) keeps
+// its best c; odd runs are loaded reversed so that neighbouring runs form
+// bitonic sequences
+__global__ void __launch_bounds__(TK_RED_THREADS) k_topk_reduce(const uint64_t* in0, const uint64_t* in1, int rn,
+                                                                int c, uint64_t* out0, uint64_t* out1)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_topk_reduce"));
+    extern __shared__ __align__(16) char sm[];
+    uint64_t* k0 = reinterpret_cast<uint64_t*>(sm);
+    uint64_t* k1 = k0 + TK_RED_ROWS;
+    const size_t base = (size_t)blockIdx.x * rn;
+    for (int i = threadIdx.x; i < rn; i += blockDim.x) {
+        const int q = i / c, r = i - q * c;
+        const int d = (q & 1) ? q * c + (c - 1 - r) : i;
+        VELO_TRACE_AT(TS_TOPK, in0 + base + i);
+        k0[d] = in0[base + i];
+        k1[d] = in1[base + i];
+    }
+    topk_net<TK_RED_ROWS / 2 / TK_RED_THREADS>(k0, k1, rn, c, TK_M1, true);
+    for (int j = threadIdx.x; j < c; j += blockDim.x) {
+        VELO_TRACE_AT(TS_TOPK, out0 + (size_t)blockIdx.x * c + j);
+        out0[(size_t)blockIdx.x * c + j] = k0[j];
+        out1[(size_t)blockIdx.x * c + j] = k1[j];
     }
 }
 
-// the best `c` rows of every sorted tile of 2^lt rows: tiles with bit lt of
-// their first row clear were sorted ascending (best first), the others
-// descending (best last); row positions depend only on the tile index
-__global__ void k_topk_candidates(const uint64_t* t0, const uint64_t* t1, const uint64_t* t2, int lt, int c,
-                                  size_t ntiles, uint64_t* c0, uint64_t* c1, uint64_t* c2)
-{
-    VELO_TRACE_KERNEL(velo_site_hash("k_topk_candidates"));
-    const size_t total = ntiles * (size_t)c;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, total);
-         i += (size_t)gridDim.x * blockDim.x) {
-        const size_t tile = i / (size_t)c, r = i % (size_t)c;
-        const size_t base = tile << lt;
-        const size_t src = (tile & 1) ? base + ((size_t)1 << lt) - 1 - r : base + r;
-        c0[i] = t0[src];
-        c1[i] = t1[src];
-        c2[i] = t2[src];
-    }
-}
-
-__global__ void k_topk_out(const uint64_t* t0, const uint64_t* t1, const uint64_t* t2, size_t k, int64_t* out,
-                           const uint64_t* n_groups, const uint64_t* n_joined, uint64_t* d_counts)
+__global__ void k_topk_out(const uint64_t* t0, const uint64_t* t1, size_t k, int64_t* out, const uint64_t* n_groups,
+                           const uint64_t* n_joined, uint64_t* d_counts)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_topk_out"));
     for (size_t i = threadIdx.x; i < k; i += blockDim.x) {
         VELO_TRACE_AT(TS_TOPK, t0 + i);
-        const bool ok = (t0[i] >> 63) == 0;
-        out[i * 3 + 0] = ok ? (int64_t)(int32_t)((uint32_t)(t2[i] >> 32) ^ 0x80000000u) : 0;
-        out[i * 3 + 1] = ok ? (int64_t)(~t1[i] ^ 0x8000000000000000ull) : 0;
-        out[i * 3 + 2] = ok ? (int64_t)(t2[i] & 0xFFFFFFFFull) : 0;
+        const uint64_t a = t0[i], b = t1[i];
+        const bool ok = (a >> 63) == 0;
+        const uint64_t ts = (a << 1) | (b >> 63);
+        out[i * 3 + 0] = ok ? (int64_t)(int32_t)((uint32_t)(b >> 31) ^ 0x80000000u) : 0;
+        out[i * 3 + 1] = ok ? (int64_t)(~ts ^ SIGN64) : 0;
+        out[i * 3 + 2] = ok ? (int64_t)(b & 0x7FFFFFFFull) : 0;
     }
     if (threadIdx.x == 0) {
         d_counts[0] = *n_joined;
@@ -267,24 +276,37 @@ __global__ void __launch_bounds__(1024) k_jseg_carries(const SegTileAgg* aggs, c
     JSeg::carries(aggs, runs, ntiles, carry_in, tail_prefix, n_groups, sm);
 }
 
-__global__ void __launch_bounds__(SEG_THREADS) k_jseg_emit_rows(JRec::Cols c, int ntiles, const SegTileAgg* aggs,
-                                                                const int64_t* carry_in, GRec::Cols g)
+// the group-by's last pass fused with the first top-k round: the tile's group
+// rows become top-k keys in shared memory and only its best `cand` are stored
+constexpr size_t JSEG_KEYS_OFF = (JSeg::SMEM + 15) & ~(size_t)15;
+constexpr size_t JSEG_TOPK_SMEM = JSEG_KEYS_OFF + (size_t)2 * SEG_TS * 8;
+
+__global__ void __launch_bounds__(SEG_THREADS) k_jseg_emit_topk(JRec::Cols c, int ntiles, const SegTileAgg* aggs,
+                                                                const int64_t* carry_in, int cand, uint64_t* out0,
+                                                                uint64_t* out1)
 {
-    VELO_TRACE_KERNEL(velo_site_hash("k_jseg_emit_rows"));
+    VELO_TRACE_KERNEL(velo_site_hash("k_jseg_emit_topk"));
     extern __shared__ __align__(16) char sm[];
-    JSeg::emit_rows(c.w, blockIdx.x, ntiles, aggs, carry_in, g.w, JoinAgg::Params {}, sm);
+    JSeg::emit_stage(c.w, blockIdx.x, ntiles, aggs, carry_in, JoinAgg::Params {}, sm);
+    const uint64_t* so = reinterpret_cast<const uint64_t*>(sm);
+    uint64_t* k0 = reinterpret_cast<uint64_t*>(sm + JSEG_KEYS_OFF);
+    uint64_t* k1 = k0 + SEG_TS;
+    for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS)
+        topk_key(so[seg_slot(i)], so[SEG_TS_PAD + seg_slot(i)], so[2 * SEG_TS_PAD + seg_slot(i)], k0[i], k1[i]);
+    topk_net<SEG_TS / 2 / SEG_THREADS>(k0, k1, SEG_TS, cand, TK_M1, false);
+    for (int j = threadIdx.x; j < cand; j += SEG_THREADS) {
+        VELO_TRACE_AT(TS_TOPK, out0 + (size_t)blockIdx.x * cand + j);
+        out0[(size_t)blockIdx.x * cand + j] = k0[j];
+        out1[(size_t)blockIdx.x * cand + j] = k1[j];
+    }
 }
 
 struct JoinScratch {
     uint64_t* u[2];      // union records
-    uint64_t* g[3];      // group records
-    uint64_t* t[3];      // top-k sort records (aliases the union area)
+    uint64_t* cand[2];   // top-k candidates of the group-by tiles (later rounds reuse u)
     uint32_t* counts;
     uint32_t* prefix;
     uint64_t* n_joined;
-    uint32_t* gcounts;
-    uint32_t* gprefix;
-    uint64_t* n_grp_rows;
     DimCarry* tile_last;
     DimCarry* fcarry;
     SegTileAgg* aggs;
@@ -292,7 +314,7 @@ struct JoinScratch {
     int64_t* carry;
     uint32_t* tail_prefix;
     uint64_t* n_groups;
-    size_t bytes, n_rec, n_top;
+    size_t bytes, n_rec;
 };
 
 static JoinScratch join_layout(char* base, size_t nd, size_t nf)
@@ -303,7 +325,6 @@ static JoinScratch join_layout(char* base, size_t nd, size_t nf)
     n_rec = n_rec < floor_rows ? floor_rows : n_rec;
     n_rec = n_rec < (size_t)SEG_TS ? (size_t)SEG_TS : n_rec;
     s.n_rec = n_rec;
-    s.n_top = next_pow2(nd);
     const size_t ntc = n_rec >> J_LT, nts = n_rec / SEG_TS, ntf = n_rec / FILL_TS;
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -313,14 +334,12 @@ static JoinScratch join_layout(char* base, size_t nd, size_t nf)
     };
     for (int i = 0; i < 2; i++)
         s.u[i] = reinterpret_cast<uint64_t*>(take(n_rec * 8));
-    for (int i = 0; i < 3; i++)
-        s.g[i] = reinterpret_cast<uint64_t*>(take(n_rec * 8));
+    // at most SEG_TS candidates a tile (k <= 1024)
+    for (int i = 0; i < 2; i++)
+        s.cand[i] = reinterpret_cast<uint64_t*>(take(n_rec * 8));
     s.counts = reinterpret_cast<uint32_t*>(take(ntc * 4));
     s.prefix = reinterpret_cast<uint32_t*>(take((ntc + 1) * 4));
     s.n_joined = reinterpret_cast<uint64_t*>(take(8));
-    s.gcounts = reinterpret_cast<uint32_t*>(take(ntc * 4));
-    s.gprefix = reinterpret_cast<uint32_t*>(take((ntc + 1) * 4));
-    s.n_grp_rows = reinterpret_cast<uint64_t*>(take(8));
     s.tile_last = reinterpret_cast<DimCarry*>(take(ntf * sizeof(DimCarry)));
     s.fcarry = reinterpret_cast<DimCarry*>(take(ntf * sizeof(DimCarry)));
     s.aggs = reinterpret_cast<SegTileAgg*>(take(nts * sizeof(SegTileAgg)));
@@ -329,11 +348,6 @@ static JoinScratch join_layout(char* base, size_t nd, size_t nf)
     s.tail_prefix = reinterpret_cast<uint32_t*>(take(nts * 4));
     s.n_groups = reinterpret_cast<uint64_t*>(take(8));
     s.bytes = off;
-    // the top-k records reuse the union area (free after the group-by) plus
-    // the group area's third word
-    s.t[0] = s.u[0];
-    s.t[1] = s.u[1];
-    s.t[2] = base ? reinterpret_cast<uint64_t*>(base) + 0 : nullptr;
     return s;
 }
 
@@ -346,7 +360,11 @@ static velo_status join_attrs()
         return VELO_OK;
     VELO_CUDA_TRY(cudaFuncSetAttribute(k_jseg_summary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JSeg::SMEM_IN),
                   "cudaFuncSetAttribute");
-    VELO_CUDA_TRY(cudaFuncSetAttribute(k_jseg_emit_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)JSeg::SMEM),
+    VELO_CUDA_TRY(cudaFuncSetAttribute(k_jseg_emit_topk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)JSEG_TOPK_SMEM),
+                  "cudaFuncSetAttribute");
+    VELO_CUDA_TRY(cudaFuncSetAttribute(k_topk_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(2 * TK_RED_ROWS * 8)),
                   "cudaFuncSetAttribute");
     if (dev >= 0 && dev < 64)
         done[dev] = 1;
@@ -359,9 +377,7 @@ using namespace velo;
 
 extern "C" size_t velo_join_groupby_topk_scratch_bytes(size_t n_dim, size_t n_fact)
 {
-    JoinScratch s = join_layout(nullptr, n_dim, n_fact);
-    // the top-k records need a third word array of next_pow2(n_dim) rows
-    return s.bytes + align_up(s.n_top * 8, 256);
+    return join_layout(nullptr, n_dim, n_fact).bytes;
 }
 
 extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const velo_join_pred* pred, uint32_t k,
@@ -377,12 +393,10 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     if (t->n_dim + t->n_fact > ((size_t)1 << MAX_LOGN))
         return einval("velo_join_groupby_topk: tables too large");
     JoinScratch s = join_layout(static_cast<char*>(d_scratch), t->n_dim, t->n_fact);
-    const size_t need = s.bytes + align_up(s.n_top * 8, 256);
-    if (!d_scratch || scratch_bytes < need) {
+    if (!d_scratch || scratch_bytes < s.bytes) {
         set_error("velo_join_groupby_topk: scratch must hold velo_join_groupby_topk_scratch_bytes() bytes");
         return VELO_ENOMEM;
     }
-    s.t[2] = reinterpret_cast<uint64_t*>(static_cast<char*>(d_scratch) + s.bytes);
     cudaStream_t st = (cudaStream_t)stream;
     velo_status rc = join_attrs();
     if (rc != VELO_OK)
@@ -435,89 +449,33 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     }
     tm.mark();
     // 5. group-by fk over the joined prefix (already in fk order: the
-    // compaction keeps the sorted order of the joined rows)
+    // compaction keeps the sorted order of the joined rows), fused with the
+    // first top-k round: the best `cand` groups of every tile
     const int nts = (int)(s.n_rec / SEG_TS);
-    GRec::Cols gc;
-    for (int i = 0; i < 3; i++) {
-        gc.w[i] = s.g[i];
-        gc.pad[i] = ~0ull;
-    }
-    gc.mask[0] = ~0ull;
-    gc.mark_bit = 63;
-    gc.mark_inv = 1;
-    gc.mark_word = 0;
+    const int cand = k <= (uint32_t)J_TOPK_MIN ? J_TOPK_MIN : (int)next_pow2(k);
     k_jseg_summary<<<nts, SEG_THREADS, JSeg::SMEM_IN, st>>>(uc, s.aggs, s.runs);
     k_jseg_carries<<<1, 1024, JoinAgg::V * 1024 * 8 + 2 * 1024 * 4, st>>>(s.aggs, s.runs, nts, s.carry,
                                                                             s.tail_prefix, s.n_groups);
-    k_jseg_emit_rows<<<nts, SEG_THREADS, JSeg::SMEM, st>>>(uc, nts, s.aggs, s.carry, gc);
+    k_jseg_emit_topk<<<nts, SEG_THREADS, JSEG_TOPK_SMEM, st>>>(uc, nts, s.aggs, s.carry, cand, s.cand[0],
+                                                              s.cand[1]);
     VELO_CUDA_TRY(cudaGetLastError(), "join group-by launch");
-    {
-        const int ntc = logR > J_LT ? 1 << (logR - J_LT) : 1;
-        k_count_marks<GRec><<<ntc, 256, 0, st>>>(gc, s.n_rec, J_LT, s.gcounts);
-        k_scan_tiles<<<1, 1024, 0, st>>>(s.gcounts, ntc, s.gprefix, s.n_grp_rows);
-        std::vector<NetPass> passes;
-        plan_compact(logR, J_LT, J_LMAX, passes);
-        rc = launch_net12<GRec>(gc, NetGeom { s.n_rec, logR, 0 }, passes, s.gprefix, st);
-        if (rc != VELO_OK)
-            return rc;
-    }
     tm.mark();
-    // 6. top-k: sort the first next_pow2(n_dim) group records (the public
-    // bound on the number of groups) on (sum desc, fk asc)
-    const size_t n_top = s.n_top;
-    k_topk_pack<<<148 * 4, 256, 0, st>>>(s.g[0], s.g[1], s.g[2], n_top, s.t[0], s.t[1], s.t[2]);
-    TRec::Cols tc;
-    for (int i = 0; i < 3; i++) {
-        tc.w[i] = s.t[i];
-        tc.pad[i] = ~0ull;
+    // 6. top-k rounds over blocks of candidates (the union area is free now)
+    uint64_t* cur[2] = { s.cand[0], s.cand[1] };
+    uint64_t* nxt[2] = { s.u[0], s.u[1] };
+    size_t n_c = (size_t)nts * cand;
+    while (n_c > (size_t)cand) {
+        const int rn = n_c < (size_t)TK_RED_ROWS ? (int)n_c : TK_RED_ROWS;
+        const size_t blocks = n_c / rn;
+        k_topk_reduce<<<(unsigned)blocks, TK_RED_THREADS, 2 * TK_RED_ROWS * 8, st>>>(cur[0], cur[1], rn, cand, nxt[0],
+                                                                                    nxt[1]);
+        VELO_CUDA_TRY(cudaGetLastError(), "top-k round launch");
+        n_c = blocks * cand;
+        std::swap(cur[0], nxt[0]);
+        std::swap(cur[1], nxt[1]);
     }
-    tc.mask[0] = 1ull << 63;
-    tc.mask[1] = ~0ull;
-    tc.mask[2] = 0xFFFFFFFF00000000ull;
-    tc.mark_bit = 63;
-    tc.mark_inv = 1;
-    tc.mark_word = 0;
-    const int logT = ilog2_floor(n_top);
-    const uint64_t* w0 = s.t[0];
-    const uint64_t* w1 = s.t[1];
-    const uint64_t* w2 = s.t[2];
-    if (logT > J_LT && k <= J_TOPK_CAND) {
-        // top-k without a full sort: the in-tile pass sorts every tile of
-        // 2^J_LT rows, the best J_TOPK_CAND rows of each tile are gathered
-        // (the overall best k lie among them), and the candidates are sorted
-        std::vector<NetPass> passes { NetPass { P_SORT_TILE, J_LT, 0, 0 } };
-        rc = launch_net12<TRec>(tc, NetGeom { n_top, logT, 0 }, passes, nullptr, st);
-        if (rc != VELO_OK)
-            return rc;
-        const size_t ntiles = n_top >> J_LT;
-        const size_t nc = ntiles * J_TOPK_CAND;
-        k_topk_candidates<<<148 * 4, 256, 0, st>>>(s.t[0], s.t[1], s.t[2], J_LT, J_TOPK_CAND, ntiles, s.g[0],
-                                                    s.g[1], s.g[2]);
-        VELO_CUDA_TRY(cudaGetLastError(), "top-k candidates launch");
-        TRec::Cols cc = tc;
-        for (int i = 0; i < 3; i++)
-            cc.w[i] = s.g[i];
-        const int logC = ilog2_floor(nc);
-        passes.clear();
-        plan_sort(logC, J_LT, J_LMAX, passes);
-        rc = launch_net12<TRec>(cc, NetGeom { nc, logC, 0 }, passes, nullptr, st);
-        if (rc != VELO_OK)
-            return rc;
-        w0 = s.g[0];
-        w1 = s.g[1];
-        w2 = s.g[2];
-    } else if (logT > 0) {
-        std::vector<NetPass> passes;
-        plan_sort(logT, J_LT, J_LMAX, passes);
-        rc = launch_net12<TRec>(tc, NetGeom { n_top, logT, 0 }, passes, nullptr, st);
-        if (rc != VELO_OK)
-            return rc;
-    }
-    const size_t kk = k < n_top ? k : n_top;
-    k_topk_out<<<1, 256, 0, st>>>(w0, w1, w2, kk, d_out, s.n_groups, s.n_joined, d_counts);
+    k_topk_out<<<1, 256, 0, st>>>(cur[0], cur[1], k, d_out, s.n_groups, s.n_joined, d_counts);
     VELO_CUDA_TRY(cudaGetLastError(), "top-k launch");
-    if (kk < k)
-        VELO_CUDA_TRY(cudaMemsetAsync(d_out + kk * 3, 0, (k - kk) * 3 * 8, st), "cudaMemsetAsync");
     tm.mark();
     tm.finish();
     return VELO_OK;

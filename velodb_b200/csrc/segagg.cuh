@@ -441,6 +441,22 @@ struct SegAgg {
     __device__ static void emit_rows(uint64_t* const* words, int tile, int ntiles, const SegTileAgg* aggs,
                                      const int64_t* carry_in, uint64_t* const* out, const Params& prm, char* smem)
     {
+        emit_stage(words, tile, ntiles, aggs, carry_in, prm, smem);
+        const uint64_t* so = reinterpret_cast<const uint64_t*>(smem);
+        const size_t base = (size_t)tile * SEG_TS;
+        for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
+            VELO_TRACE_AT(TS_SEG_OUT, out[0] + base + i);
+#pragma unroll
+            for (int x = 0; x <= V; x++)
+                out[x][base + i] = so[(size_t)x * SEG_TS_PAD + seg_slot(i)];
+        }
+    }
+
+    // emit_rows without the stores: leaves the tile's 1+V output words of
+    // row i at smem word x * SEG_TS_PAD + seg_slot(i) (after a barrier)
+    __device__ static void emit_stage(uint64_t* const* words, int tile, int ntiles, const SegTileAgg* aggs,
+                                      const int64_t* carry_in, const Params& prm, char* smem)
+    {
         uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
         int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * TW * 8);
         uint32_t* sflags = reinterpret_cast<uint32_t*>(smem + (size_t)SEG_TS_PAD * TW * 8 + (size_t)V * SEG_THREADS * 8);
@@ -526,12 +542,6 @@ struct SegAgg {
                     (uint64_t)(pref[r][i] + (lead ? cin[i] : 0) + (first_run_of_tile ? tc[i] : 0));
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
-            VELO_TRACE_AT(TS_SEG_OUT, out[0] + base + i);
-#pragma unroll
-            for (int x = 0; x <= V; x++)
-                out[x][base + i] = so[(size_t)x * SEG_TS_PAD + seg_slot(i)];
-        }
     }
 
     // pass D: out[q] = sum over tiles of tile_out[tile][q]; CTA q of
