@@ -198,102 +198,149 @@ struct SegAgg {
     __device__ static void carries(const SegTileAgg* aggs, const int64_t* tail_runs, int ntiles, int64_t* carry_in,
                                    uint32_t* tail_prefix, uint64_t* n_groups, char* smem)
     {
-        // thread-sequential over a contiguous chunk, then a block scan of the
-        // chunk aggregates (chunks are at most ntiles/1024 tiles)
-        const int nt = blockDim.x;
-        const int per = (ntiles + nt - 1) / nt;
-        const int t0 = threadIdx.x * per;
-        const int t1 = min(ntiles, t0 + per);
-        // segmented scan state for carry_out over my chunk
-        bool f = false; // a run boundary occurred in my chunk (reset)
-        int64_t acc[V];
+        // Rounds of blockDim.x consecutive tiles (coalesced loads, all issued
+        // at once), each a block-wide segmented scan chained to the previous
+        // round through (run_prev, cnt_prev).  Per tile t:
+        //   run_out(t) = tail_runs[t] + (t continues t-1's run and is one run
+        //                ? run_out(t-1) : 0)       (the run crossing t's end)
+        //   carry_in[t] = t's first run continues t-1's last ? run_out(t-1) : 0
+        //   tail_prefix[t] = groups ending in tiles before t
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        int64_t* wv = reinterpret_cast<int64_t*>(smem);                 // [V][32] warp prefixes
+        uint32_t* wc = reinterpret_cast<uint32_t*>(smem + (size_t)V * 32 * 8);  // [32]
+        int64_t* rv = reinterpret_cast<int64_t*>(smem + (size_t)V * 32 * 8 + 32 * 4);  // [V] round carry
+        uint32_t* rc = reinterpret_cast<uint32_t*>(rv + V);              // [1]
+        int64_t run_prev[V];
 #pragma unroll
         for (int i = 0; i < V; i++)
-            acc[i] = 0;
-        uint32_t tcount = 0;
-        for (int t = t0; t < t1; t++) {
-            VELO_TRACE_AT(TS_SEG_META, aggs + t);
-            const SegTileAgg a = aggs[t];
-            const bool cont = (t > 0) && (aggs[t - 1].tail_key == a.head_key) && a.uniform;
-            if (!cont) {
-                f = true;
+            run_prev[i] = 0;
+        uint32_t cnt_prev = 0;
+        for (int base = 0; base < ntiles; base += blockDim.x) {
+            const int t = base + (int)threadIdx.x;
+            const bool in = t < ntiles;
+            SegTileAgg a {};
+            uint64_t prev_tail = 0, next_head = 0;
+            int64_t x[V];
+            if (in) {
+                VELO_TRACE_AT(TS_SEG_META, aggs + t);
+                a = aggs[t];
+                prev_tail = t > 0 ? aggs[t - 1].tail_key : 0;
+                next_head = t + 1 < ntiles ? aggs[t + 1].head_key : 0;
+            }
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                x[i] = in ? tail_runs[(size_t)t * V + i] : 0;
+            const bool joins = in && t > 0 && prev_tail == a.head_key;
+            bool f = !(joins && a.uniform != 0); // a new run starts in this tile
+            const bool last_tail = (t + 1 < ntiles) ? (a.tail_key != next_head) : true;
+            const uint32_t cnt = in ? a.tails + ((last_tail && a.tail_valid != 0) ? 1u : 0u) : 0u;
+            uint32_t c = cnt;
+            // warp-inclusive segmented scan of x (resetting at f) and scan of c
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                int64_t y[V];
 #pragma unroll
                 for (int i = 0; i < V; i++)
-                    acc[i] = 0;
-            }
-#pragma unroll
-            for (int i = 0; i < V; i++)
-                acc[i] += tail_runs[(size_t)t * V + i];
-            const bool last_tail = (t + 1 < ntiles) ? (a.tail_key != aggs[t + 1].head_key) : true;
-            tcount += a.tails + ((last_tail & (a.tail_valid != 0)) ? 1u : 0u);
-        }
-        // block-level exclusive segmented scan of (f, acc) and of tcount
-        int64_t* sv = reinterpret_cast<int64_t*>(smem);
-        uint32_t* sf = reinterpret_cast<uint32_t*>(smem + (size_t)V * 1024 * 8);
-        uint32_t* sc = sf + 1024;
-        int64_t inc[V];
-#pragma unroll
-        for (int i = 0; i < V; i++)
-            inc[i] = acc[i];
-        bool fl = f;
-        uint32_t cinc = tcount;
-        for (int off = 1; off < nt; off <<= 1) {
-            __syncthreads();
-            sf[threadIdx.x] = fl ? 1u : 0u;
-            sc[threadIdx.x] = cinc;
-#pragma unroll
-            for (int i = 0; i < V; i++)
-                sv[i * 1024 + threadIdx.x] = inc[i];
-            __syncthreads();
-            if ((int)threadIdx.x >= off) {
-                const bool pf = sf[threadIdx.x - off] != 0;
-                if (!fl) {
+                    y[i] = __shfl_up_sync(0xFFFFFFFFu, x[i], off);
+                const int fy = __shfl_up_sync(0xFFFFFFFFu, f ? 1 : 0, off);
+                const uint32_t cy = __shfl_up_sync(0xFFFFFFFFu, c, off);
+                if (lane >= off) {
 #pragma unroll
                     for (int i = 0; i < V; i++)
-                        inc[i] += sv[i * 1024 + threadIdx.x - off];
+                        x[i] = f ? x[i] : x[i] + y[i];
+                    f = f || fy != 0;
+                    c += cy;
                 }
-                fl = fl | pf;
-                cinc += sc[threadIdx.x - off];
             }
+            if (lane == 31) {
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    wv[i * 32 + warp] = x[i];
+                wc[warp] = (c << 1) | (f ? 1u : 0u);
+            }
+            __syncthreads();
+            if (warp == 0) {
+                // scan of the warp totals, then exclusive prefixes that start
+                // from the previous rounds' carry
+                int64_t z[V];
+                bool g = false;
+                uint32_t d = 0;
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    z[i] = lane < nw ? wv[i * 32 + lane] : 0;
+                if (lane < nw) {
+                    g = (wc[lane] & 1u) != 0;
+                    d = wc[lane] >> 1;
+                }
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    int64_t y[V];
+#pragma unroll
+                    for (int i = 0; i < V; i++)
+                        y[i] = __shfl_up_sync(0xFFFFFFFFu, z[i], off);
+                    const int gy = __shfl_up_sync(0xFFFFFFFFu, g ? 1 : 0, off);
+                    const uint32_t dy = __shfl_up_sync(0xFFFFFFFFu, d, off);
+                    if (lane >= off) {
+#pragma unroll
+                        for (int i = 0; i < V; i++)
+                            z[i] = g ? z[i] : z[i] + y[i];
+                        g = g || gy != 0;
+                        d += dy;
+                    }
+                }
+                int64_t ez[V];
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    ez[i] = __shfl_up_sync(0xFFFFFFFFu, z[i], 1);
+                int eg = __shfl_up_sync(0xFFFFFFFFu, g ? 1 : 0, 1);
+                uint32_t ed = __shfl_up_sync(0xFFFFFFFFu, d, 1);
+                if (lane == 0) {
+#pragma unroll
+                    for (int i = 0; i < V; i++)
+                        ez[i] = 0;
+                    eg = 0;
+                    ed = 0;
+                }
+                __syncwarp();
+                if (lane < nw) {
+#pragma unroll
+                    for (int i = 0; i < V; i++)
+                        wv[i * 32 + lane] = eg ? ez[i] : run_prev[i] + ez[i];
+                    wc[lane] = cnt_prev + ed;
+                }
+                if (lane == nw - 1) {
+#pragma unroll
+                    for (int i = 0; i < V; i++)
+                        rv[i] = g ? z[i] : run_prev[i] + z[i];
+                    rc[0] = cnt_prev + d;
+                }
+            }
+            __syncthreads();
+            int64_t ro[V], pr[V];
+#pragma unroll
+            for (int i = 0; i < V; i++) {
+                const int64_t wp = wv[i * 32 + warp];
+                ro[i] = f ? x[i] : wp + x[i]; // run_out(t)
+                pr[i] = __shfl_up_sync(0xFFFFFFFFu, ro[i], 1);
+                if (lane == 0)
+                    pr[i] = wp; // run_out(t - 1)
+            }
+            const uint32_t cin = wc[warp] + c - cnt;
+            if (in) {
+                VELO_TRACE_AT(TS_SEG_META, carry_in + (size_t)t * V);
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    carry_in[(size_t)t * V + i] = joins ? pr[i] : 0;
+                tail_prefix[t] = cin;
+            }
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                run_prev[i] = rv[i];
+            cnt_prev = rc[0];
+            __syncthreads();
         }
-        __syncthreads();
-        // exclusive values for my chunk = inclusive of thread - 1
-        sf[threadIdx.x] = fl ? 1u : 0u;
-        sc[threadIdx.x] = cinc;
-#pragma unroll
-        for (int i = 0; i < V; i++)
-            sv[i * 1024 + threadIdx.x] = inc[i];
-        __syncthreads();
-        int64_t run_out[V]; // carry_out of the tile before my chunk
-        uint32_t cpre = 0;
-        if (threadIdx.x > 0) {
-#pragma unroll
-            for (int i = 0; i < V; i++)
-                run_out[i] = sv[i * 1024 + threadIdx.x - 1];
-            cpre = sc[threadIdx.x - 1];
-        } else {
-#pragma unroll
-            for (int i = 0; i < V; i++)
-                run_out[i] = 0;
-        }
-        // replay my chunk producing carry_in and tail_prefix per tile
-        for (int t = t0; t < t1; t++) {
-            VELO_TRACE_AT(TS_SEG_META, carry_in + (size_t)t * V);
-            const SegTileAgg a = aggs[t];
-            const bool joins = (t > 0) && (aggs[t - 1].tail_key == a.head_key);
-#pragma unroll
-            for (int i = 0; i < V; i++)
-                carry_in[(size_t)t * V + i] = joins ? run_out[i] : 0;
-            tail_prefix[t] = cpre;
-            const bool cont = joins && a.uniform;
-#pragma unroll
-            for (int i = 0; i < V; i++)
-                run_out[i] = (cont ? run_out[i] : 0) + tail_runs[(size_t)t * V + i];
-            const bool last_tail = (t + 1 < ntiles) ? (a.tail_key != aggs[t + 1].head_key) : true;
-            cpre += a.tails + ((last_tail & (a.tail_valid != 0)) ? 1u : 0u);
-        }
-        if (threadIdx.x == nt - 1)
-            *n_groups = cinc;
+        if (threadIdx.x == 0)
+            *n_groups = cnt_prev;
     }
 
     // pass C
