@@ -90,6 +90,25 @@ __device__ __forceinline__ int64_t warp_sum_i64(int64_t x)
     return x;
 }
 
+// Warp reduce-scatter of 32 int64 values a lane: five halving steps (each
+// lane keeps the half its lane bit selects and adds the partner's copy of
+// it); afterwards a[0] of lane L is the warp sum of value L.
+__device__ __forceinline__ void warp_reduce_scatter32(int64_t (&a)[32], int lane)
+{
+#pragma unroll
+    for (int step = 0; step < 5; step++) {
+        const int o = 16 >> step;
+        const int h = 16 >> step; // current length / 2
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < h; k++) {
+            const int64_t keep = up ? a[h + k] : a[k];
+            const int64_t send = up ? a[k] : a[h + k];
+            a[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+}
+
 // Agg: static constexpr int W (record words), V (values); struct Params
 //      (public decoding parameters passed to every pass);
 //      static uint64_t key(const uint64_t* w)      -- run key (includes validity)
@@ -449,35 +468,45 @@ struct SegAgg {
         // every row is folded into every slot with a mask
         __syncthreads();
         int64_t* red = reinterpret_cast<int64_t*>(smem); // reuse the tile area
-        for (int j = 0; j < G; j++) {
-            int64_t acc[1 + V];
+        // slots in chunks of 4: every lane folds its rows into 4 x 8 values
+        // (slot, value; values past 1+V stay zero), then a warp reduce-scatter
+        // leaves lane L with the warp sum of value L
+        static_assert(1 + V <= 8, "a slot's key and values fit 8 words");
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int j0 = 0; j0 < G; j0 += 4) {
+            int64_t acc[32];
 #pragma unroll
-            for (int i = 0; i <= V; i++)
-                acc[i] = 0;
+            for (int q = 0; q < 32; q++)
+                acc[q] = 0;
             uint32_t rank = rank0;
 #pragma unroll
             for (int r = 0; r < SEG_RPT; r++) {
-                const bool hit = tail[r] & (rank == (uint32_t)j);
-                acc[0] += hit ? Agg::out_key_from(keys[r]) : 0;
+                const int64_t kv = Agg::out_key_from(keys[r]);
 #pragma unroll
-                for (int i = 0; i < V; i++)
-                    acc[1 + i] += hit ? pref[r][i] : 0;
+                for (int jj = 0; jj < 4; jj++) {
+                    const bool hit = tail[r] & (rank == (uint32_t)(j0 + jj));
+                    acc[jj * 8] += hit ? kv : 0;
+#pragma unroll
+                    for (int i = 0; i < V; i++)
+                        acc[jj * 8 + 1 + i] += hit ? pref[r][i] : 0;
+                }
                 rank += tail[r] ? 1u : 0u;
             }
+            warp_reduce_scatter32(acc, lane);
+            red[lane * 8 + warp] = acc[0];
+            __syncthreads();
+            const int gn = G - j0 < 4 ? G - j0 : 4;
+            for (int q = threadIdx.x; q < gn * (1 + V); q += SEG_THREADS) {
+                const int jj = q / (1 + V), i = q - jj * (1 + V);
+                const size_t o = (size_t)tile * G * (1 + V) + (size_t)(j0 + jj) * (1 + V) + i;
+                VELO_TRACE_AT(TS_SEG_OUT, tile_out + o);
+                int64_t sum = 0;
 #pragma unroll
-            for (int i = 0; i <= V; i++) {
-                const int64_t sum = warp_sum_i64(acc[i]);
-                if ((threadIdx.x & 31) == 0)
-                    red[(j * (1 + V) + i) * 8 + (threadIdx.x >> 5)] = sum;
+                for (int w = 0; w < SEG_THREADS / 32; w++)
+                    sum += red[(jj * 8 + i) * 8 + w];
+                tile_out[o] = sum;
             }
-        }
-        __syncthreads();
-        for (int q = threadIdx.x; q < G * (1 + V); q += SEG_THREADS) {
-            VELO_TRACE_AT(TS_SEG_OUT, tile_out + (size_t)tile * G * (1 + V) + q);
-            int64_t sum = 0;
-            for (int w = 0; w < SEG_THREADS / 32; w++)
-                sum += red[q * 8 + w];
-            tile_out[(size_t)tile * G * (1 + V) + q] = sum;
+            __syncthreads();
         }
     }
 
