@@ -322,14 +322,9 @@ static velo_status run_groupby(const LiScratch& s, const LiCols& c, size_t n, co
         VELO_CUDA_TRY(cudaStreamSynchronize(st), "cudaStreamSynchronize");
         logS = ilog2_floor(next_pow2(cnt ? cnt : 1));
     }
-    if (logS > 0) {
-        std::vector<NetPass> passes;
-        plan_sort(logS, LI_LT, LI_LMAX, passes);
-        NetGeom g { (size_t)1 << logS, logS, 0 };
-        rc = launch_net12<Rec>(rc3, g, passes, nullptr, st);
-        if (rc != VELO_OK)
-            return rc;
-    }
+    rc = launch_sort_records<Rec>(rc3, logS, st);
+    if (rc != VELO_OK)
+        return rc;
     tm.mark();
     // 4. segmented sums with public output bound
     size_t nseg = (size_t)1 << logS;

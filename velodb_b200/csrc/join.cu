@@ -421,13 +421,9 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     uc.mark_inv = 0;
     uc.mark_word = 0;
     // 2. sort the union on (key, tag)
-    if (logU > 0) {
-        std::vector<NetPass> passes;
-        plan_sort(logU, J_LT, J_LMAX, passes);
-        rc = launch_net12<JRec>(uc, NetGeom { (size_t)1 << logU, logU, 0 }, passes, nullptr, st);
-        if (rc != VELO_OK)
-            return rc;
-    }
+    rc = launch_sort_records<JRec>(uc, logU, st);
+    if (rc != VELO_OK)
+        return rc;
     tm.mark();
     // 3. forward fill of the dimension side -> joined flag
     const int ntf = (int)(s.n_rec / FILL_TS);

@@ -210,7 +210,7 @@ struct Net {
             bool d = dm;
             if constexpr (PER_E)
                 d = (dpat & (1u << e)) != 0u;
-            R::cswap(v[e], v[e2], R::swap_pred(v[e], v[e2], d, c));
+            Cswap<R, Q & 1>::run(v[e], v[e2], R::swap_pred(v[e], v[e2], d, c));
         }
     }
 
