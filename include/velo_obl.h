@@ -439,9 +439,10 @@ typedef struct velo_join_pred {
  * (include/cuda/sort_merge_join.cuh:63-199,
  * src/operator/sort_merge_join_operator.cpp:27-257) with union -> bitonic
  * sort on (key, tag) -> forward fill -> ORCompact -> segmented sums ->
- * ORCompact of the groups (public bound n_dim) -> bitonic sort on
- * (sum desc, fk asc).  d_out: k rows x 3 int64 = (fk, sum price, count),
- * unused rows zero.  d_counts: 2 u64 = (joined fact rows, groups). */
+ * bitonic top-k network on (sum desc, fk asc) (each group-by tile keeps its
+ * best max(16, next_pow2(k)) groups, then rounds over candidate blocks).
+ * k is 1..1024.  d_out: k rows x 3 int64 = (fk, sum price, count), unused
+ * rows zero.  d_counts: 2 u64 = (joined fact rows, groups). */
 size_t velo_join_groupby_topk_scratch_bytes(size_t n_dim, size_t n_fact);
 velo_status velo_join_groupby_topk(const velo_join_tables* tables, const velo_join_pred* pred, uint32_t k,
                                    int64_t* d_out, uint64_t* d_counts, void* d_scratch, size_t scratch_bytes,
