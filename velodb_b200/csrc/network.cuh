@@ -149,7 +149,13 @@ struct Net {
 
     static constexpr size_t smem_rows() { return ((size_t)T * R::SMEM_BYTES + 15) & ~(size_t)15; }
     static constexpr size_t smem_bytes_sort() { return smem_rows(); }
-    static constexpr size_t smem_bytes_compact() { return smem_rows() + (size_t)T * 4 + 33 * 4; }
+    // the tile prefix array holds one pad word after every 16 (ppos)
+    static constexpr size_t smem_bytes_compact() { return smem_rows() + (size_t)(T + T / 16) * 4 + 33 * 4; }
+
+    // slot of tile prefix entry l: one pad word every 16 entries, so that a
+    // warp reading entries 16 apart (the block starts of the lowest levels
+    // in layout 0) hits 32 different banks instead of 2
+    __device__ __forceinline__ static int ppos(int l) { return l + (l >> 4); }
 
     // thread part of the local row index in layout s
     __device__ __forceinline__ static int tidpart(int s)
@@ -272,7 +278,7 @@ struct Net {
             const int e2 = e | (1 << Q);
             const int l = tp | (e << s);
             const int blk = l & ~(int)(2 * half - 1);
-            const uint32_t ps = p_tile + pre[blk];
+            const uint32_t ps = p_tile + pre[ppos(blk)];
             bool sw;
             if (b == 0) {
                 // compact_offset, n == 2 (algorithms.c:123-128)
@@ -280,7 +286,7 @@ struct Net {
                 sw = ((!ml) & mr) != ((ps & 1u) == 1u);
             } else {
                 // compact_offset, n > 2 (algorithms.c:130-152)
-                const uint32_t left = pre[blk + half] - pre[blk];
+                const uint32_t left = pre[ppos(blk + (int)half)] - pre[ppos(blk)];
                 const uint32_t off = ps & (2 * half - 1);
                 const uint32_t i = (uint32_t)(l - blk);
                 const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
@@ -298,25 +304,29 @@ struct Net {
                                                                 const uint32_t* gpre, int C, int b_lo,
                                                                 size_t cta_bits, int L)
     {
-        const int tp = tidpart(s);
-        const uint64_t half = 1ull << b;
+        // 32-bit index arithmetic: row indices are below 2^MAX_LOGN = 2^31,
+        // so g, 2 * half - 1 and (off + left) all fit
+        const uint32_t tp = (uint32_t)tidpart(s);
+        const uint32_t half = 1u << b;
+        const uint32_t bm = 2u * half - 1u;
         const uint32_t mmask = (1u << L) - 1u;
+        const uint32_t cb = (uint32_t)cta_bits;
+        const uint32_t cm = (1u << C) - 1u;
 #pragma unroll
         for (int e = 0; e < E; e++) {
             if (e & (1 << Q))
                 continue;
             const int e2 = e | (1 << Q);
-            const int l = tp | (e << s);
-            const uint64_t g = (uint64_t)(l & ((1 << C) - 1)) | ((uint64_t)(l >> C) << b_lo) | cta_bits;
-            const uint64_t blk = g & ~(2 * half - 1);
-            const uint32_t mb = (uint32_t)(blk >> b_lo) & mmask;
+            const uint32_t l = tp | ((uint32_t)e << s);
+            const uint32_t g = (l & cm) | ((l >> C) << b_lo) | cb;
+            const uint32_t mb = ((g & ~bm) >> b_lo) & mmask;
             const uint32_t ps = gpre[mb];
             const uint32_t pm = gpre[mb | (1u << (b - b_lo))];
-            const uint64_t left = pm - ps;
-            const uint64_t off = ps & (2 * half - 1);
-            const uint64_t i = g - blk;
-            const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
-            const bool sw = sb != (i >= ((off + left) & (half - 1)));
+            const uint32_t left = pm - ps;
+            const uint32_t off = ps & bm;
+            const uint32_t i = g & bm;
+            const bool sb = (((off & (half - 1u)) + left) >= half) != (off >= half);
+            const bool sw = sb != (i >= ((off + left) & (half - 1u)));
             R::cswap(v[e], v[e2], sw);
         }
     }
@@ -398,7 +408,7 @@ struct Net {
             if (p.kind == P_COMPACT_TILE) {
                 // prefix of the original marks over the tile, in local-index order
                 uint32_t* pre = reinterpret_cast<uint32_t*>(sm + smem_rows());
-                uint32_t* tmp = pre + T;
+                uint32_t* tmp = pre + T + T / 16;
                 transpose(v, s, 0, sm);
                 s = 0;
                 uint32_t cnt = 0, m[E];
@@ -412,7 +422,7 @@ struct Net {
                 const int tp0 = tidpart(0);
 #pragma unroll
                 for (int e = 0; e < E; e++)
-                    pre[tp0 | e] = base + m[e];
+                    pre[ppos(tp0 | e)] = base + m[e];
                 __syncthreads();
                 VELO_TRACE_AT(TS_TILE_PREFIX, tile_prefix + cta);
                 const uint32_t p_tile = __ldcg(tile_prefix + cta);
