@@ -9,8 +9,15 @@ namespace velo {
 
 // 256-thread CTAs are asked to fit two per SM (at most 128 registers a
 // thread): with one 8-warp CTA per SM the in-tile levels stall on latency.
-template <int LOG_NT>
+// Rows of at most 12 bytes also have a three-CTA form (at most 85 registers)
+// for sorts larger than L2, whose global passes need the third CTA to hide
+// HBM latency; below that the two-CTA code is faster (2^20 key-payload sort
+// 0.18 ms against 0.22 ms, 2^23 1.65 ms against 1.45 ms).
+template <class R, int LOG_NT>
 constexpr int net_min_blocks() { return LOG_NT <= 8 ? 2 : 1; }
+template <class R, int LOG_NT>
+constexpr bool net_has_wide() { return LOG_NT <= 8 && sizeof(R) <= 12; }
+constexpr int NET_WIDE_LOGN = 21; // sorts of 2^21 rows and more take the three-CTA form
 
 // Passes of one sequence are launched with programmatic stream serialization:
 // the next pass may be launched while this one drains, and waits here until
@@ -21,18 +28,20 @@ __device__ __forceinline__ void net_pass_prologue()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-template <class R, int LOG_NT, int LOG_E>
-__global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<LOG_NT>())
+// bitonic passes: the tile sort and in-tile merges (PK_LOCAL) and the fused
+// global passes (PK_GLOBAL) are separate kernels
+template <class R, int LOG_NT, int LOG_E, int PK, int MB = net_min_blocks<R, LOG_NT>()>
+__global__ void __launch_bounds__(1 << LOG_NT, MB)
     k_sort_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];
     net_pass_prologue();
     VELO_TRACE_KERNEL(TS_K_SORT_PASS);
-    Net<R, LOG_NT, LOG_E>::template run<true>(c, g, p, tile_prefix, blockIdx.x, sm);
+    Net<R, LOG_NT, LOG_E>::template run<true, PK>(c, g, p, tile_prefix, blockIdx.x, sm);
 }
 
 template <class R, int LOG_NT, int LOG_E>
-__global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<LOG_NT>())
+__global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<R, LOG_NT>())
     k_compact_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];
@@ -49,12 +58,21 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
     if (passes.empty())
         return VELO_OK;
     const bool compact = passes[0].kind == P_COMPACT_TILE || passes[0].kind == P_COMPACT_GLOBAL;
-    auto kern = compact ? k_compact_pass<R, LOG_NT, LOG_E> : k_sort_pass<R, LOG_NT, LOG_E>;
+    constexpr int MB = net_min_blocks<R, LOG_NT>();
+    constexpr int MBW = net_has_wide<R, LOG_NT>() ? 3 : MB;
+    const bool wide = MBW != MB && g.logN >= NET_WIDE_LOGN;
+    auto k_local = wide ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_LOCAL, MBW> : k_sort_pass<R, LOG_NT, LOG_E, N::PK_LOCAL, MB>;
+    auto k_global = wide ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MBW>
+                         : k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MB>;
+    auto k_comp = k_compact_pass<R, LOG_NT, LOG_E>;
     const size_t smem = compact ? N::smem_bytes_compact() : N::smem_bytes_sort();
     if (smem > MAX_SMEM_BYTES)
         return einval("tile configuration needs more shared memory than a CTA can have");
-    static int done_sort[64] = {}, done_compact[64] = {};
-    velo_status rc = ensure_smem(kern, MAX_SMEM_BYTES, compact ? done_compact : done_sort);
+    static int done_local[2][64] = {}, done_global[2][64] = {}, done_compact[64] = {};
+    velo_status rc = compact ? ensure_smem(k_comp, MAX_SMEM_BYTES, done_compact)
+                             : ensure_smem(k_local, MAX_SMEM_BYTES, done_local[wide ? 1 : 0]);
+    if (rc == VELO_OK && !compact)
+        rc = ensure_smem(k_global, MAX_SMEM_BYTES, done_global[wide ? 1 : 0]);
     if (rc != VELO_OK)
         return rc;
     const int lt = N::LT;
@@ -72,6 +90,7 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
         cfg.stream = st;
         cfg.attrs = attr;
         cfg.numAttrs = i > 0 ? 1 : 0;
+        auto kern = compact ? k_comp : passes[i].kind == P_SORT_GLOBAL ? k_global : k_local;
         VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, c, g, passes[i], tile_prefix), "network pass launch");
     }
     return VELO_OK;

@@ -184,9 +184,57 @@ struct Net {
         }
     }
 
+    // Transposes with the layout as a compile-time value (CT): the code for
+    // layout S is picked at run time among 0 .. LT - LOG_E by a compare chain,
+    // and each register's slot is the thread's base XOR a constant, instead
+    // of a per-register XOR chain over run-time basis values.  Used by the
+    // in-tile sort kernel, where transposes are a third of the ALU work.
+    template <int S>
+    __device__ __forceinline__ static int ct_base()
+    {
+        const int tp = (int)(threadIdx.x & ((1u << S) - 1)) | (int)((threadIdx.x >> S) << (S + LOG_E));
+        return TL::template swz<SWZ>(tp);
+    }
+    template <int S = 0>
+    __device__ __forceinline__ static void store_ct(const R (&v)[E], int s, char* sm)
+    {
+        if constexpr (S <= LT - LOG_E) {
+            if (s == S) {
+                const int base = ct_base<S>();
+#pragma unroll
+                for (int e = 0; e < E; e++)
+                    R::sstore(sm, T, base ^ TL::template swz<SWZ>(e << S), v[e]);
+            } else {
+                store_ct<S + 1>(v, s, sm);
+            }
+        }
+    }
+    template <int S = 0>
+    __device__ __forceinline__ static void load_ct(R (&v)[E], int s, const char* sm)
+    {
+        if constexpr (S <= LT - LOG_E) {
+            if (s == S) {
+                const int base = ct_base<S>();
+#pragma unroll
+                for (int e = 0; e < E; e++)
+                    v[e] = R::sload(sm, T, base ^ TL::template swz<SWZ>(e << S));
+            } else {
+                load_ct<S + 1>(v, s, sm);
+            }
+        }
+    }
+
     // re-layout the tile from layout `from` to layout `to` through smem
+    template <bool CT = false>
     __device__ __forceinline__ static void transpose(R (&v)[E], int from, int to, char* sm)
     {
+        if constexpr (CT) {
+            __syncthreads();
+            store_ct(v, from, sm);
+            __syncthreads();
+            load_ct(v, to, sm);
+            return;
+        }
         int slot[E];
         __syncthreads();
         slots(from, slot);
@@ -333,12 +381,18 @@ struct Net {
 
     // ---- one pass over one tile (CTA `cta`) --------------------------------
     // SORT = true compiles only the bitonic pass kinds, false only ORCompact.
-    template <bool SORT>
+    // PK: the pass kinds this instantiation handles (a separate kernel each,
+    // so that each gets its own register allocation)
+    enum : int { PK_ANY = 0, PK_LOCAL = 1, PK_GLOBAL = 2 };
+    template <bool SORT, int PK = PK_ANY>
     __device__ static void run(const Cols& c, const NetGeom& g, const NetPass& p, const uint32_t* tile_prefix,
                                int cta, char* sm)
     {
+        constexpr bool CT = SORT && PK == PK_LOCAL;
         const size_t Np = (size_t)1 << g.logN;
-        const bool is_global = (p.kind == P_SORT_GLOBAL) || (p.kind == P_COMPACT_GLOBAL);
+        const bool is_global = PK == PK_GLOBAL ? true
+            : PK == PK_LOCAL                   ? false
+                                               : (p.kind == P_SORT_GLOBAL) || (p.kind == P_COMPACT_GLOBAL);
         int C = LT, b_lo = 0;
         size_t cta_bits = (size_t)cta << LT;
         if (is_global) {
@@ -370,7 +424,7 @@ struct Net {
         }
 
         if constexpr (SORT) {
-            if (p.kind == P_SORT_TILE) {
+            if (PK != PK_GLOBAL && p.kind == P_SORT_TILE) {
                 for (int K = 1; K <= p.K; K++) {
                     const bool dconst = K >= LT;
                     const bool asc_c = ((cta_bits >> K) & 1) == 0;
@@ -378,7 +432,7 @@ struct Net {
                     while (b >= 0) {
                         if (b < s || b >= s + LOG_E) {
                             const int ns = window_down(b, LOG_E, LT);
-                            transpose(v, s, ns, sm);
+                            transpose<CT>(v, s, ns, sm);
                             s = ns;
                         }
                         bitonic_window(v, c, s, b, s, K, dconst, asc_c);
@@ -396,7 +450,7 @@ struct Net {
                     if (b < s || b >= s + LOG_E) {
                         int ns = window_down(b, LOG_E, LT);
                         ns = ns < smin ? smin : ns;
-                        transpose(v, s, ns, sm);
+                        transpose<CT>(v, s, ns, sm);
                         s = ns;
                     }
                     const int lo = s > bottom ? s : bottom;
@@ -409,7 +463,7 @@ struct Net {
                 // prefix of the original marks over the tile, in local-index order
                 uint32_t* pre = reinterpret_cast<uint32_t*>(sm + smem_rows());
                 uint32_t* tmp = pre + T + T / 16;
-                transpose(v, s, 0, sm);
+                transpose<CT>(v, s, 0, sm);
                 s = 0;
                 uint32_t cnt = 0, m[E];
 #pragma unroll
@@ -430,7 +484,7 @@ struct Net {
                 while (b < p.K) {
                     if (b < s || b >= s + LOG_E) {
                         const int ns = window_up(b, LOG_E, LT);
-                        transpose(v, s, ns, sm);
+                        transpose<CT>(v, s, ns, sm);
                         s = ns;
                     }
                     const int hi = (s + LOG_E - 1 < p.K - 1) ? s + LOG_E - 1 : p.K - 1;
@@ -468,7 +522,7 @@ struct Net {
                     if (lb < s || lb >= s + LOG_E) {
                         int ns = window_up(lb, LOG_E, LT);
                         ns = ns < smin ? smin : ns;
-                        transpose(v, s, ns, sm);
+                        transpose<CT>(v, s, ns, sm);
                         s = ns;
                     }
                     const int hi = (s + LOG_E - 1 < top) ? s + LOG_E - 1 : top;
@@ -493,7 +547,7 @@ struct Net {
         }
 
         if (s < 5) {
-            transpose(v, s, S0, sm);
+            transpose<CT>(v, s, S0, sm);
             s = S0;
         }
         {
