@@ -64,6 +64,22 @@ def test_osort_kp_ties_keep_network_arrangement(cuda, orc):
         assert np.array_equal(gk, ok) and np.array_equal(gp, op)
 
 
+@pytest.mark.parametrize("logn", [21, 22])
+def test_osort_kp_three_cta_form_bit_exact(cuda, orc, logn):
+    # from 2^21 rows the passes run in their three-CTA-per-SM form
+    n = 1 << logn
+    keys, pay = W.sort_kp(n, seed=W.SEED_SORT + logn)
+    gk, gp = gpu_sort_kp(keys, pay)
+    ok, op = orc.bitonic_kp(keys, pay)
+    assert np.array_equal(gk, ok) and np.array_equal(gp, op)
+    rng = np.random.default_rng(logn)
+    keys = rng.integers(0, 5, n).astype(np.uint64)  # ties: the network's own arrangement
+    pay = rng.integers(0, 3, n).astype(np.uint32)
+    gk, gp = gpu_sort_kp(keys, pay)
+    ok, op = orc.bitonic_kp(keys, pay)
+    assert np.array_equal(gk, ok) and np.array_equal(gp, op)
+
+
 def test_osort_kp_large_property(cuda):
     # 2^23 rows: beyond what the oracle does in seconds; check order + multiset
     n = 1 << 23
