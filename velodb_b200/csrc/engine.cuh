@@ -200,6 +200,17 @@ struct RowKP {
     {
         reinterpret_cast<uint4*>(sm)[i] = make_uint4(r.kl, r.kh, r.p, 0u);
     }
+    // the same at byte offset `b` = slot * SLOT_BYTES
+    static constexpr int SLOT_BYTES = 16;
+    __device__ __forceinline__ static void sstore_b(char* sm, int, uint32_t b, const RowKP& r)
+    {
+        *reinterpret_cast<uint4*>(sm + b) = make_uint4(r.kl, r.kh, r.p, 0u);
+    }
+    __device__ __forceinline__ static RowKP sload_b(const char* sm, int, uint32_t b)
+    {
+        const uint4 x = *reinterpret_cast<const uint4*>(sm + b);
+        return RowKP { x.x, x.y, x.z };
+    }
     __device__ __forceinline__ static RowKP sload(const char* sm, int, int i)
     {
         const uint4 x = reinterpret_cast<const uint4*>(sm)[i];
@@ -249,6 +260,16 @@ struct RowKPM {
     __device__ __forceinline__ static void sstore(char* sm, int, int i, const RowKPM& r)
     {
         reinterpret_cast<uint4*>(sm)[i] = make_uint4(r.kl, r.kh, r.p, r.m);
+    }
+    static constexpr int SLOT_BYTES = 16;
+    __device__ __forceinline__ static void sstore_b(char* sm, int, uint32_t b, const RowKPM& r)
+    {
+        *reinterpret_cast<uint4*>(sm + b) = make_uint4(r.kl, r.kh, r.p, r.m);
+    }
+    __device__ __forceinline__ static RowKPM sload_b(const char* sm, int, uint32_t b)
+    {
+        const uint4 x = *reinterpret_cast<const uint4*>(sm + b);
+        return RowKPM { x.x, x.y, x.z, x.w };
     }
     __device__ __forceinline__ static RowKPM sload(const char* sm, int, int i)
     {
@@ -316,6 +337,35 @@ struct RowRec {
 #pragma unroll
         for (int i = 0; i < W; i++)
             r.w[i] = c.pad[i];
+        return r;
+    }
+    // slot at byte offset b = slot * SLOT_BYTES (words past the second in
+    // 8-byte arrays at b / 2)
+    static constexpr int SLOT_BYTES = W == 1 ? 8 : 16;
+    __device__ __forceinline__ static void sstore_b(char* sm, int T, uint32_t b, const RowRec& r)
+    {
+        if constexpr (W == 1) {
+            *reinterpret_cast<uint64_t*>(sm + b) = r.w[0];
+        } else {
+            *reinterpret_cast<ulonglong2*>(sm + b) = make_ulonglong2(r.w[0], r.w[1]);
+#pragma unroll
+            for (int x = 2; x < W; x++)
+                *reinterpret_cast<uint64_t*>(sm + (size_t)16 * T + (size_t)8 * T * (x - 2) + (b >> 1)) = r.w[x];
+        }
+    }
+    __device__ __forceinline__ static RowRec sload_b(const char* sm, int T, uint32_t b)
+    {
+        RowRec r;
+        if constexpr (W == 1) {
+            r.w[0] = *reinterpret_cast<const uint64_t*>(sm + b);
+        } else {
+            const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(sm + b);
+            r.w[0] = x.x;
+            r.w[1] = x.y;
+#pragma unroll
+            for (int y = 2; y < W; y++)
+                r.w[y] = *reinterpret_cast<const uint64_t*>(sm + (size_t)16 * T + (size_t)8 * T * (y - 2) + (b >> 1));
+        }
         return r;
     }
     __device__ __forceinline__ static void sstore(char* sm, int T, int i, const RowRec& r)

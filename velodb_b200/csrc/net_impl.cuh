@@ -37,7 +37,8 @@ __global__ void __launch_bounds__(1 << LOG_NT, MB)
     extern __shared__ __align__(16) char sm[];
     net_pass_prologue();
     VELO_TRACE_KERNEL(TS_K_SORT_PASS);
-    Net<R, LOG_NT, LOG_E>::template run<true, PK>(c, g, p, tile_prefix, blockIdx.x, sm);
+    Net<R, LOG_NT, LOG_E>::template run<true, PK, (MB > net_min_blocks<R, LOG_NT>())>(c, g, p, tile_prefix, blockIdx.x,
+                                                                                     sm);
 }
 
 template <class R, int LOG_NT, int LOG_E>

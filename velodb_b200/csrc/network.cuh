@@ -195,44 +195,61 @@ struct Net {
         const int tp = (int)(threadIdx.x & ((1u << S) - 1)) | (int)((threadIdx.x >> S) << (S + LOG_E));
         return TL::template swz<SWZ>(tp);
     }
-    template <int S = 0>
+    // BOFF: XOR on byte offsets, (base ^ c) * SZ == (base * SZ) ^ (c * SZ),
+    // so no multiply per register; the three-CTA forms (at most 85
+    // registers) keep slot indices, measured faster there
+    template <bool BOFF, int S = 0>
     __device__ __forceinline__ static void store_ct(const R (&v)[E], int s, char* sm)
     {
         if constexpr (S <= LT - LOG_E) {
             if (s == S) {
-                const int base = ct_base<S>();
+                if constexpr (BOFF) {
+                    const uint32_t bb = (uint32_t)ct_base<S>() * R::SLOT_BYTES;
 #pragma unroll
-                for (int e = 0; e < E; e++)
-                    R::sstore(sm, T, base ^ TL::template swz<SWZ>(e << S), v[e]);
+                    for (int e = 0; e < E; e++)
+                        R::sstore_b(sm, T, bb ^ (uint32_t)(TL::template swz<SWZ>(e << S) * R::SLOT_BYTES), v[e]);
+                } else {
+                    const int base = ct_base<S>();
+#pragma unroll
+                    for (int e = 0; e < E; e++)
+                        R::sstore(sm, T, base ^ TL::template swz<SWZ>(e << S), v[e]);
+                }
             } else {
-                store_ct<S + 1>(v, s, sm);
+                store_ct<BOFF, S + 1>(v, s, sm);
             }
         }
     }
-    template <int S = 0>
+    template <bool BOFF, int S = 0>
     __device__ __forceinline__ static void load_ct(R (&v)[E], int s, const char* sm)
     {
         if constexpr (S <= LT - LOG_E) {
             if (s == S) {
-                const int base = ct_base<S>();
+                if constexpr (BOFF) {
+                    const uint32_t bb = (uint32_t)ct_base<S>() * R::SLOT_BYTES;
 #pragma unroll
-                for (int e = 0; e < E; e++)
-                    v[e] = R::sload(sm, T, base ^ TL::template swz<SWZ>(e << S));
+                    for (int e = 0; e < E; e++)
+                        v[e] = R::sload_b(sm, T, bb ^ (uint32_t)(TL::template swz<SWZ>(e << S) * R::SLOT_BYTES));
+                } else {
+                    const int base = ct_base<S>();
+#pragma unroll
+                    for (int e = 0; e < E; e++)
+                        v[e] = R::sload(sm, T, base ^ TL::template swz<SWZ>(e << S));
+                }
             } else {
-                load_ct<S + 1>(v, s, sm);
+                load_ct<BOFF, S + 1>(v, s, sm);
             }
         }
     }
 
     // re-layout the tile from layout `from` to layout `to` through smem
-    template <bool CT = false>
+    template <bool CT = false, bool BOFF = true>
     __device__ __forceinline__ static void transpose(R (&v)[E], int from, int to, char* sm)
     {
         if constexpr (CT) {
             __syncthreads();
-            store_ct(v, from, sm);
+            store_ct<BOFF>(v, from, sm);
             __syncthreads();
-            load_ct(v, to, sm);
+            load_ct<BOFF>(v, to, sm);
             return;
         }
         int slot[E];
@@ -384,11 +401,12 @@ struct Net {
     // PK: the pass kinds this instantiation handles (a separate kernel each,
     // so that each gets its own register allocation)
     enum : int { PK_ANY = 0, PK_LOCAL = 1, PK_GLOBAL = 2 };
-    template <bool SORT, int PK = PK_ANY>
+    template <bool SORT, int PK = PK_ANY, bool WIDE = false>
     __device__ static void run(const Cols& c, const NetGeom& g, const NetPass& p, const uint32_t* tile_prefix,
                                int cta, char* sm)
     {
         constexpr bool CT = SORT && PK == PK_LOCAL;
+        constexpr bool BOFF = !WIDE;
         const size_t Np = (size_t)1 << g.logN;
         const bool is_global = PK == PK_GLOBAL ? true
             : PK == PK_LOCAL                   ? false
@@ -432,7 +450,7 @@ struct Net {
                     while (b >= 0) {
                         if (b < s || b >= s + LOG_E) {
                             const int ns = window_down(b, LOG_E, LT);
-                            transpose<CT>(v, s, ns, sm);
+                            transpose<CT, BOFF>(v, s, ns, sm);
                             s = ns;
                         }
                         bitonic_window(v, c, s, b, s, K, dconst, asc_c);
@@ -450,7 +468,7 @@ struct Net {
                     if (b < s || b >= s + LOG_E) {
                         int ns = window_down(b, LOG_E, LT);
                         ns = ns < smin ? smin : ns;
-                        transpose<CT>(v, s, ns, sm);
+                        transpose<CT, BOFF>(v, s, ns, sm);
                         s = ns;
                     }
                     const int lo = s > bottom ? s : bottom;
@@ -463,7 +481,7 @@ struct Net {
                 // prefix of the original marks over the tile, in local-index order
                 uint32_t* pre = reinterpret_cast<uint32_t*>(sm + smem_rows());
                 uint32_t* tmp = pre + T + T / 16;
-                transpose<CT>(v, s, 0, sm);
+                transpose<CT, BOFF>(v, s, 0, sm);
                 s = 0;
                 uint32_t cnt = 0, m[E];
 #pragma unroll
@@ -484,7 +502,7 @@ struct Net {
                 while (b < p.K) {
                     if (b < s || b >= s + LOG_E) {
                         const int ns = window_up(b, LOG_E, LT);
-                        transpose<CT>(v, s, ns, sm);
+                        transpose<CT, BOFF>(v, s, ns, sm);
                         s = ns;
                     }
                     const int hi = (s + LOG_E - 1 < p.K - 1) ? s + LOG_E - 1 : p.K - 1;
@@ -522,7 +540,7 @@ struct Net {
                     if (lb < s || lb >= s + LOG_E) {
                         int ns = window_up(lb, LOG_E, LT);
                         ns = ns < smin ? smin : ns;
-                        transpose<CT>(v, s, ns, sm);
+                        transpose<CT, BOFF>(v, s, ns, sm);
                         s = ns;
                     }
                     const int hi = (s + LOG_E - 1 < top) ? s + LOG_E - 1 : top;
@@ -547,7 +565,7 @@ struct Net {
         }
 
         if (s < 5) {
-            transpose<CT>(v, s, S0, sm);
+            transpose<CT, BOFF>(v, s, S0, sm);
             s = S0;
         }
         {
