@@ -100,14 +100,67 @@ __device__ __forceinline__ DimCarry dim_combine(const DimCarry& left, const DimC
 
 constexpr int FILL_TS = 2048, FILL_THREADS = 256, FILL_RPT = FILL_TS / FILL_THREADS;
 
+__device__ __forceinline__ DimCarry dim_shfl(const DimCarry& c, int src_delta, bool up)
+{
+    DimCarry r;
+    const uint32_t hv = c.has | (c.valid << 1);
+    const uint32_t x = up ? __shfl_up_sync(0xFFFFFFFFu, hv, src_delta) : __shfl_xor_sync(0xFFFFFFFFu, hv, src_delta);
+    r.key = up ? __shfl_up_sync(0xFFFFFFFFu, c.key, src_delta) : __shfl_xor_sync(0xFFFFFFFFu, c.key, src_delta);
+    r.has = x & 1u;
+    r.valid = (x >> 1) & 1u;
+    return r;
+}
+
+// Block-wide exclusive scan of "the last dimension row" (warp shuffles, then
+// one shared-memory round over the warp totals); wsm holds 33 entries.
+__device__ __forceinline__ DimCarry block_dim_scan_excl(const DimCarry& mine, DimCarry* wsm, DimCarry* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    DimCarry inc = mine;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const DimCarry y = dim_shfl(inc, off, true);
+        if (lane >= off)
+            inc = dim_combine(y, inc);
+    }
+    __syncthreads(); // wsm may still be read by a previous call
+    if (lane == 31)
+        wsm[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        DimCarry z = lane < nw ? wsm[lane] : DimCarry { 0, 0, 0 };
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const DimCarry y = dim_shfl(z, off, true);
+            if (lane >= off)
+                z = dim_combine(y, z);
+        }
+        DimCarry ez = dim_shfl(z, 1, true);
+        if (lane == 0)
+            ez = DimCarry { 0, 0, 0 };
+        __syncwarp();
+        if (lane < nw)
+            wsm[lane] = ez;
+        if (lane == nw - 1)
+            wsm[32] = z; // block total
+    }
+    __syncthreads();
+    DimCarry ex = dim_shfl(inc, 1, true);
+    if (lane == 0)
+        ex = DimCarry { 0, 0, 0 };
+    if (total)
+        *total = wsm[32];
+    return dim_combine(wsm[warp], ex);
+}
+
 __global__ void __launch_bounds__(FILL_THREADS) k_fill_summary(const uint64_t* w0, DimCarry* tile_last)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_fill_summary"));
     // the tile's last dimension row: every thread keeps the last one of its
     // stride (rows are visited in increasing order), then a max-index
-    // reduction picks the overall last
-    __shared__ DimCarry sm[FILL_THREADS];
-    __shared__ int idx[FILL_THREADS];
+    // reduction (warp shuffles, one shared-memory round) picks the overall last
+    __shared__ DimCarry sm[FILL_THREADS / 32];
+    __shared__ int idx[FILL_THREADS / 32];
     const size_t base = (size_t)blockIdx.x * FILL_TS;
     DimCarry c { 0, 0, 0 };
     int last = -1;
@@ -117,46 +170,50 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_summary(const uint64_t* w
         c = dim_combine(c, d);
         last = d.has ? i : last;
     }
-    sm[threadIdx.x] = c;
-    idx[threadIdx.x] = last;
-    __syncthreads();
-    for (int off = FILL_THREADS / 2; off > 0; off >>= 1) {
-        if ((int)threadIdx.x < off) {
-            const int x = idx[threadIdx.x], y = idx[threadIdx.x + off];
-            const bool take_y = y > x;
-            sm[threadIdx.x] = take_y ? sm[threadIdx.x + off] : sm[threadIdx.x];
-            idx[threadIdx.x] = take_y ? y : x;
-        }
-        __syncthreads();
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const DimCarry oc = dim_shfl(c, off, false);
+        const int oi = __shfl_xor_sync(0xFFFFFFFFu, last, off);
+        const bool take = oi > last;
+        c = take ? oc : c;
+        last = take ? oi : last;
     }
-    if (threadIdx.x == 0)
-        tile_last[blockIdx.x] = sm[0];
+    if ((threadIdx.x & 31) == 0) {
+        sm[threadIdx.x >> 5] = c;
+        idx[threadIdx.x >> 5] = last;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DimCarry b = sm[0];
+        int bi = idx[0];
+        for (int w = 1; w < FILL_THREADS / 32; w++) {
+            const bool take = idx[w] > bi;
+            b = take ? sm[w] : b;
+            bi = take ? idx[w] : bi;
+        }
+        tile_last[blockIdx.x] = b;
+    }
 }
 
-// exclusive "last dimension row" scan over tiles; one CTA of 1024 threads
+// exclusive "last dimension row" scan over tiles; one CTA of 1024 threads,
+// rounds of 1024 consecutive tiles chained through the running carry
 __global__ void __launch_bounds__(1024) k_fill_carries(const DimCarry* tile_last, int ntiles, DimCarry* carry)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_fill_carries"));
-    __shared__ DimCarry sm[1024];
-    const int per = (ntiles + 1023) / 1024;
-    const int t0 = threadIdx.x * per, t1 = min(ntiles, t0 + per);
-    DimCarry c { 0, 0, 0 };
-    for (int t = t0; t < t1; t++) {
-        VELO_TRACE_AT(TS_FILL, tile_last + t);
-        c = dim_combine(c, tile_last[t]);
-    }
-    sm[threadIdx.x] = c;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        DimCarry prev = (int)threadIdx.x >= off ? sm[threadIdx.x - off] : DimCarry { 0, 0, 0 };
-        __syncthreads();
-        sm[threadIdx.x] = dim_combine(prev, sm[threadIdx.x]);
-        __syncthreads();
-    }
-    DimCarry run = threadIdx.x > 0 ? sm[threadIdx.x - 1] : DimCarry { 0, 0, 0 };
-    for (int t = t0; t < t1; t++) {
-        carry[t] = run;
-        run = dim_combine(run, tile_last[t]);
+    __shared__ DimCarry wsm[33];
+    DimCarry run { 0, 0, 0 };
+    for (int base = 0; base < ntiles; base += blockDim.x) {
+        const int t = base + (int)threadIdx.x;
+        DimCarry x { 0, 0, 0 };
+        if (t < ntiles) {
+            VELO_TRACE_AT(TS_FILL, tile_last + t);
+            x = tile_last[t];
+        }
+        DimCarry total;
+        const DimCarry ex = block_dim_scan_excl(x, wsm, &total);
+        if (t < ntiles)
+            carry[t] = dim_combine(run, ex);
+        run = dim_combine(run, total);
     }
 }
 
@@ -164,7 +221,7 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_apply(uint64_t* w0, const
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_fill_apply"));
     __shared__ uint64_t sw[FILL_TS];
-    __shared__ DimCarry st[FILL_THREADS];
+    __shared__ DimCarry wsm[33];
     const size_t base = (size_t)blockIdx.x * FILL_TS;
     for (int i = threadIdx.x; i < FILL_TS; i += FILL_THREADS) {
         VELO_TRACE_AT(TS_FILL, w0 + base + i);
@@ -176,15 +233,8 @@ __global__ void __launch_bounds__(FILL_THREADS) k_fill_apply(uint64_t* w0, const
 #pragma unroll
     for (int r = 0; r < FILL_RPT; r++)
         mine = dim_combine(mine, dim_of(sw[r0 + r]));
-    st[threadIdx.x] = mine;
-    __syncthreads();
-    for (int off = 1; off < FILL_THREADS; off <<= 1) {
-        DimCarry prev = (int)threadIdx.x >= off ? st[threadIdx.x - off] : DimCarry { 0, 0, 0 };
-        __syncthreads();
-        st[threadIdx.x] = dim_combine(prev, st[threadIdx.x]);
-        __syncthreads();
-    }
-    DimCarry run = dim_combine(carry[blockIdx.x], threadIdx.x > 0 ? st[threadIdx.x - 1] : DimCarry { 0, 0, 0 });
+    const DimCarry ex = block_dim_scan_excl(mine, wsm, nullptr);
+    DimCarry run = dim_combine(carry[blockIdx.x], ex);
 #pragma unroll
     for (int r = 0; r < FILL_RPT; r++) {
         const uint64_t a = sw[r0 + r];
