@@ -9,14 +9,25 @@ namespace velo {
 
 // 256-thread CTAs are asked to fit two per SM (at most 128 registers a
 // thread): with one 8-warp CTA per SM the in-tile levels stall on latency.
-// Rows of at most 12 bytes also have a three-CTA form (at most 85 registers)
-// for sorts larger than L2, whose global passes need the third CTA to hide
-// HBM latency; below that the two-CTA code is faster (2^20 key-payload sort
-// 0.18 ms against 0.22 ms, 2^23 1.65 ms against 1.45 ms).
+// Some row types also have a three-CTA form (at most 85 registers) for sorts
+// of 2^21 rows and more, whose passes need the third CTA to hide latency;
+// below that the two-CTA code is faster (2^20 key-payload sort 0.18 ms
+// against 0.22 ms, 2^23 1.65 ms against 1.45 ms).
 template <class R, int LOG_NT>
 constexpr int net_min_blocks() { return LOG_NT <= 8 ? 2 : 1; }
+// rows of at most 12 bytes, and two-word records keyed on 32 bits (the
+// group-by's: 2^23-row sort 1.78 -> 1.63 ms); two-word records compared on a
+// whole word need their 128 registers (measured 1 % slower at 85)
+template <class R>
+struct NetWide {
+    static constexpr bool ok = sizeof(R) <= 12;
+};
+template <bool S>
+struct NetWide<RowRec<2, 1, S, KEY_HI32>> {
+    static constexpr bool ok = true;
+};
 template <class R, int LOG_NT>
-constexpr bool net_has_wide() { return LOG_NT <= 8 && sizeof(R) <= 12; }
+constexpr bool net_has_wide() { return LOG_NT <= 8 && NetWide<R>::ok; }
 constexpr int NET_WIDE_LOGN = 21; // sorts of 2^21 rows and more take the three-CTA form
 
 // Passes of one sequence are launched with programmatic stream serialization:

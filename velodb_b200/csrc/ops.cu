@@ -192,6 +192,60 @@ __device__ __forceinline__ FillCarry fill_combine(const FillCarry& l, const Fill
 
 constexpr int FL_TS = 2048, FL_THREADS = 256, FL_RPT = FL_TS / FL_THREADS;
 
+__device__ __forceinline__ FillCarry fill_shfl(const FillCarry& c, int d, bool up)
+{
+    FillCarry r;
+    const uint32_t hv = c.has | (c.valid << 1);
+    const uint32_t x = up ? __shfl_up_sync(0xFFFFFFFFu, hv, d) : __shfl_xor_sync(0xFFFFFFFFu, hv, d);
+    r.key = up ? __shfl_up_sync(0xFFFFFFFFu, c.key, d) : __shfl_xor_sync(0xFFFFFFFFu, c.key, d);
+    r.val = up ? __shfl_up_sync(0xFFFFFFFFu, c.val, d) : __shfl_xor_sync(0xFFFFFFFFu, c.val, d);
+    r.has = x & 1u;
+    r.valid = (x >> 1) & 1u;
+    return r;
+}
+
+// block-wide exclusive "last source row" scan (warp shuffles, then one
+// shared-memory round over the warp totals); wsm holds 33 entries, the
+// block total is left in wsm[32]
+__device__ __forceinline__ FillCarry block_fill_scan_excl(const FillCarry& mine, FillCarry* wsm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const FillCarry zero { 0, 0, 0, 0 };
+    FillCarry inc = mine;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const FillCarry y = fill_shfl(inc, off, true);
+        if (lane >= off)
+            inc = fill_combine(y, inc);
+    }
+    __syncthreads(); // wsm may still be read by a previous call
+    if (lane == 31)
+        wsm[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        FillCarry z = lane < nw ? wsm[lane] : zero;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const FillCarry y = fill_shfl(z, off, true);
+            if (lane >= off)
+                z = fill_combine(y, z);
+        }
+        FillCarry ez = fill_shfl(z, 1, true);
+        if (lane == 0)
+            ez = zero;
+        __syncwarp();
+        if (lane < nw)
+            wsm[lane] = ez;
+        if (lane == nw - 1)
+            wsm[32] = z;
+    }
+    __syncthreads();
+    FillCarry ex = fill_shfl(inc, 1, true);
+    if (lane == 0)
+        ex = zero;
+    return fill_combine(wsm[warp], ex);
+}
+
 // Src: static FillCarry src(w0, w1, w2) -- has = row is a source
 //      static void apply(uint64_t& w0, uint64_t& w1, uint64_t& w2, const FillCarry& last)
 template <class F>
@@ -199,8 +253,8 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, con
                                                          FillCarry* tile_last)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_fill_sum"));
-    __shared__ FillCarry sm[FL_THREADS];
-    __shared__ int idx[FL_THREADS];
+    __shared__ FillCarry sm[FL_THREADS / 32];
+    __shared__ int idx[FL_THREADS / 32];
     const size_t base = (size_t)blockIdx.x * FL_TS;
     FillCarry c { 0, 0, 0, 0 };
     int last = -1;
@@ -211,47 +265,51 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, con
         c = fill_combine(c, d);
         last = d.has ? i : last;
     }
-    sm[threadIdx.x] = c;
-    idx[threadIdx.x] = last;
-    __syncthreads();
-    for (int off = FL_THREADS / 2; off > 0; off >>= 1) {
-        if ((int)threadIdx.x < off) {
-            const int x = idx[threadIdx.x], y = idx[threadIdx.x + off];
-            const bool take_y = y > x;
-            sm[threadIdx.x] = take_y ? sm[threadIdx.x + off] : sm[threadIdx.x];
-            idx[threadIdx.x] = take_y ? y : x;
-        }
-        __syncthreads();
+    // the source row with the largest index: warp shuffles, then warp 0
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const FillCarry oc = fill_shfl(c, off, false);
+        const int oi = __shfl_xor_sync(0xFFFFFFFFu, last, off);
+        const bool take = oi > last;
+        c = take ? oc : c;
+        last = take ? oi : last;
     }
+    if ((threadIdx.x & 31) == 0) {
+        sm[threadIdx.x >> 5] = c;
+        idx[threadIdx.x >> 5] = last;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
+        FillCarry b = sm[0];
+        int bi = idx[0];
+        for (int w = 1; w < FL_THREADS / 32; w++) {
+            const bool take = idx[w] > bi;
+            b = take ? sm[w] : b;
+            bi = take ? idx[w] : bi;
+        }
         VELO_TRACE_AT(TS_FILL, tile_last + blockIdx.x);
-        tile_last[blockIdx.x] = sm[0];
+        tile_last[blockIdx.x] = b;
     }
 }
 
+// exclusive scan of the tile carries; one CTA of 1024 threads, rounds of
+// 1024 consecutive tiles chained through the running carry
 __global__ void __launch_bounds__(1024) k_fill_scan(const FillCarry* tile_last, int ntiles, FillCarry* carry)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_fill_scan"));
-    __shared__ FillCarry sm[1024];
-    const int per = (ntiles + 1023) / 1024;
-    const int t0 = threadIdx.x * per, t1 = min(ntiles, t0 + per);
-    FillCarry c { 0, 0, 0, 0 };
-    for (int t = t0; t < t1; t++) {
-        VELO_TRACE_AT(TS_FILL, tile_last + t);
-        c = fill_combine(c, tile_last[t]);
-    }
-    sm[threadIdx.x] = c;
-    __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        const FillCarry prev = (int)threadIdx.x >= off ? sm[threadIdx.x - off] : FillCarry { 0, 0, 0, 0 };
-        __syncthreads();
-        sm[threadIdx.x] = fill_combine(prev, sm[threadIdx.x]);
-        __syncthreads();
-    }
-    FillCarry run = threadIdx.x > 0 ? sm[threadIdx.x - 1] : FillCarry { 0, 0, 0, 0 };
-    for (int t = t0; t < t1; t++) {
-        carry[t] = run;
-        run = fill_combine(run, tile_last[t]);
+    __shared__ FillCarry wsm[33];
+    FillCarry run { 0, 0, 0, 0 };
+    for (int base = 0; base < ntiles; base += blockDim.x) {
+        const int t = base + (int)threadIdx.x;
+        FillCarry x { 0, 0, 0, 0 };
+        if (t < ntiles) {
+            VELO_TRACE_AT(TS_FILL, tile_last + t);
+            x = tile_last[t];
+        }
+        const FillCarry ex = block_fill_scan_excl(x, wsm);
+        if (t < ntiles)
+            carry[t] = fill_combine(run, ex);
+        run = fill_combine(run, wsm[32]);
     }
 }
 
@@ -260,7 +318,7 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_
                                                            const FillCarry* carry, unsigned long long* d_stat)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_fill_apply"));
-    __shared__ FillCarry st[FL_THREADS];
+    __shared__ FillCarry wsm[33];
     __shared__ uint32_t tmp[33];
     const size_t base = (size_t)blockIdx.x * FL_TS + (size_t)threadIdx.x * FL_RPT;
     uint64_t a[FL_RPT], b[FL_RPT], c[FL_RPT];
@@ -273,15 +331,7 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_
         c[r] = w2[base + r];
         mine = fill_combine(mine, F::src(a[r], b[r], c[r]));
     }
-    st[threadIdx.x] = mine;
-    __syncthreads();
-    for (int off = 1; off < FL_THREADS; off <<= 1) {
-        const FillCarry prev = (int)threadIdx.x >= off ? st[threadIdx.x - off] : FillCarry { 0, 0, 0, 0 };
-        __syncthreads();
-        st[threadIdx.x] = fill_combine(prev, st[threadIdx.x]);
-        __syncthreads();
-    }
-    FillCarry run = fill_combine(carry[blockIdx.x], threadIdx.x > 0 ? st[threadIdx.x - 1] : FillCarry { 0, 0, 0, 0 });
+    FillCarry run = fill_combine(carry[blockIdx.x], block_fill_scan_excl(mine, wsm));
     uint32_t stat = 0;
 #pragma unroll
     for (int r = 0; r < FL_RPT; r++) {
