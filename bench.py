@@ -38,9 +38,8 @@ sys.path.insert(0, ROOT)
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu
-# capture (profiles/k_sort_pass_groupby_rec2_2p23.md: mean of the tile,
-# global and merge passes; profiles/k_sort_pass_kp_2p20_2p24.md), or None when
-# the workload's launch is too large to capture.
+# capture (the mean over the tile, global and merge passes of one sort), or
+# None when the workload's launch is too large to capture.
 TRAFFIC = {"groupby": 210.1e6, "sort": 12.65e6, "batch": None}
 FALLBACK_HBM_GBS = 6650.0
 

@@ -150,11 +150,12 @@ size_t velo_compact_scratch_bytes(size_t capacity, const velo_tune* tune);
  * owned by its own pool allocator, a latency-critical path that cannot take
  * cudaMalloc's implicit device synchronisation, a plugin host without an
  * allocation hook.  It takes no scratch argument and allocates nothing: its
- * scratch is a fixed 256.5 KiB array in the library's device memory, held on
- * every GPU that loads the library until the process exits.  Limit: n up to
- * 2^28 rows (larger n returns VELO_EINVAL).  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the array: calls that overlap
+ * scratch is a fixed array of 262,400 B (256 KiB + 256 B) in the library's
+ * device memory, held on every GPU that loads the library until the process
+ * exits.  Limit: n up to 2^28 rows (larger n returns VELO_EINVAL).  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and keeps it; make that first call before any stream capture, and do not
+ * reset the device (cudaDeviceReset) after it.  All calls share the array: calls that overlap
  * on the GPU race and must be serialised by the caller.  Every call rewrites
  * the array before reading it, so results never depend on earlier calls.
  * This entry point has no counterpart in the reference. */

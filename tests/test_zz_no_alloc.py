@@ -21,13 +21,6 @@ from velodb_b200._lib import check
 pytestmark = pytest.mark.gpu
 
 
-def _inputs(n, seed):
-    keys = W.splitmix64(seed, n, 0)
-    pay = np.arange(n, dtype=np.uint32)
-    marks = (W.lemire(W.splitmix64(seed, n, 1), 10) < 3).astype(np.uint8)
-    return keys, pay, marks
-
-
 def _dev(keys, pay, marks):
     cap = capi.next_pow2(len(keys))
     return capi.to_dev_u64(keys, cap), capi.to_dev_u32(pay, cap), capi.to_dev_u8(marks, cap)
@@ -51,11 +44,24 @@ def _with_scratch(keys, pay, marks):
     return k.cpu().numpy(), p.cpu().numpy(), m.cpu().numpy(), int(cnt.item())
 
 
-def test_noalloc_matches_scratch_entry_point_twice(cuda):
-    # two calls in a row; the second has more tiles than the first, so stale
-    # scratch from the first call would show up in the second
-    for n, seed in [(300_001, 11), (2_000_003, 12)]:
-        keys, pay, marks = _inputs(n, seed)
+def _inputs_density(n, seed, tenths):
+    keys = W.splitmix64(seed, n, 0)
+    pay = np.arange(n, dtype=np.uint32)
+    marks = (W.lemire(W.splitmix64(seed, n, 1), 10) < tenths).astype(np.uint8)
+    return keys, pay, marks
+
+
+@pytest.mark.parametrize("calls", [
+    # small then large: the second call has more tiles than the first
+    [(300_001, 11, 3), (2_000_003, 12, 3)],
+    # large then small with another mark density: the per-tile counts and
+    # prefix values of the first call stay in the array past the second
+    # call's tiles, where a scan that read beyond its own tiles would see them
+    [(2_000_003, 13, 7), (300_001, 14, 2)],
+])
+def test_noalloc_matches_scratch_entry_point_twice(cuda, calls):
+    for n, seed, tenths in calls:
+        keys, pay, marks = _inputs_density(n, seed, tenths)
         a = _noalloc(keys, pay, marks)
         b = _with_scratch(keys, pay, marks)
         assert a[3] == b[3] == int(marks.sum())

@@ -34,16 +34,21 @@ constexpr size_t NOALLOC_MAX_TILES = (size_t)1 << (NOALLOC_MAX_LOGN - NOALLOC_LT
 constexpr size_t NOALLOC_PREFIX_OFFSET = (NOALLOC_MAX_TILES * 4 + 255) / 256 * 256;
 constexpr size_t NOALLOC_SCRATCH_BYTES = NOALLOC_PREFIX_OFFSET + ((NOALLOC_MAX_TILES + 1) * 4 + 255) / 256 * 256;
 
-// The scratch of every call (256 KiB + 512 B).  Host code must not pass this
-// name to a kernel: on the host it is only a stand-in for the symbol, so its
-// device address is looked up with cudaGetSymbolAddress.
+// The scratch of every call: 131,072 B of counts + 131,328 B of prefix =
+// 262,400 B (256 KiB + 256 B).  Host code must not pass this name to a
+// kernel: on the host it is only a stand-in for the symbol, so its device
+// address is looked up with cudaGetSymbolAddress.
+static_assert(NOALLOC_SCRATCH_BYTES == 262400, "the documented size of the no-alloc scratch");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
 static std::mutex g_noalloc_mutex;
 static void* g_noalloc_addr[64] = {};
 
 // Device address of the scratch array on the current device, looked up once
-// per device (the first call on a device does this set-up).
+// per device (the first call on a device does this set-up) and kept for the
+// life of the process.  A cudaDeviceReset after that first call is not
+// supported: the reset rebuilds the module, the array may move, and later
+// calls would still use the old address.
 static velo_status noalloc_scratch(void** out)
 {
     int dev = 0;
