@@ -1,25 +1,35 @@
 #!/usr/bin/env python3
 """Benchmark of the oblivious operator hot path on B200.
 
-Default workload: oblivious filter + group-by over the synthetic
-6,001,215-row lineitem-shaped fact table (predicate -> ORCompact -> bitonic
-sort on (flag1, flag2) -> segmented int64 sums, output padded to 8 groups).
-One step = one pass of that pipeline over one batch of input.
+Headline workload (the default): the oblivious PK-FK sort-merge join of a
+1,500,000-row dimension table and a 6,000,000-row fact table, followed by an
+oblivious group-by on the foreign key and the top-10 groups by sum(price)
+(union -> bitonic sort on (key, tag) -> forward fill -> ORCompact -> segmented
+sums -> bitonic top-k).  One step = one pass of that pipeline over the two
+tables.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload groupby|sort|batch|serve|join]
+                    [--workload join|sort|groupby|batch|serve] [--extras all|none]
 
-Workloads: groupby (6,001,215-row filter + group-by, the default), sort
-(plain 2^20-row sort), join (1.5 M x 6 M-row PK-FK join + group-by + top-10), batch (512 uneven sorts/compactions in one persistent
-launch replayed from a CUDA graph, beside 512 plain launch sequences), serve
-(query stream over resident 60 M / 15 M / 150 M-row tables: served vs plain
-one-at-a-time throughput and p50/p99 latency).
+At N = 1 the same run also measures, each in its own key of `extras` and
+each checked against the oracle: the plain sort of 2^20 (u64 key, u32
+payload) rows and of 2^24 rows (inputs far beyond L2: the HBM case), the
+filter + group-by over the 6,001,215-row fact table, the batch of 512 uneven
+sorts and compactions (one persistent launch from a CUDA graph against 512
+plain launch sequences), and the served query stream (p50/p99 latency and
+throughput, served against plain one-at-a-time).
+
+Every network pass is also timed on its own with CUDA events (the library's
+pass timer) and the line reports the achieved HBM bandwidth per pass kind:
+tile sort, in-tile merge, fused global levels, ORCompact tile and global
+passes.
 
 Multi-GPU: one process per GPU (torchrun); the path does not shard, so every
-rank runs an independent replica of the workload ("replicas only") and the
-aggregate throughput is the total rows of all ranks over the slowest rank's
-time.  `--impl reference` times the reference's CPU algorithm (the C oracle
-port in the reference's network order, all host cores) on rank 0.
+rank runs an independent replica of the headline workload ("replicas only")
+and the aggregate throughput is the total rows of all ranks over the slowest
+rank's time.  `--impl reference` times the CPU oblivious path on rank 0: the
+oracle's oblivious pipeline (network sorts over all next_pow2(n) rows in the
+reference's network order, ORCompact, segmented sums) on all host cores.
 """
 from __future__ import annotations
 
@@ -36,12 +46,17 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "obliv sort & join Mrows/s (frac of HBM peak); p50/p99 latency served vs plain"
 
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu
-# capture (the mean over the tile, global and merge passes of one sort), or
-# None when the workload's launch is too large to capture.
-TRAFFIC = {"groupby": 210.1e6, "sort": 12.65e6, "batch": None}
-FALLBACK_HBM_GBS = 6650.0
+# capture of the same pipeline (the mean over its sort passes), or None when
+# no capture of that launch exists.
+TRAFFIC = {"groupby": 210.1e6, "sort": 12.65e6, "join": None, "batch": None}
+
+# warm-up runs at least this long (seconds) so that the clock samples taken
+# from the end of the warm-up through the timed steps show the GPU under load
+SOAK_S = 1.5
 
 
 def hbm_peak():
@@ -53,7 +68,7 @@ def hbm_peak():
 
 
 # --------------------------------------------------------------------------
-# pass-count model (mirrors plan_sort / plan_compact of the library)
+# pass-count models
 # --------------------------------------------------------------------------
 
 # levels fused per global pass: plain (u64, u32) sorts keep 32 contiguous rows
@@ -73,7 +88,7 @@ def compact_passes(logn: int, lt: int, lmax: int) -> int:
 
 
 def rdm_psort(np_rows: int) -> int:
-    """Pass count of the survey's algorithmic-bytes model: T = 2^13, L = 8."""
+    """Pass count of the algorithmic-bytes model: T = 2^13, L = 8."""
     m = max(0, int(np.log2(np_rows)) - 13)
     return 1 + sum(-(-i // 8) + 1 for i in range(1, m + 1))
 
@@ -95,7 +110,7 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join("/tmp", f"velo_clocks_{os.getpid()}.csv")
+        self.path = os.path.join("/tmp", f"velo_clocks_{os.getpid()}_{index}.csv")
 
     def start(self):
         try:
@@ -127,125 +142,21 @@ class ClockSampler:
                     reasons.add(nm)
         os.unlink(self.path)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window": f"the last {SOAK_S} s of the warm-up and the timed steps"}
 
 
 # --------------------------------------------------------------------------
 # workloads (ours)
 # --------------------------------------------------------------------------
 
-class GroupBy:
-    """Config-1 shape: filter + group-by over 6,001,215 rows."""
-    name = "filter_groupby"
-
-    def __init__(self, torch, capi, W, device):
-        self.torch, self.capi = torch, capi
-        self.n = W.LINEITEM_ROWS
-        self.pred = W.LINEITEM_PRED
-        self.G = W.LINEITEM_GROUP_BOUND
-        self.host = W.lineitem(self.n)
-        self.pinned = {k: torch.from_numpy(v).pin_memory() for k, v in self.host.items()}
-        self.dev = {k: torch.empty_like(v, device=device) for k, v in self.pinned.items()}
-        for k in self.dev:
-            self.dev[k].copy_(self.pinned[k])
-        self.scratch = torch.empty(capi.filter_groupby_scratch_bytes(self.n, self.G), dtype=torch.uint8,
-                                   device=device)
-        self.out = torch.empty((self.G, 6), dtype=torch.int64, device=device)
-        self.counts = torch.empty(2, dtype=torch.int64, device=device)
-        self.out_host = torch.empty((self.G, 6), dtype=torch.int64).pin_memory()
-        self.counts_host = torch.empty(2, dtype=torch.int64).pin_memory()
-        self.in_bytes = sum(v.numel() * v.element_size() for v in self.pinned.values())
-        self.np_rows = 1 << int(np.ceil(np.log2(self.n)))
-        self.rec_bytes = 16  # 2-word records (the predicate's bands fit the packed layout)
-        self.flush_l2 = False  # inputs (156 MB) and records (134 MB) exceed the 126 MB L2
-
-    def step(self):
-        self.capi.filter_groupby(self.dev, self.n, self.pred, self.G, scratch=self.scratch, out=self.out,
-                                 counts=self.counts)
-
-    def step_e2e(self):
-        for k in self.dev:
-            self.dev[k].copy_(self.pinned[k], non_blocking=True)
-        self.step()
-        self.out_host.copy_(self.out, non_blocking=True)
-        self.counts_host.copy_(self.counts, non_blocking=True)
-
-    def d2h_bytes(self):
-        return self.out.numel() * 8 + self.counts.numel() * 8
-
-    def launches(self):
-        logn = int(np.log2(self.np_rows))
-        return 2 + compact_passes(logn, 12, PIPE_LMAX) + sort_passes(logn, 12, PIPE_LMAX) + 4
-
-    def rdm_bytes(self):
-        npr = self.np_rows
-        pred = self.n * 9
-        comp = self.n * 5 + 2 * npr * 24 * rdm_pcomp(npr)
-        srt = 2 * npr * 40 * rdm_psort(npr)
-        heads = 2 * npr * 40
-        return pred + comp + srt + heads
-
-    def check(self, orc):
-        g, keys, sums = orc.filter_groupby(self.host, self.pred, self.G)
-        out = self.out.cpu().numpy()
-        cnt = self.counts.cpu().numpy()
-        ok = int(cnt[1]) == g and np.array_equal(out[:g, 0], keys.astype(np.int64)) and np.array_equal(
-            out[:g, 1:], sums)
-        return bool(ok)
-
-    def dominant(self, device):
-        """The dominant kernel is the bitonic pass kernel of the pipeline's
-        sort stage (about 70 % of the step in the ncu launch list).  Its
-        launches are timed inside the pipeline itself: with stage timing on,
-        velo_filter_groupby records CUDA events on its stream around each
-        stage, and the sort stage's time is divided by its launch count.  The
-        records are 2 words (16 B: the predicate's quantity and discount bands
-        fit the packed layout) over next_pow2(6,001,215) = 2^23 rows, and
-        every launch reads and writes every record once: 2 x 2^23 x 16 B."""
-        capi = self.capi
-        logn = int(np.log2(self.np_rows))
-        launches = sort_passes(logn, 12, PIPE_LMAX)
-        capi.set_stage_timing(True)
-        ts = []
-        try:
-            for i in range(6):
-                self.step()
-                st = capi.last_stage_times()
-                if i:
-                    ts.append(st[2])
-        finally:
-            capi.set_stage_timing(False)
-        return {"kernel": "k_sort_pass<RowRec<2,1,false,KEY_HI32>,8,4> (bitonic passes of the sort stage, "
-                          "2^23 x 16 B records)",
-                "launches_per_sort": launches, "avg_launch_us": float(np.mean(ts)) * 1e3 / launches,
-                "bytes_per_launch": int(2 * self.np_rows * 16)}
-
-
-def dominant_timing(torch, run, reset, launches, bytes_per_launch, name, reps=5):
-    """Average launch duration of the dominant kernel from CUDA events around
-    whole sorts (each sort = `launches` launches of the kernel), with the
-    input restored between sorts outside the timed events."""
-    ts = []
-    for i in range(reps + 1):
-        reset()
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        run()
-        e.record()
-        torch.cuda.synchronize()
-        if i:
-            ts.append(s.elapsed_time(e))
-    per_launch_ms = float(np.mean(ts)) / launches
-    return {"kernel": name, "launches_per_sort": launches, "avg_launch_us": per_launch_ms * 1e3,
-            "bytes_per_launch": int(bytes_per_launch)}
-
-
 class JoinTopK:
-    """Config-2 shape: oblivious PK-FK join of a 1,500,000-row dimension
-    table and a 6,000,000-row fact table (~50 % filters on each side),
-    group-by fk over the joined rows, top-10 groups by sum(price).  Throughput
-    counts the 7.5 M input rows."""
+    """Oblivious PK-FK join of a 1,500,000-row dimension table and a
+    6,000,000-row fact table (~50 % filters on each side), group-by fk over
+    the joined rows, top-10 groups by sum(price).  Throughput counts the
+    7.5 M input rows."""
     name = "join_groupby_top10"
+    key = "join"
 
     def __init__(self, torch, capi, W, device):
         self.torch, self.capi = torch, capi
@@ -270,6 +181,8 @@ class JoinTopK:
         self.np_rows = 1 << int(np.ceil(np.log2(self.n)))
         self.rec_bytes = 16
         self.flush_l2 = False  # inputs (60 MB) plus union records (268 MB) exceed the 126 MB L2
+        self.kernel = ("k_sort_pass<RowRec<2,1,false,KEY_FULL>,8,4,PK,2> (union sort: 2^23 two-word records, "
+                       "4096-row tiles, two CTAs per SM)")
 
     def step(self):
         self.capi.join_groupby_topk(self.dev, self.pred, self.k, scratch=self.scratch, out=self.out,
@@ -306,55 +219,174 @@ class JoinTopK:
                 + 2 * u * 24 * rdm_pcomp(u) + 2 * d * 16 * rdm_psort(d) + 2 * 2 * u * 24)
 
     def check(self, orc):
+        """The oracle's pipeline, and an independent numpy join + bincount."""
         dim, fact = self.host
         g, ofk, osum, ocnt = orc.join_groupby_topk(dim, fact, self.pred, self.k)
         out = self.out.cpu().numpy()
         cnt = self.counts.cpu().numpy()
         m = min(g, self.k)
-        return bool(int(cnt[1]) == g and np.array_equal(out[:m, 0], ofk) and np.array_equal(out[:m, 1], osum)
-                    and np.array_equal(out[:m, 2], ocnt))
-
-    def dominant(self, device):
-        """The dominant kernel is the bitonic pass kernel of the union sort
-        (next_pow2(7.5 M) = 2^23 records of 2 words, 4096-row tiles), timed
-        live through the pipeline's stage timer (stage 2 = the union sort)."""
-        capi = self.capi
-        launches = sort_passes(int(np.log2(self.np_rows)), 12, PIPE_LMAX)
-        capi.set_stage_timing(True)
-        ts = []
-        try:
-            for i in range(6):
-                self.step()
-                st = capi.last_stage_times()
-                if i:
-                    ts.append(st[1])
-        finally:
-            capi.set_stage_timing(False)
-        return {"kernel": "k_sort_pass<RowRec<2,1,false,KEY_FULL>,8,4> (union sort, 2^23 x 16 B records)",
-                "launches_per_sort": launches, "avg_launch_us": float(np.mean(ts)) * 1e3 / launches,
-                "bytes_per_launch": int(2 * self.np_rows * 16)}
+        ok = int(cnt[1]) == g and np.array_equal(out[:m, 0], ofk) and np.array_equal(out[:m, 1], osum) \
+            and np.array_equal(out[:m, 2], ocnt)
+        nfk, nsum, ncnt, ng = numpy_join_topk(dim, fact, self.pred, self.k)
+        ok = ok and ng == g and np.array_equal(out[:m, 0], nfk) and np.array_equal(out[:m, 1], nsum) \
+            and np.array_equal(out[:m, 2], ncnt)
+        return bool(ok)
 
 
-def make_workload(name, torch, capi, W, device):
-    if name == "groupby":
-        return GroupBy(torch, capi, W, device)
-    if name == "join":
-        return JoinTopK(torch, capi, W, device)
-    if name == "sort":
-        return SortKP(torch, capi, W, device)
-    if name == "batch":
-        return Batched(torch, capi, W, device)
-    raise SystemExit(f"unknown workload {name}")
+def numpy_join_topk(dim, fact, pred, k):
+    """The join + group-by + top-k computed directly with numpy (no oracle
+    code): dimension rows passing the date filter, fact rows passing the price
+    filter and whose key has a passing dimension row, sums by bincount, the k
+    largest sums with ties to the smaller key."""
+    nd = len(dim["key"])
+    keep_dim = np.zeros(nd + 2, bool)
+    keep_dim[dim["key"][dim["date"] < pred["date_hi"]]] = True
+    fk = fact["fk"].astype(np.int64)
+    joined = (fact["price"] < pred["price_hi"]) & keep_dim[fk]
+    cnts = np.bincount(fk[joined], minlength=nd + 2).astype(np.int64)
+    psum = np.zeros(nd + 2, np.int64)
+    np.add.at(psum, fk[joined], fact["price"][joined])
+    groups = np.nonzero(cnts)[0]
+    order = np.lexsort((groups, -psum[groups]))[:k]
+    top = groups[order]
+    return top.astype(np.int64), psum[top], cnts[top], int(len(groups))
+
+
+class GroupBy:
+    """Filter + group-by over the 6,001,215-row fact table."""
+    name = "filter_groupby"
+    key = "groupby"
+
+    def __init__(self, torch, capi, W, device):
+        self.torch, self.capi = torch, capi
+        self.n = W.LINEITEM_ROWS
+        self.pred = W.LINEITEM_PRED
+        self.G = W.LINEITEM_GROUP_BOUND
+        self.host = W.lineitem(self.n)
+        self.pinned = {k: torch.from_numpy(v).pin_memory() for k, v in self.host.items()}
+        self.dev = {k: torch.empty_like(v, device=device) for k, v in self.pinned.items()}
+        for k in self.dev:
+            self.dev[k].copy_(self.pinned[k])
+        self.scratch = torch.empty(capi.filter_groupby_scratch_bytes(self.n, self.G), dtype=torch.uint8,
+                                   device=device)
+        self.out = torch.empty((self.G, 6), dtype=torch.int64, device=device)
+        self.counts = torch.empty(2, dtype=torch.int64, device=device)
+        self.out_host = torch.empty((self.G, 6), dtype=torch.int64).pin_memory()
+        self.counts_host = torch.empty(2, dtype=torch.int64).pin_memory()
+        self.in_bytes = sum(v.numel() * v.element_size() for v in self.pinned.values())
+        self.np_rows = 1 << int(np.ceil(np.log2(self.n)))
+        self.rec_bytes = 16  # 2-word records (the predicate's bands fit the packed layout)
+        self.flush_l2 = False  # inputs (156 MB) and records (134 MB) exceed the 126 MB L2
+        self.kernel = ("k_sort_pass<RowRec<2,1,false,KEY_HI32>,8,4,PK,3> (sort stage: 2^23 two-word records, "
+                       "4096-row tiles, three CTAs per SM)")
+
+    def step(self):
+        self.capi.filter_groupby(self.dev, self.n, self.pred, self.G, scratch=self.scratch, out=self.out,
+                                 counts=self.counts)
+
+    def step_e2e(self):
+        for k in self.dev:
+            self.dev[k].copy_(self.pinned[k], non_blocking=True)
+        self.step()
+        self.out_host.copy_(self.out, non_blocking=True)
+        self.counts_host.copy_(self.counts, non_blocking=True)
+
+    def d2h_bytes(self):
+        return self.out.numel() * 8 + self.counts.numel() * 8
+
+    def launches(self):
+        logn = int(np.log2(self.np_rows))
+        return 2 + compact_passes(logn, 12, PIPE_LMAX) + sort_passes(logn, 12, PIPE_LMAX) + 4
+
+    def rdm_bytes(self):
+        npr = self.np_rows
+        pred = self.n * 9
+        comp = self.n * 5 + 2 * npr * 24 * rdm_pcomp(npr)
+        srt = 2 * npr * 40 * rdm_psort(npr)
+        heads = 2 * npr * 40
+        return pred + comp + srt + heads
+
+    def check(self, orc):
+        g, keys, sums = orc.filter_groupby(self.host, self.pred, self.G)
+        out = self.out.cpu().numpy()
+        cnt = self.counts.cpu().numpy()
+        ok = int(cnt[1]) == g and np.array_equal(out[:g, 0], keys.astype(np.int64)) and np.array_equal(
+            out[:g, 1:], sums)
+        return bool(ok)
+
+
+class SortKP:
+    """Plain oblivious sort of n (u64 key, u32 payload) rows."""
+    key = "sort"
+
+    def __init__(self, torch, capi, W, device, n=1 << 20):
+        self.torch, self.capi = torch, capi
+        self.n = n
+        self.name = f"plain_sort_2^{int(np.log2(n))}"
+        keys, pay = W.sort_kp(self.n)
+        self.pinned_k = torch.from_numpy(keys.view(np.int64)).pin_memory()
+        self.pinned_p = torch.from_numpy(pay.view(np.int32)).pin_memory()
+        self.k0 = self.pinned_k.to(device)
+        self.p0 = self.pinned_p.to(device)
+        self.k = torch.empty_like(self.k0)
+        self.p = torch.empty_like(self.p0)
+        self.kh = torch.empty_like(self.pinned_k).pin_memory()
+        self.ph = torch.empty_like(self.pinned_p).pin_memory()
+        self.in_bytes = self.n * 12
+        self.np_rows = self.n
+        self.rec_bytes = 12
+        # up to 2^23 rows (100 MB) the rows fit in L2 and it is flushed
+        # between steps; 2^24 rows (201 MB) exceed it
+        self.flush_l2 = self.n * 12 < (126 << 20)
+        self.kernel = (f"k_sort_pass<RowKP,8,4,PK,{3 if n >= (1 << 21) else 2}> (2^{int(np.log2(n))} rows of "
+                       f"12 B, 4096-row tiles)")
+
+    def step(self):
+        # the network sorts in place: restore the unsorted input first (the
+        # restore is a device copy inside the timed step)
+        self.k.copy_(self.k0)
+        self.p.copy_(self.p0)
+        self.capi.osort_kp(self.k, self.p, self.n)
+
+    def step_e2e(self):
+        self.k.copy_(self.pinned_k, non_blocking=True)
+        self.p.copy_(self.pinned_p, non_blocking=True)
+        self.capi.osort_kp(self.k, self.p, self.n)
+        self.kh.copy_(self.k, non_blocking=True)
+        self.ph.copy_(self.p, non_blocking=True)
+
+    def d2h_bytes(self):
+        return self.n * 12
+
+    def launches(self):
+        return sort_passes(int(np.log2(self.n)), 12, 7)
+
+    def rdm_bytes(self):
+        return 2 * self.n * 12 * rdm_psort(self.n)
+
+    def check(self, orc):
+        k = self.k.cpu().numpy().view(np.uint64)
+        p = self.p.cpu().numpy().view(np.uint32)
+        if self.n <= (1 << 20):
+            ok_, op_ = orc.bitonic_kp(self.k0.cpu().numpy().view(np.uint64), self.p0.cpu().numpy().view(np.uint32))
+            return bool(np.array_equal(k, ok_) and np.array_equal(p, op_))
+        # every (key, payload) row is unique, so the sorted output is the
+        # lexicographic sort of the input
+        k0 = self.k0.cpu().numpy().view(np.uint64)
+        p0 = self.p0.cpu().numpy().view(np.uint32)
+        o = np.lexsort((p0, k0))
+        return bool(np.array_equal(k, k0[o]) and np.array_equal(p, p0[o]))
 
 
 class Batched:
-    """Config-3 shape: 512 independent instances (log-uniform 2^10..2^22
-    rows; even = sort of (u64 key, u32 payload), odd = compaction with
-    Bernoulli(0.3) keep flags), each padded to its own power of two, run by
-    ONE persistent launch captured in a CUDA graph, tile configuration picked
-    by the autotuner.  The plain path (one launch sequence per instance,
-    back to back) is timed beside it."""
+    """512 independent instances (log-uniform 2^10..2^22 rows; even = sort of
+    (u64 key, u32 payload), odd = compaction with Bernoulli(0.3) keep flags),
+    each padded to its own power of two, run by ONE persistent launch captured
+    in a CUDA graph, tile configuration picked by the autotuner.  The plain
+    path (one launch sequence per instance, back to back) is timed beside
+    it."""
     name = "batched_512"
+    key = "batch"
 
     def __init__(self, torch, capi, W, device):
         self.torch, self.capi = torch, capi
@@ -390,6 +422,7 @@ class Batched:
                         torch.from_numpy(h["marks"]).pin_memory() if h["kind"] == "compact" else None)
                        for h in insts]
         self.count_host = torch.zeros(len(self.items), dtype=torch.int64).pin_memory()
+        self.kernel = "k_sched (persistent)"
 
     def step(self):
         self.graph.replay()
@@ -428,115 +461,46 @@ class Batched:
                 tot += it["n"] * 5 + 2 * npr * 13 * rdm_pcomp(npr)
         return tot
 
-    def check(self, orc):
-        self.batch.status(stream=self.stream)
-        ok = True
-        for it, h in list(zip(self.items, self.host))[:24]:
-            if it["kind"] == "sort":
-                k = it["keys"].cpu().numpy().view(np.uint64)[: it["n"]]
-                o = np.sort(h["keys"])
-                ok &= bool(np.array_equal(k, o))
-            else:
-                c = int(it["count"].item())
-                ok &= c == int(h["marks"].sum())
-                k = it["keys"].cpu().numpy().view(np.uint64)[:c]
-                ok &= bool(np.array_equal(k, h["keys"][h["marks"].astype(bool)]))
-        return ok
-
-    def dominant(self, device):
-        """The persistent scheduler kernel is the only kernel of the step;
-        its algorithmic bytes per launch are the batch's network bytes."""
-        torch = self.torch
-        ts = []
-        for i in range(4):
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            self.graph.replay()
-            e.record()
-            torch.cuda.synchronize()
-            if i:
-                ts.append(s.elapsed_time(e))
-        bytes_ = 0
+    def network_bytes(self):
+        """Bytes the batch's passes read and write, by the library's own pass
+        plan for the chosen tile."""
+        tot = 0
         for it in self.items:
             npr = self.capi.next_pow2(it["n"])
             lt = self.tune[0]
             lmax = min(8, lt - 5)
             if it["kind"] == "sort":
-                bytes_ += 2 * npr * 12 * sort_passes(int(np.log2(npr)), lt, lmax)
+                tot += 2 * npr * 12 * sort_passes(int(np.log2(npr)), lt, lmax)
             else:
-                bytes_ += 2 * npr * 13 * compact_passes(int(np.log2(npr)), lt, lmax) + npr * 5
-        return {"kernel": f"k_sched (persistent, tile 2^{self.tune[0]} x {self.tune[1]} threads)",
-                "launches_per_sort": 1, "avg_launch_us": float(np.mean(ts)) * 1e3, "bytes_per_launch": int(bytes_)}
-
-
-class SortKP:
-    """Config-0 shape: plain oblivious sort of 2^20 (u64 key, u32 payload) rows."""
-    name = "plain_sort_2^20"
-
-    def __init__(self, torch, capi, W, device):
-        self.torch, self.capi = torch, capi
-        self.n = 1 << 20
-        keys, pay = W.sort_kp(self.n)
-        self.pinned_k = torch.from_numpy(keys.view(np.int64)).pin_memory()
-        self.pinned_p = torch.from_numpy(pay.view(np.int32)).pin_memory()
-        self.k0 = self.pinned_k.to(device)
-        self.p0 = self.pinned_p.to(device)
-        self.k = torch.empty_like(self.k0)
-        self.p = torch.empty_like(self.p0)
-        self.kh = torch.empty_like(self.pinned_k).pin_memory()
-        self.ph = torch.empty_like(self.pinned_p).pin_memory()
-        self.in_bytes = self.n * 12
-        self.np_rows = self.n
-        self.rec_bytes = 12
-        self.flush_l2 = True  # 12.6 MB fits in L2: flushed between steps
-
-    def step(self):
-        # the network sorts in place: restore the unsorted input first (the
-        # restore is a device copy inside the timed step)
-        self.k.copy_(self.k0)
-        self.p.copy_(self.p0)
-        self.capi.osort_kp(self.k, self.p, self.n)
-
-    def step_e2e(self):
-        self.k.copy_(self.pinned_k, non_blocking=True)
-        self.p.copy_(self.pinned_p, non_blocking=True)
-        self.capi.osort_kp(self.k, self.p, self.n)
-        self.kh.copy_(self.k, non_blocking=True)
-        self.ph.copy_(self.p, non_blocking=True)
-
-    def d2h_bytes(self):
-        return self.n * 12
-
-    def launches(self):
-        return sort_passes(20, 12, 7)
-
-    def rdm_bytes(self):
-        return 2 * self.n * 12 * rdm_psort(self.n)
+                tot += 2 * npr * 13 * compact_passes(int(np.log2(npr)), lt, lmax) + npr * 5
+        return tot
 
     def check(self, orc):
-        k = self.k.cpu().numpy().view(np.uint64)
-        p = self.p.cpu().numpy().view(np.uint32)
-        ok_, op_ = orc.bitonic_kp(self.k0.cpu().numpy().view(np.uint64), self.p0.cpu().numpy().view(np.uint32))
-        return bool(np.array_equal(k, ok_) and np.array_equal(p, op_))
-
-    def dominant(self, device):
-        """The bitonic pass kernel is the only kernel of the step; every
-        launch reads and writes every (8 B key + 4 B payload) row once."""
-        run = lambda: self.capi.osort_kp(self.k, self.p, self.n)  # noqa: E731
-
-        def reset():
-            self.k.copy_(self.k0)
-            self.p.copy_(self.p0)
-
-        return dominant_timing(self.torch, run, reset, self.launches(), 2 * self.n * 12,
-                               "k_sort_pass<RowKP> (bitonic passes, 2^20 x 12 B rows)")
+        """Every instance against numpy; a stride sample against the oracle."""
+        self.batch.status(stream=self.stream)
+        ok = True
+        for i, (it, h) in enumerate(zip(self.items, self.host)):
+            if it["kind"] == "sort":
+                k = it["keys"].cpu().numpy().view(np.uint64)[: it["n"]]
+                ok &= bool(np.array_equal(k, np.sort(h["keys"])))
+                if i % 61 == 0 and it["n"] <= (1 << 20):
+                    ok_, _ = orc.bitonic_kp(h["keys"], h["pay"])
+                    ok &= bool(np.array_equal(k, ok_[: it["n"]]))
+            else:
+                c = int(it["count"].item())
+                ok &= c == int(h["marks"].sum())
+                k = it["keys"].cpu().numpy().view(np.uint64)[:c]
+                ok &= bool(np.array_equal(k, h["keys"][h["marks"].astype(bool)]))
+        return bool(ok)
 
 
 # --------------------------------------------------------------------------
+# timing
+# --------------------------------------------------------------------------
 
-def time_steps(torch, fn, steps, flush=None, stream=None):
-    """Per-step CUDA-event durations (ms) of `fn`, flushing L2 between steps
-    outside the timed events when asked."""
+def time_steps(torch, fn, steps, flush=None):
+    """Per-step CUDA-event durations (ms) of `fn` on the current stream,
+    flushing L2 between steps outside the timed events when asked."""
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     for s, e in evs:
         if flush is not None:
@@ -548,283 +512,60 @@ def time_steps(torch, fn, steps, flush=None, stream=None):
     return [s.elapsed_time(e) for s, e in evs]
 
 
-def cpu_baseline_groupby(W, orc):
-    import multiprocessing as mp
-
-    cores = os.cpu_count() or 1
-    n = 1 << 21
-    cols = W.lineitem(n)
+def warm(torch, fn, warmup, min_s=SOAK_S):
+    """At least `warmup` untimed steps, continuing until `min_s` seconds of
+    work have run, so the clock samples see the GPU under steady load."""
     t0 = time.perf_counter()
-    reps = 0
-    while True:
-        orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores)
-        reps += 1
-        if time.perf_counter() - t0 > 10.0 or reps >= 50:
-            break
-    dt = (time.perf_counter() - t0) / reps
-    del mp
-    return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
-            "sample": f"first {n} rows of the 6,001,215-row table, {reps} runs, OpenMP over all cores"}
-
-
-def cpu_baseline_sort(W, orc):
-    cores = os.cpu_count() or 1
-    n = 1 << 20
-    keys, pay = W.sort_kp(n)
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        orc.bitonic_kp(keys, pay, n_threads=cores)
-        reps += 1
-        if time.perf_counter() - t0 > 10.0 or reps >= 200:
-            break
-    dt = (time.perf_counter() - t0) / reps
-    return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
-            "sample": f"full 2^20-row sort, {reps} runs, OpenMP over all cores"}
-
-
-def cpu_baseline_join(W, orc):
-    cores = os.cpu_count() or 1
-    dim, fact = W.join_tables()
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        orc.join_groupby_topk(dim, fact, W.JOIN_PRED, W.JOIN_TOPK, n_threads=cores)
-        reps += 1
-        if time.perf_counter() - t0 > 10.0 or reps >= 20:
-            break
-    dt = (time.perf_counter() - t0) / reps
-    n = len(dim["key"]) + len(fact["fk"])
-    return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
-            "sample": f"full 1.5 M + 6 M-row join, {reps} runs, OpenMP over all cores"}
-
-
-def cpu_baseline_batch(W, orc):
-    """The oracle on instances of the 512 in a fixed stride order until about
-    10 s of CPU work: sorts on all cores, compactions single-threaded."""
-    cores = os.cpu_count() or 1
-    insts = W.batch_instances()
-    rows, t_tot, used = 0, 0.0, 0
-    for i in range(len(insts)):
-        it = insts[(i * 97) % len(insts)]
-        if it["kind"] == "sort":
-            t0 = time.perf_counter()
-            orc.bitonic_kp(it["keys"], it["pay"], n_threads=cores)
-        else:
-            r = np.zeros((it["n"], 16), np.uint8)
-            r[:, :8] = it["keys"].view(np.uint8).reshape(-1, 8)
-            r[:, 8:12] = it["pay"].view(np.uint8).reshape(-1, 4)
-            t0 = time.perf_counter()
-            orc.ocompact(r, it["marks"])
-        t_tot += time.perf_counter() - t0
-        rows += it["n"]
-        used += 1
-        if t_tot > 10.0:
-            break
-    return {"value": rows / t_tot / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
-            "sample": f"{used} of the 512 instances (stride 97 through the list, {rows} rows); sorts on all "
-                      f"cores, compactions single-threaded"}
-
-
-def run_reference(args, rank):
-    """CPU reference arm: the reference's algorithm for the path (the oracle
-    port in the reference's network order) on all host cores, rank 0 only.
-    Each step is a bounded sample of the workload: the whole table for
-    groupby and sort, one instance of the 512 for batch, one query of the
-    stream for serve."""
-    if rank != 0:
-        return
-    import oracle as orc
-    from velodb_b200 import workloads as W
-
-    orc.lib()
-    cores = os.cpu_count() or 1
-    unit = "Mrows/s"
-    if args.workload == "sort":
-        n = 1 << 20
-        keys, pay = W.sort_kp(n)
-        steps = [(lambda: orc.bitonic_kp(keys, pay, n_threads=cores), n)]
-        sample, wl = "full 2^20-row sort per step", "plain_sort_2^20"
-    elif args.workload == "batch":
-        insts = W.batch_instances()
-        order = [(i * 97) % len(insts) for i in range(len(insts))]
-
-        def inst_fn(it):
-            if it["kind"] == "sort":
-                return lambda: orc.bitonic_kp(it["keys"], it["pay"], n_threads=cores)
-            rows = np.zeros((it["n"], 16), np.uint8)
-            rows[:, :8] = it["keys"].view(np.uint8).reshape(-1, 8)
-            rows[:, 8:12] = it["pay"].view(np.uint8).reshape(-1, 4)
-            return lambda: orc.ocompact(rows, it["marks"])
-
-        steps = [(inst_fn(insts[i]), insts[i]["n"]) for i in order]
-        sample = "one of the 512 instances per step (stride 97 through the list); sorts on all cores, " \
-                 "compactions single-threaded"
-        wl = "batched_512"
-    elif args.workload == "join":
-        dim, fact = W.join_tables()
-        steps = [(lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, W.JOIN_TOPK, n_threads=cores),
-                  len(dim["key"]) + len(fact["fk"]))]
-        sample, wl = "full 1.5 M + 6 M-row join per step", "join_groupby_top10"
-    elif args.workload == "serve":
-        from velodb_b200 import serving as S
-
-        hs = S.HostSlices(**S.FULL_SCALE)
-        lo, hi = SERVE_DISTS["short"]
-        qs = [q for q in S.query_stream(hs, 4 * (args.steps + args.warmup) + 8, seed=0xB200000000000004,
-                                        lo_log2=lo, hi_log2=hi) if q.shape != S.Q_JOIN3]
-
-        def q_fn(q):
-            if q.shape == S.Q_FILTER_GROUPBY:
-                cols = hs.lineitem(q.offset, q.n)
-                return lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores)
-            dim, fact = hs.join_inputs(q)
-            return lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, 10, n_threads=cores)
-
-        steps = [(q_fn(q), 1) for q in qs]
-        unit = "queries/s"
-        sample = "one query per step from the served stream (sizes 2^10..2^18), filter+group-by and " \
-                 "two-way join shapes (the three-way chain has no oracle pipeline)"
-        wl = "served_stream"
-    else:
-        # the reference reveals the filtered count and sorts next_pow2(count)
-        # rows (src/operator/filter_compaction_operator.cpp:171-178)
-        n = W.LINEITEM_ROWS
-        cols = W.lineitem(n)
-        steps = [(lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores), n)]
-        sample, wl = "full 6,001,215-row table per step (filtered count revealed)", "filter_groupby"
-    for i in range(args.warmup):
-        steps[i % len(steps)][0]()
-    ts, units = [], 0
-    for i in range(args.steps):
-        fn, u = steps[(args.warmup + i) % len(steps)]
-        t0 = time.perf_counter()
+    i = 0
+    while i < warmup or time.perf_counter() - t0 < min_s:
         fn()
-        ts.append(time.perf_counter() - t0)
-        units += u
-    total = float(np.sum(ts))
-    ms = 1e3 * total / args.steps
-    value = units / total / (1e6 if unit == "Mrows/s" else 1.0)
-    line = {
-        "impl": "reference", "metric": metric_name(args.workload), "value": value, "unit": unit,
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": wl},
-        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
-        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-
-
-# --------------------------------------------------------------------------
-# served query stream (resident tables, continuous admission)
-# --------------------------------------------------------------------------
-
-SERVE_DISTS = {"short": (10.0, 18.0), "analytic": (14.0, 22.0)}
-SERVE_LOADS = (0.5, 0.9, 1.5, 3.0, 6.0)
-
-
-def _lat(results, t_key="submit_ms"):
-    lat = np.asarray([r.end_ms - getattr(r, t_key) for r in results])
-    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
-
-
-def run_serve(args, world, rank, local):
-    """Config-4 shape: a seeded query stream (50 % filter + group-by, 35 %
-    two-way join + top-10, 15 % three-way chain) over resident tables of
-    60 M / 15 M / 150 M rows, admitted by a 120 GB HBM budget.  The plain
-    path is the same request loop with one slot, each query submitted after
-    the previous one returned; the served path admits up to 16 queries at a
-    time on their own streams.  Latency is submit -> result in host memory on
-    the host clock (the request loop spans many streams, so no single device
-    event brackets it); `value` is the served throughput at saturation."""
-    import torch
-    import torch.distributed as dist
-
-    from velodb_b200 import serving as S
-
-    device = torch.device("cuda", local)
-    torch.cuda.set_device(device)
-    if world > 1:
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
-    t0 = time.perf_counter()
-    tab = S.ServedTables(**S.FULL_SCALE)
+        i += 1
+        if i % 8 == 0:
+            torch.cuda.synchronize()
     torch.cuda.synchronize()
-    build_s = time.perf_counter() - t0
-    free, _ = torch.cuda.mem_get_info()
-    budget = int(min(120 << 30, free - (4 << 30)))
-    nq = max(128, 32 * args.steps)
-    slots = 16
+    return i
+
+
+PASS_KINDS = ("tile_sort", "merge", "global", "compact_tile", "compact_global")
+
+
+def pass_roofline(torch, capi, run, peak, reps=3, reset=None):
+    """Every network pass of `run` timed on its own (the library's pass timer:
+    CUDA events around each pass, on the pass's stream) and grouped by pass
+    kind.  Algorithmic bytes of a pass: every row read and written once,
+    2 x rows x row bytes."""
+    rows = []
+    for _ in range(reps):
+        if reset is not None:
+            reset()
+        torch.cuda.synchronize()
+        capi.set_pass_timing(True)
+        try:
+            run()
+            torch.cuda.synchronize()
+            rows.extend(capi.last_pass_times())
+        finally:
+            capi.set_pass_timing(False)
     out = {}
-    clocks = ClockSampler(torch.cuda.current_device())
-    clocks.start()
-    for dname, (lo, hi) in SERVE_DISTS.items():
-        qs = S.query_stream(tab, nq, seed=0xB200000000000004, lo_log2=lo, hi_log2=hi)
-        srv = S.Server(tab, slots=1, budget_bytes=budget)
-        S.run_closed_one_at_a_time(srv, qs[: max(8, args.warmup)])
-        plain_res, plain_s = S.run_closed_one_at_a_time(srv, qs)
-        plain_qps = nq / plain_s
-        plain_loads = {}
-        for f in (0.5, 0.9):
-            r, _ = S.run_open_loop(srv, qs, S.arrivals(nq, f * plain_qps, seed=int(f * 1000)))
-            plain_loads[f"{f}x"] = {"offered_qps": f * plain_qps, **_lat(r)}
-        srv.close()
-        srv = S.Server(tab, slots=slots, budget_bytes=budget)
-        S.run_open_loop(srv, qs[: max(16, args.warmup)], np.zeros(max(16, args.warmup)))
-        sat_res, sat_s = S.run_open_loop(srv, qs, np.zeros(nq))
-        served_qps = nq / sat_s
-        loads = {}
-        for f in SERVE_LOADS:
-            r, s = S.run_open_loop(srv, qs, S.arrivals(nq, f * plain_qps, seed=int(f * 1000)))
-            loads[f"{f}x"] = {"offered_qps": f * plain_qps, "achieved_qps": nq / s, **_lat(r)}
-        st = srv.stats()
-        srv.close()
-        same = all(S.result_key(a) == S.result_key(b) and a.status == 0 and b.status == 0
-                   for a, b in zip(plain_res, sat_res))
-        shapes = {S.SHAPE_NAMES[k]: int(sum(1 for q in qs if q.shape == k)) for k in S.SHAPE_NAMES}
-        out[dname] = {
-            "sizes_log2": [lo, hi], "queries": nq, "mix": shapes,
-            "plain": {"qps": plain_qps, **_lat(plain_res), "under_poisson": plain_loads},
-            "served": {"qps_saturation": served_qps, **_lat(sat_res), "slots": slots,
-                       "peak_inflight": st["peak_inflight"], "peak_arena_bytes": st["peak_arena_bytes"],
-                       "poisson": loads},
-            "speedup_served_vs_plain": served_qps / plain_qps,
-            "results_identical_alone_and_in_mix": bool(same),
-        }
-    clk = clocks.stop()
-    head = out["short"]
-    value = head["served"]["qps_saturation"]
-    value, _ = aggregate_throughput(1.0, 1e3 / value, world, device, scale=1.0)
-    from velodb_b200._lib import VeloQuery, VeloQueryResult
-
-    line = {
-        "metric": metric_name("serve"), "value": value, "unit": "queries/s", "n_gpus": world,
-        "steps": nq, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": "served_stream", "tables_rows": dict(S.FULL_SCALE),
-                   "resident_bytes": int(tab.bytes), "table_build_s": build_s, "hbm_budget_bytes": budget,
-                   "headline_sizes_log2": list(SERVE_DISTS["short"]), "parallelism": f"replicas{world}",
-                   "timing": "host clock, submit -> result in host memory",
-                   "l2": "inputs larger than L2 (resident tables 4.9 GB)"},
-        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": C_sizeof(VeloQuery),
-                "d2h_bytes_per_step": C_sizeof(VeloQueryResult),
-                "note": "the served numbers are end to end: a query descriptor in, a result struct out"},
-        "serve": out, "clocks": clk,
-        "gpu_launches": None,
-    }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-
-
-def C_sizeof(t):
-    import ctypes
-
-    return ctypes.sizeof(t)
+    for kind in PASS_KINDS:
+        xs = [(2 * (1 << lg) * rb, ms) for (k, lg, rb, ms) in rows if k == kind and ms > 0]
+        if not xs:
+            continue
+        byt = sum(b for b, _ in xs)
+        t = sum(m for _, m in xs)
+        fr = [b / (m / 1e3) / 1e9 / peak for b, m in xs]
+        out[kind] = {"launches_per_step": len(xs) // reps, "avg_launch_us": t / len(xs) * 1e3,
+                     "achieved_gbs": byt / (t / 1e3) / 1e9, "frac": byt / (t / 1e3) / 1e9 / peak,
+                     "min_frac": min(fr), "max_frac": max(fr)}
+    # the dominant sort: the sort passes of the largest padded size
+    sorts = [(lg, rb, ms) for (k, lg, rb, ms) in rows if k in ("tile_sort", "merge", "global") and ms > 0]
+    dom = None
+    if sorts:
+        lg_max = max(lg for lg, _, _ in sorts)
+        xs = [(2 * (1 << lg) * rb, ms) for lg, rb, ms in sorts if lg == lg_max]
+        dom = {"launches_per_step": len(xs) // reps, "avg_launch_us": sum(m for _, m in xs) / len(xs) * 1e3,
+               "algorithmic_bytes_per_launch": xs[0][0], "log2_rows": lg_max}
+    return out, dom
 
 
 def max_over_ranks(x: float, world: int, device=None) -> float:
@@ -845,16 +586,404 @@ def aggregate_throughput(units_per_rank: float, ms: float, world: int, device=No
     return world * units_per_rank / (ms_max / 1e3) / scale, ms_max
 
 
-def metric_name(workload):
-    if workload == "join":
-        return "oblivious PK-FK join + group-by + top-10 input throughput (1.5 M dim + 6 M fact rows)"
-    if workload == "serve":
-        return "served query throughput at saturation (queries/s; p50/p99 vs plain one-at-a-time)"
-    if workload == "batch":
-        return "batched oblivious sorts+compactions throughput (512 instances, 2^10..2^22 rows)"
-    if workload == "sort":
-        return "oblivious bitonic sort throughput (2^20 rows, u64 key + u32 payload)"
-    return "oblivious filter+group-by input throughput (6,001,215-row fact table)"
+def measure(torch, capi, wl, args, world, device, peak, peak_kind, with_e2e=True):
+    """Warm-up, K timed steps (max over ranks), the end-to-end form through
+    the public API with host buffers, and the algorithmic-bytes model."""
+    import torch.distributed as dist
+
+    l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=device) if wl.flush_l2 else None
+    flush = (lambda: l2_flush.fill_(1)) if l2_flush is not None else None
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    warm(torch, wl.step, args.warmup)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ts = time_steps(torch, wl.step, args.steps, flush)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+    value, ms = aggregate_throughput(wl.n, float(np.mean(ts)), world, device)
+    res = {"value": value, "unit": "Mrows/s", "ms_per_step": ms, "clocks": clk,
+           "l2": "flushed between steps" if wl.flush_l2 else "inputs larger than L2",
+           "config": {"workload": wl.name, "rows": int(wl.n), "padded_rows": int(wl.np_rows),
+                      "record_bytes": wl.rec_bytes}}
+    if with_e2e:
+        for _ in range(2):
+            wl.step_e2e()
+        torch.cuda.synchronize()
+        te = time_steps(torch, wl.step_e2e, max(3, args.steps // 2))
+        e2e_value, ems = aggregate_throughput(wl.n, float(np.mean(te)), world, device)
+        res["e2e"] = {"value": e2e_value, "unit": "Mrows/s", "h2d_bytes_per_step": int(wl.in_bytes),
+                      "d2h_bytes_per_step": int(wl.d2h_bytes()), "ms_per_step": ems}
+    rdm = wl.rdm_bytes()
+    res["rdm"] = {"bytes_per_step": int(rdm), "achieved_gbs": rdm / (ms / 1e3) / 1e9,
+                  "frac_of_hbm": rdm / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind}
+    res["gpu_launches"] = int(wl.launches() * args.steps)
+    return res
+
+
+def roofline_of(torch, capi, wl, peak, peak_kind):
+    """The `roofline` object: the dominant kernel (the bitonic pass kernel of
+    the workload's largest sort) and every pass kind."""
+    reset = None
+    run = wl.step
+    if isinstance(wl, SortKP):
+        def reset():
+            wl.k.copy_(wl.k0)
+            wl.p.copy_(wl.p0)
+
+        def run():
+            wl.capi.osort_kp(wl.k, wl.p, wl.n)
+    kinds, dom = pass_roofline(torch, capi, run, peak, reset=reset)
+    if dom is None:
+        return None
+    achieved = dom["algorithmic_bytes_per_launch"] / (dom["avg_launch_us"] / 1e6) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+            "traffic": TRAFFIC.get(wl.key), "kernel": wl.kernel, "avg_launch_us": dom["avg_launch_us"],
+            "launches_per_step": dom["launches_per_step"],
+            "algorithmic_bytes_per_launch": dom["algorithmic_bytes_per_launch"],
+            "timing": "each pass bracketed by CUDA events on its stream (library pass timer), mean of 3 runs",
+            "by_pass_kind": kinds}
+
+
+# --------------------------------------------------------------------------
+# CPU baselines (the oracle's oblivious pipelines, all host cores)
+# --------------------------------------------------------------------------
+
+def _timed_reps(fn, min_s, max_reps):
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        fn()
+        reps += 1
+        if time.perf_counter() - t0 > min_s or reps >= max_reps:
+            break
+    return (time.perf_counter() - t0) / reps, reps
+
+
+def _batch_compact_rows(orc, it):
+    """An instance's (key, payload | mark << 32) records over next_pow2(n)
+    rows for the CPU ORCompact (pads unmarked)."""
+    npr = int(orc.next_pow2(it["n"]))
+    r = np.full((npr, 2), np.uint64(2**64 - 1), np.uint64)
+    r[: it["n"], 0] = it["keys"]
+    r[: it["n"], 1] = it["pay"].astype(np.uint64) | (it["marks"].astype(np.uint64) << np.uint64(32))
+    r[it["n"]:, 1] = np.uint64(0)
+    return r
+
+
+def cpu_baseline(wl_key, W, orc, budget_s=10.0):
+    cores = os.cpu_count() or 1
+    if wl_key == "join":
+        dim, fact = W.join_tables()
+        n = len(dim["key"]) + len(fact["fk"])
+        dt, reps = _timed_reps(lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, W.JOIN_TOPK,
+                                                             n_threads=cores, oblivious=True), budget_s, 20)
+        rdt, rreps = _timed_reps(lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, W.JOIN_TOPK,
+                                                               n_threads=cores), budget_s / 4, 5)
+        return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port", "same_config": True,
+                "sample": f"the full 1.5 M + 6 M-row join per run, {reps} runs, oblivious: network sort of all "
+                          f"2^23 union rows in the reference's network order (OpenMP, cache-blocked levels), "
+                          f"chunked forward fill, ORCompact (parallel halves), chunked segmented sums, ORCompact "
+                          f"of the groups, network sort of 2^21 group records; the chunk-carry steps are serial",
+                "revealing_reference_semantics": {
+                    "value": n / rdt / 1e6, "unit": "Mrows/s", "runs": rreps,
+                    "what": "the same join with the joined rows found by a serial branching scan (the count "
+                            "is revealed and only the joined groups are sorted)"}}
+    if wl_key == "groupby":
+        n = W.LINEITEM_ROWS
+        cols = W.lineitem(n)
+        dt, reps = _timed_reps(lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores,
+                                                          oblivious=True), budget_s, 20)
+        rdt, rreps = _timed_reps(lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores),
+                                 budget_s / 4, 20)
+        return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port", "same_config": True,
+                "sample": f"the full 6,001,215-row table per run, {reps} runs, oblivious: predicate, ORCompact "
+                          f"of all 2^23 rows (parallel halves), network sort of all 2^23 rows (OpenMP, "
+                          f"cache-blocked levels), chunked segmented sums into 8 ranked slots",
+                "revealing_reference_semantics": {
+                    "value": n / rdt / 1e6, "unit": "Mrows/s", "runs": rreps,
+                    "what": "filter by a serial stable scatter, then a network sort of only the rows that "
+                            "pass (the count is revealed, as src/operator/filter_compaction_operator.cpp:"
+                            "171-178 does)"}}
+    if wl_key == "sort":
+        n = 1 << 20
+        keys, pay = W.sort_kp(n)
+        dt, reps = _timed_reps(lambda: orc.bitonic_kp(keys, pay, n_threads=cores), budget_s, 200)
+        return {"value": n / dt / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port", "same_config": True,
+                "sample": f"full 2^20-row network sort in the reference's network order, {reps} runs, OpenMP "
+                          f"over all cores"}
+    if wl_key == "batch":
+        insts = W.batch_instances()
+        rows, t_tot, used = 0, 0.0, 0
+        for i in range(len(insts)):
+            it = insts[(i * 97) % len(insts)]
+            if it["kind"] == "sort":
+                t0 = time.perf_counter()
+                orc.bitonic_kp(it["keys"], it["pay"], n_threads=cores)
+            else:
+                r = _batch_compact_rows(orc, it)
+                t0 = time.perf_counter()
+                orc.obl_compact_rec2(r, 1, 32, 0, n_threads=cores)
+            t_tot += time.perf_counter() - t0
+            rows += it["n"]
+            used += 1
+            if t_tot > budget_s:
+                break
+        return {"value": rows / t_tot / 1e6, "unit": "Mrows/s", "cores": cores, "kind": "port",
+                "same_config": False,
+                "sample": f"{used} of the 512 instances (stride 97 through the list, {rows} rows): network sorts "
+                          f"and ORCompact over each instance's next_pow2(n) rows, OpenMP over all cores"}
+    return None
+
+
+# --------------------------------------------------------------------------
+# served query stream (resident tables, continuous admission)
+# --------------------------------------------------------------------------
+
+SERVE_SIZES_LOG2 = (10.0, 18.0)
+
+
+def _lat(results, t_key="submit_ms"):
+    lat = np.asarray([r.end_ms - getattr(r, t_key) for r in results])
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
+
+
+def measure_serve(torch, nq=256, slots=16):
+    """A seeded query stream (50 % filter + group-by, 35 % two-way join +
+    top-10, 15 % three-way chain; slice sizes 2^10..2^18) over resident tables
+    of 60 M / 15 M / 150 M rows, admitted by a 120 GB HBM budget.  Plain = the
+    same request loop with one slot, each query submitted after the previous
+    one returned.  Served = up to 16 queries in flight on their own streams,
+    at saturation (every query offered at once) and under Poisson arrivals at
+    0.9x and 3x the plain capacity.  Latency is submit -> result in host
+    memory, on the host clock."""
+    from velodb_b200 import serving as S
+
+    t0 = time.perf_counter()
+    tab = S.ServedTables(**S.FULL_SCALE)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(120 << 30, free - (4 << 30)))
+    lo, hi = SERVE_SIZES_LOG2
+    qs = S.query_stream(tab, nq, seed=0xB200000000000004, lo_log2=lo, hi_log2=hi)
+    srv = S.Server(tab, slots=1, budget_bytes=budget)
+    S.run_closed_one_at_a_time(srv, qs[:16])
+    plain_res, plain_s = S.run_closed_one_at_a_time(srv, qs)
+    plain_qps = nq / plain_s
+    r09, _ = S.run_open_loop(srv, qs, S.arrivals(nq, 0.9 * plain_qps, seed=900))
+    srv.close()
+    srv = S.Server(tab, slots=slots, budget_bytes=budget)
+    S.run_open_loop(srv, qs[:32], np.zeros(32))
+    sat_res, sat_s = S.run_open_loop(srv, qs, np.zeros(nq))
+    loads = {}
+    for f in (0.9, 3.0):
+        r, s = S.run_open_loop(srv, qs, S.arrivals(nq, f * plain_qps, seed=int(f * 1000)))
+        loads[f"{f}x_plain_capacity"] = {"offered_qps": f * plain_qps, "achieved_qps": nq / s, **_lat(r)}
+    st = srv.stats()
+    srv.close()
+    same = all(S.result_key(a) == S.result_key(b) and a.status == 0 and b.status == 0
+               for a, b in zip(plain_res, sat_res))
+    shapes = {S.SHAPE_NAMES[k]: int(sum(1 for q in qs if q.shape == k)) for k in S.SHAPE_NAMES}
+    out = {
+        "tables_rows": dict(S.FULL_SCALE), "resident_bytes": int(tab.bytes), "table_build_s": build_s,
+        "hbm_budget_bytes": budget, "sizes_log2": [lo, hi], "queries": nq, "mix": shapes,
+        "plain": {"qps": plain_qps, **_lat(plain_res),
+                  "poisson_0.9x": {"offered_qps": 0.9 * plain_qps, **_lat(r09)}},
+        "served": {"qps_saturation": nq / sat_s, **_lat(sat_res), "slots": slots,
+                   "peak_inflight": st["peak_inflight"], "peak_arena_bytes": st["peak_arena_bytes"],
+                   "poisson": loads},
+        "speedup_served_vs_plain": (nq / sat_s) / plain_qps,
+        "results_identical_alone_and_in_mix": bool(same),
+        "timing": "host clock, submit -> result in host memory",
+    }
+    del tab
+    torch.cuda.empty_cache()
+    return out
+
+
+# --------------------------------------------------------------------------
+# reference arm
+# --------------------------------------------------------------------------
+
+def run_reference(args, rank):
+    """CPU reference arm: the reference's algorithm for the path as the
+    oracle's oblivious pipeline (network sorts in the reference's network
+    order over all next_pow2(n) rows, ORCompact, segmented sums) on all host
+    cores, rank 0 only, on the same workload as our arm.  Each step is one run
+    of the whole workload (one instance of the batch, one query of the stream
+    for serve)."""
+    if rank != 0:
+        return
+    import oracle as orc
+    from velodb_b200 import workloads as W
+
+    orc.lib()
+    cores = os.cpu_count() or 1
+    unit = "Mrows/s"
+    extra = None
+    if args.workload == "sort":
+        n = 1 << 20
+        keys, pay = W.sort_kp(n)
+        steps = [(lambda: orc.bitonic_kp(keys, pay, n_threads=cores), n)]
+        sample, wl = "full 2^20-row network sort per step", "plain_sort_2^20"
+    elif args.workload == "batch":
+        insts = W.batch_instances()
+        order = [(i * 97) % len(insts) for i in range(len(insts))]
+
+        def inst_fn(it):
+            if it["kind"] == "sort":
+                return lambda: orc.bitonic_kp(it["keys"], it["pay"], n_threads=cores)
+            r = _batch_compact_rows(orc, it)
+            return lambda: orc.obl_compact_rec2(r, 1, 32, 0, n_threads=cores)
+
+        steps = [(inst_fn(insts[i]), insts[i]["n"]) for i in order]
+        sample = "one of the 512 instances per step (stride 97 through the list); network sorts and ORCompact " \
+                 "over next_pow2(n) rows, all cores"
+        wl = "batched_512"
+    elif args.workload == "groupby":
+        n = W.LINEITEM_ROWS
+        cols = W.lineitem(n)
+        steps = [(lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores, oblivious=True), n)]
+        sample, wl = "full 6,001,215-row table per step, oblivious pipeline", "filter_groupby"
+        extra = ("revealing_reference_semantics",
+                 lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores), n)
+    elif args.workload == "serve":
+        from velodb_b200 import serving as S
+
+        hs = S.HostSlices(**S.FULL_SCALE)
+        lo, hi = SERVE_SIZES_LOG2
+        qs = [q for q in S.query_stream(hs, 4 * (args.steps + args.warmup) + 8, seed=0xB200000000000004,
+                                        lo_log2=lo, hi_log2=hi) if q.shape != S.Q_JOIN3]
+
+        def q_fn(q):
+            if q.shape == S.Q_FILTER_GROUPBY:
+                cols = hs.lineitem(q.offset, q.n)
+                return lambda: orc.filter_groupby(cols, W.LINEITEM_PRED, 8, n_threads=cores, oblivious=True)
+            dim, fact = hs.join_inputs(q)
+            return lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, 10, n_threads=cores, oblivious=True)
+
+        steps = [(q_fn(q), 1) for q in qs]
+        unit = "queries/s"
+        sample = "one query per step from the served stream (sizes 2^10..2^18), filter+group-by and " \
+                 "two-way join shapes (the three-way chain has no oracle pipeline), oblivious pipelines"
+        wl = "served_stream"
+    else:
+        dim, fact = W.join_tables()
+        n = len(dim["key"]) + len(fact["fk"])
+        steps = [(lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, W.JOIN_TOPK, n_threads=cores,
+                                                oblivious=True), n)]
+        sample, wl = "full 1.5 M + 6 M-row join per step, oblivious pipeline", "join_groupby_top10"
+        extra = ("revealing_reference_semantics",
+                 lambda: orc.join_groupby_topk(dim, fact, W.JOIN_PRED, W.JOIN_TOPK, n_threads=cores), n)
+    for i in range(args.warmup):
+        steps[i % len(steps)][0]()
+    ts, units = [], 0
+    for i in range(args.steps):
+        fn, u = steps[(args.warmup + i) % len(steps)]
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+        units += u
+    total = float(np.sum(ts))
+    ms = 1e3 * total / args.steps
+    value = units / total / (1e6 if unit == "Mrows/s" else 1.0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": unit,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": wl},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    if extra is not None:
+        name, fn, u = extra
+        dt, reps = _timed_reps(fn, 3.0, 5)
+        line[name] = {"value": u / dt / 1e6, "unit": unit, "runs": reps,
+                      "what": "the reference's count-revealing semantics (the filtered or joined rows found by "
+                              "a serial scan, only those sorted)"}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+
+def make_workload(name, torch, capi, W, device):
+    if name == "groupby":
+        return GroupBy(torch, capi, W, device)
+    if name == "join":
+        return JoinTopK(torch, capi, W, device)
+    if name == "sort":
+        return SortKP(torch, capi, W, device)
+    if name == "batch":
+        return Batched(torch, capi, W, device)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def batch_plain(torch, wl, args):
+    """The plain path of the batch (512 launch sequences back to back) and the
+    batch's network bytes against both."""
+    peak, _ = hbm_peak()
+    for _ in range(2):
+        wl.step_plain()
+    torch.cuda.synchronize()
+    tp = time_steps(torch, wl.step_plain, max(3, args.steps // 2))
+    pms = float(np.mean(tp))
+    tb = time_steps(torch, wl.step, max(3, args.steps // 2))
+    bms = float(np.mean(tb))
+    nb = wl.network_bytes()
+    return {"plain_path": {"ms_per_step": pms, "value": wl.n / (pms / 1e3) / 1e6,
+                           "network_frac_of_hbm": nb / (pms / 1e3) / 1e9 / peak},
+            "batched_ms_per_step": bms, "speedup_batched_vs_plain": pms / bms,
+            "batched_network_frac_of_hbm": nb / (bms / 1e3) / 1e9 / peak,
+            "network_bytes_per_step": int(nb), "tune": list(wl.tune),
+            "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in wl.tune_ms.items()}}
+
+
+def run_extras(torch, capi, W, device, args, peak, peak_kind, orc):
+    """The other configurations, each measured and checked on its own (N = 1
+    only).  A failure is recorded in its key instead of ending the run."""
+    out = {}
+    sub = argparse.Namespace(steps=args.steps, warmup=args.warmup)
+
+    def one(key, mk, cpu_key=None):
+        try:
+            wl = mk()
+            r = measure(torch, capi, wl, sub, 1, device, peak, peak_kind)
+            r["roofline"] = roofline_of(torch, capi, wl, peak, peak_kind)
+            r["checked_against_oracle"] = wl.check(orc)
+            if cpu_key is not None:
+                r["cpu_baseline"] = cpu_baseline(cpu_key, W, orc, budget_s=5.0)
+            out[key] = r
+            del wl
+        except Exception as e:  # noqa: BLE001
+            out[key] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+
+    if args.workload != "sort":
+        one("sort_2^20", lambda: SortKP(torch, capi, W, device, 1 << 20), "sort")
+    one("sort_2^24", lambda: SortKP(torch, capi, W, device, 1 << 24))
+    if args.workload != "groupby":
+        one("filter_groupby", lambda: GroupBy(torch, capi, W, device), "groupby")
+    if args.workload != "batch":
+        try:
+            wl = Batched(torch, capi, W, device)
+            r = measure(torch, capi, wl, sub, 1, device, peak, peak_kind, with_e2e=False)
+            r.update(batch_plain(torch, wl, sub))
+            r["checked_against_oracle"] = wl.check(orc)
+            out["batched"] = r
+            del wl
+        except Exception as e:  # noqa: BLE001
+            out["batched"] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+    try:
+        out["served"] = measure_serve(torch)
+    except Exception as e:  # noqa: BLE001
+        out["served"] = {"error": f"{type(e).__name__}: {e}"}
+    return out
 
 
 def main():
@@ -863,7 +992,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "sort", "batch", "serve", "join"])
+    ap.add_argument("--workload", default="join", choices=["join", "sort", "groupby", "batch", "serve"])
+    ap.add_argument("--extras", default="all", choices=["all", "none"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -874,9 +1004,6 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, rank)
-        return
-    if args.workload == "serve":
-        run_serve(args, world, rank, local)
         return
 
     import torch
@@ -890,81 +1017,55 @@ def main():
         from datetime import timedelta
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
+    peak, peak_kind = hbm_peak()
+
+    if args.workload == "serve":
+        import ctypes
+
+        from velodb_b200._lib import VeloQuery, VeloQueryResult
+
+        res = measure_serve(torch)
+        value, _ = aggregate_throughput(res["served"]["qps_saturation"], 1e3, world, device, scale=1.0)
+        line = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": res["queries"],
+                "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+                "config": {"workload": "served_stream", "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2 (resident tables 4.9 GB)"},
+                "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": ctypes.sizeof(VeloQuery),
+                        "d2h_bytes_per_step": ctypes.sizeof(VeloQueryResult)},
+                "serve": res, "gpu_launches": None}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     wl = make_workload(args.workload, torch, capi, W, device)
-    l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=device) if wl.flush_l2 else None
-    flush = (lambda: l2_flush.fill_(1)) if l2_flush is not None else None
-
-    for _ in range(args.warmup):
-        wl.step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(torch.cuda.current_device())
-    clocks.start()
-    ts = time_steps(torch, wl.step, args.steps, flush)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    if world > 1:
-        dist.barrier()
-    rows_per_step = wl.n
-    value, ms = aggregate_throughput(rows_per_step, float(np.mean(ts)), world, device)
-
-    # end to end through the public API with host buffers
-    for _ in range(2):
-        wl.step_e2e()
-    torch.cuda.synchronize()
-    te = time_steps(torch, wl.step_e2e, max(3, args.steps // 2))
-    e2e_value, ems = aggregate_throughput(rows_per_step, float(np.mean(te)), world, device)
-    e2e = {"value": e2e_value, "unit": "Mrows/s",
-           "h2d_bytes_per_step": int(wl.in_bytes), "d2h_bytes_per_step": int(wl.d2h_bytes()), "ms_per_step": ems}
-
-    if hasattr(wl, "step_plain"):
-        for _ in range(2):
-            wl.step_plain()
-        torch.cuda.synchronize()
-        tp = time_steps(torch, wl.step_plain, max(3, args.steps // 2))
-        pms = float(np.mean(tp))
-        plain = {"ms_per_step": pms, "value": world * rows_per_step / (pms / 1e3) / 1e6,
-                 "speedup_batched_vs_plain": pms / ms, "tune": list(wl.tune),
-                 "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in wl.tune_ms.items()}}
-    else:
-        plain = None
-
-    # the result of the last step is checked against the oracle (rank 0)
-    peak, peak_kind = hbm_peak()
-    rdm = wl.rdm_bytes()
+    res = measure(torch, capi, wl, args, world, device, peak, peak_kind)
     line = {
-        "metric": metric_name(args.workload), "value": value, "unit": "Mrows/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "metric": METRIC, "value": res["value"], "unit": "Mrows/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": wl.name, "rows": rows_per_step, "padded_rows": wl.np_rows,
-                   "record_bytes": wl.rec_bytes, "parallelism": f"replicas{world}",
-                   "l2": "flushed between steps" if wl.flush_l2 else "inputs larger than L2"},
-        "e2e": e2e,
-        "gpu_launches": int(wl.launches() * args.steps),
-        "rdm": {"bytes_per_step": int(rdm), "achieved_gbs": rdm / (ms / 1e3) / 1e9,
-                "frac_of_hbm": rdm / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind},
-        "clocks": clk,
+        "config": dict(res["config"], parallelism=f"replicas{world}", l2=res["l2"]),
+        "e2e": res["e2e"], "gpu_launches": res["gpu_launches"], "rdm": res["rdm"], "clocks": res["clocks"],
     }
-    if plain is not None:
-        line["plain_path"] = plain
-    dom = wl.dominant(device)
-    achieved = dom["bytes_per_launch"] / (dom["avg_launch_us"] / 1e6) / 1e9
-    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
-                        if peak_kind == "measured" else "fallback", "traffic": TRAFFIC.get(args.workload),
-                        "kernel": dom["kernel"], "avg_launch_us": dom["avg_launch_us"],
-                        "algorithmic_bytes_per_launch": dom["bytes_per_launch"]}
+    line["roofline"] = roofline_of(torch, capi, wl, peak, peak_kind)
+    if isinstance(wl, Batched):
+        line.update(batch_plain(torch, wl, args))
+    orc = None
     if rank == 0:
         import oracle as orc
 
         orc.lib()
         line["checked_against_oracle"] = wl.check(orc)
-        if not args.no_cpu_baseline:
-            line["cpu_baseline"] = {"groupby": cpu_baseline_groupby, "sort": cpu_baseline_sort,
-                                    "batch": cpu_baseline_batch, "join": cpu_baseline_join}[args.workload](W, orc)
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(wl.key, W, orc)
+    if world == 1 and args.extras == "all":
+        del wl
+        torch.cuda.empty_cache()
+        line["extras"] = run_extras(torch, capi, W, device, args, peak, peak_kind, orc)
+    if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -84,6 +84,29 @@ const char* velo_last_error_text(void);
 void velo_set_stage_timing(int on);
 int velo_last_stage_times(float* ms, int capacity);
 
+/*
+ * Pass timing for profilers (off by default; process-wide switch).  While it
+ * is on, every network pass (bitonic tile sort, fused global levels, in-tile
+ * merge, ORCompact tile and global passes) is bracketed by CUDA events on its
+ * stream, and each call that launches passes synchronizes that stream before
+ * returning and appends one velo_pass_time per pass to the calling thread's
+ * list (at most 1024 entries; velo_set_pass_timing and velo_pass_times_clear
+ * empty it).  kind: 0 tile sort, 1 in-tile merge, 2 global levels, 3 ORCompact
+ * tile pass, 4 ORCompact global levels; row_bytes: bytes of one row the pass
+ * reads and writes.  The events keep consecutive passes from overlapping, so
+ * the figures are per-pass durations, not the pipelined whole.
+ * No reference counterpart: a measurement hook of this implementation.
+ */
+typedef struct velo_pass_time {
+    uint32_t kind;
+    uint32_t log_n;
+    uint32_t row_bytes;
+    float ms;
+} velo_pass_time;
+void velo_set_pass_timing(int on);
+void velo_pass_times_clear(void);
+int velo_last_pass_times(velo_pass_time* out, int capacity);
+
 /* ------------------------------------------------------------------------ */
 /* Bitonic network sort                                                     */
 /* ------------------------------------------------------------------------ */
@@ -314,6 +337,24 @@ velo_status velo_ojoin_pkfk(const void* d_build_keys, const uint8_t* d_build_mas
                             const void* d_probe_keys, const uint8_t* d_probe_mask, size_t probe_n, uint32_t key_type,
                             int64_t* d_out_build_rowid, int64_t* d_out_probe_rowid, uint64_t* d_counts,
                             void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* Oblivious many-to-many equi-join: every pair (build row b, probe row p)
+ * with key_b == key_p and both rows valid (mask != 0; NULL = all valid), the
+ * output of the reference's sort-merge join (the cross product of every run
+ * of equal keys, include/cuda/sort_merge_join.cuh:63-199, sized from the true
+ * pair count in src/operator/sort_merge_join_operator.cpp:114-148), padded to
+ * the public bound max_pairs.  Rows [0, min(pairs, max_pairs)) of the two
+ * outputs hold the pairs in (key, probe row id, build row id) order, the rest
+ * -1.  d_counts: 2 u64 = (pairs, 1 if pairs > max_pairs else 0); a caller
+ * that must not lose pairs re-runs with max_pairs >= pairs, which reveals the
+ * pair count as the reference does.  Every launch and address depends only on
+ * build_n, probe_n and max_pairs (all below 2^31).  key_type: VELO_INTEGER or
+ * VELO_BIGINT.  d_scratch: velo_ojoin_mn_scratch_bytes() bytes. */
+size_t velo_ojoin_mn_scratch_bytes(size_t build_n, size_t probe_n, size_t max_pairs);
+velo_status velo_ojoin_mn(const void* d_build_keys, const uint8_t* d_build_mask, size_t build_n,
+                          const void* d_probe_keys, const uint8_t* d_probe_mask, size_t probe_n, uint32_t key_type,
+                          size_t max_pairs, int64_t* d_out_build_rowid, int64_t* d_out_probe_rowid,
+                          uint64_t* d_counts, void* d_scratch, size_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Batched form: one persistent launch for many independent commands        */

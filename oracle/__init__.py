@@ -61,6 +61,17 @@ def lib() -> C.CDLL:
         L.orc_filter_groupby.restype = sz
         L.orc_join_groupby_topk.argtypes = [sz, vp, vp, sz, vp, vp, C.c_int32, C.c_int64, sz, vp, vp, vp, i32]
         L.orc_join_groupby_topk.restype = sz
+        u64 = C.c_uint64
+        L.orc_smj_pairs.argtypes = [vp, vp, sz, vp, vp, sz, vp, vp, sz]
+        L.orc_smj_pairs.restype = sz
+        L.orc_obl_sort_rec2.argtypes = [vp, sz, u64, u64, i32]
+        L.orc_obl_sort_rec2.restype = None
+        L.orc_obl_compact_rec2.argtypes = [vp, sz, i32, i32, i32, i32]
+        L.orc_obl_compact_rec2.restype = sz
+        L.orc_obl_filter_groupby.argtypes = L.orc_filter_groupby.argtypes
+        L.orc_obl_filter_groupby.restype = sz
+        L.orc_obl_join_groupby_topk.argtypes = L.orc_join_groupby_topk.argtypes
+        L.orc_obl_join_groupby_topk.restype = sz
         _lib = L
     return _lib
 
@@ -217,23 +228,26 @@ def groupby_sorted(keys: np.ndarray, vals: np.ndarray):
     return ok[:g], os_[:g]
 
 
-def filter_groupby(cols: dict, pred: dict, max_groups: int = 8, n_threads: int = 0):
+def filter_groupby(cols: dict, pred: dict, max_groups: int = 8, n_threads: int = 0, oblivious: bool = False):
     """Filter + group-by oracle.  cols: qty, price, disc, tax, shipdate, flag1,
     flag2 (numpy arrays); pred: ship_lo/ship_hi/disc_lo/disc_hi/qty_lo/qty_hi.
-    Returns (group count, keys[g], sums[g, 5])."""
+    Returns (group count, keys[g], sums[g, 5]).  oblivious=True runs the
+    oblivious CPU pipeline (orc_obl_filter_groupby: ORCompact and a network
+    sort over all next_pow2(n) rows) instead of the count-revealing one."""
     n = len(cols["qty"])
     arrs = [np.ascontiguousarray(cols[k]) for k in ("qty", "price", "disc", "tax", "shipdate", "flag1", "flag2")]
     ok = np.zeros(max_groups, np.uint64)
     os_ = np.zeros((max_groups, 5), np.int64)
-    g = lib().orc_filter_groupby(n, *[_p(a) for a in arrs], pred["ship_lo"], pred["ship_hi"], pred["disc_lo"],
-                                 pred["disc_hi"], pred["qty_lo"], pred["qty_hi"], max_groups, _p(ok), _p(os_),
-                                 n_threads)
+    fn = lib().orc_obl_filter_groupby if oblivious else lib().orc_filter_groupby
+    g = fn(n, *[_p(a) for a in arrs], pred["ship_lo"], pred["ship_hi"], pred["disc_lo"], pred["disc_hi"],
+           pred["qty_lo"], pred["qty_hi"], max_groups, _p(ok), _p(os_), n_threads)
     g = int(g)
     return g, ok[:min(g, max_groups)], os_[:min(g, max_groups)]
 
 
-def join_groupby_topk(dim: dict, fact: dict, pred: dict, k: int = 10, n_threads: int = 0):
-    """PK-FK join + group-by + top-k oracle; returns (n_groups, fk, sum, cnt)."""
+def join_groupby_topk(dim: dict, fact: dict, pred: dict, k: int = 10, n_threads: int = 0, oblivious: bool = False):
+    """PK-FK join + group-by + top-k oracle; returns (n_groups, fk, sum, cnt).
+    oblivious=True runs the oblivious CPU pipeline (orc_obl_join_groupby_topk)."""
     dk = np.ascontiguousarray(dim["key"], np.int32)
     dd = np.ascontiguousarray(dim["date"], np.int32)
     ff = np.ascontiguousarray(fact["fk"], np.int32)
@@ -241,11 +255,44 @@ def join_groupby_topk(dim: dict, fact: dict, pred: dict, k: int = 10, n_threads:
     ofk = np.zeros(k, np.int32)
     osum = np.zeros(k, np.int64)
     ocnt = np.zeros(k, np.int64)
-    g = lib().orc_join_groupby_topk(len(dk), _p(dk), _p(dd), len(ff), _p(ff), _p(fp), pred["date_hi"],
-                                    pred["price_hi"], k, _p(ofk), _p(osum), _p(ocnt), n_threads)
+    fn = lib().orc_obl_join_groupby_topk if oblivious else lib().orc_join_groupby_topk
+    g = fn(len(dk), _p(dk), _p(dd), len(ff), _p(ff), _p(fp), pred["date_hi"], pred["price_hi"], k, _p(ofk),
+           _p(osum), _p(ocnt), n_threads)
     g = int(g)
     m = min(g, k)
     return g, ofk[:m], osum[:m], ocnt[:m]
+
+
+def smj_pairs(left_keys, left_mask, right_keys, right_mask, cap=None):
+    """Reference sort-merge join output: (left row ids, right row ids,
+    total pairs) in (key, left row id, right row id) order."""
+    lk = np.ascontiguousarray(left_keys, dtype=np.int64)
+    rk = np.ascontiguousarray(right_keys, dtype=np.int64)
+    lm = None if left_mask is None else np.ascontiguousarray(left_mask, dtype=np.uint8)
+    rm = None if right_mask is None else np.ascontiguousarray(right_mask, dtype=np.uint8)
+    if cap is None:
+        cap = lib().orc_smj_pairs(_p(lk), None if lm is None else _p(lm), len(lk), _p(rk),
+                                  None if rm is None else _p(rm), len(rk), None, None, 0)
+    ol = np.zeros(max(int(cap), 1), np.int64)
+    orr = np.zeros(max(int(cap), 1), np.int64)
+    tot = lib().orc_smj_pairs(_p(lk), None if lm is None else _p(lm), len(lk), _p(rk),
+                              None if rm is None else _p(rm), len(rk), _p(ol), _p(orr), int(cap))
+    m = min(int(tot), int(cap))
+    return ol[:m], orr[:m], int(tot)
+
+
+def obl_sort_rec2(recs: np.ndarray, m0: int, m1: int, n_threads: int = 0) -> np.ndarray:
+    """Oblivious CPU network sort of (n, 2) u64 records (n a power of two)."""
+    r = np.ascontiguousarray(recs, dtype=np.uint64).copy()
+    lib().orc_obl_sort_rec2(_p(r), r.shape[0], m0, m1, n_threads)
+    return r
+
+
+def obl_compact_rec2(recs: np.ndarray, word: int, bit: int, inv: int, n_threads: int = 0):
+    """Oblivious CPU ORCompact of (n, 2) u64 records (n a power of two)."""
+    r = np.ascontiguousarray(recs, dtype=np.uint64).copy()
+    c = lib().orc_obl_compact_rec2(_p(r), r.shape[0], word, bit, inv, n_threads)
+    return r, int(c)
 
 
 # --------------------------------------------------------------------------

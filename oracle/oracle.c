@@ -549,3 +549,72 @@ size_t orc_join_groupby_topk(size_t n_dim, const int32_t* dim_key, const int32_t
     free(s2);
     return g;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Sort-merge equi-join: reference include/cuda/sort_merge_join.cuh:63-199    */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int64_t key;
+    int64_t rowid;
+} orc_kr;
+
+static int kr_cmp(const void* a, const void* b)
+{
+    const orc_kr* x = (const orc_kr*)a;
+    const orc_kr* y = (const orc_kr*)b;
+    if (x->key != y->key)
+        return x->key < y->key ? -1 : 1;
+    return (x->rowid > y->rowid) - (x->rowid < y->rowid);
+}
+
+static size_t kr_side(const int64_t* keys, const uint8_t* mask, size_t n, orc_kr** out)
+{
+    orc_kr* s = (orc_kr*)malloc((n ? n : 1) * sizeof(orc_kr));
+    size_t m = 0;
+    for (size_t i = 0; i < n; i++)
+        if (!mask || mask[i]) {
+            s[m].key = keys[i];
+            s[m].rowid = (int64_t)i;
+            m++;
+        }
+    qsort(s, m, sizeof(orc_kr), kr_cmp);
+    *out = s;
+    return m;
+}
+
+size_t orc_smj_pairs(const int64_t* lkeys, const uint8_t* lmask, size_t nl, const int64_t* rkeys,
+                     const uint8_t* rmask, size_t nr, int64_t* out_l, int64_t* out_r, size_t cap)
+{
+    orc_kr *L, *R;
+    const size_t ln = kr_side(lkeys, lmask, nl, &L);
+    const size_t rn = kr_side(rkeys, rmask, nr, &R);
+    /* mergeBlockCount (:61-101) with one block over the whole left side, then
+     * writeJoinResults (:136-150): left-major, right-minor per key block */
+    size_t l = 0, r = 0, total = 0;
+    while (l < ln && r < rn) {
+        if (L[l].key < R[r].key) {
+            l++;
+        } else if (L[l].key > R[r].key) {
+            r++;
+        } else {
+            const int64_t key = L[l].key;
+            const size_t l0 = l, r0 = r;
+            while (l < ln && L[l].key == key)
+                l++;
+            while (r < rn && R[r].key == key)
+                r++;
+            for (size_t a = l0; a < l; a++)
+                for (size_t b = r0; b < r; b++) {
+                    if (total < cap) {
+                        out_l[total] = L[a].rowid;
+                        out_r[total] = R[b].rowid;
+                    }
+                    total++;
+                }
+        }
+    }
+    free(L);
+    free(R);
+    return total;
+}

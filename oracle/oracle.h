@@ -97,6 +97,50 @@ size_t orc_join_groupby_topk(size_t n_dim, const int32_t* dim_key, const int32_t
                              const int32_t* fact_fk, const int64_t* fact_price, int32_t date_hi, int64_t price_hi,
                              size_t k, int32_t* out_fk, int64_t* out_sum, int64_t* out_cnt, int n_threads);
 
+/* Sort-merge inner equi-join with the reference's output, reference
+ * include/cuda/sort_merge_join.cuh:63-199: both sides (rows with mask != 0;
+ * NULL = all) sorted by (key, row id), merged, and every run of equal keys
+ * written as its cross product, left row major.  Writes up to cap pairs of
+ * (left row id, right row id) in (key, left row id, right row id) order and
+ * returns the total pair count. */
+size_t orc_smj_pairs(const int64_t* lkeys, const uint8_t* lmask, size_t nl, const int64_t* rkeys,
+                     const uint8_t* rmask, size_t nr, int64_t* out_l, int64_t* out_r, size_t cap);
+
+/* ------------------------------------------------------------------------ */
+/* Oblivious CPU pipelines (oracle_obl.c): the timed CPU baseline.  The same  */
+/* steps as the device pipelines, with no data-dependent branch, address or  */
+/* size: network sorts over all next_pow2(n) rows, ORCompact, segmented      */
+/* sums with masked slot adds.  OpenMP over n_threads (<= 0: all).           */
+/* ------------------------------------------------------------------------ */
+
+/* Bitonic network (reference order, strict exchanges) over np 16-byte
+ * records {w0, w1}, ascending on (w0 & m0, w1 & m1); np a power of two. */
+void orc_obl_sort_rec2(void* recs, size_t np, uint64_t m0, uint64_t m1, int n_threads);
+
+/* ORCompact (liboblivious compact_offset, algorithms.c:118-153) of np
+ * 16-byte records; a record is marked when bit `bit` of word `word`, XOR
+ * inv, is 1.  np a power of two.  Returns the number of marked records. */
+size_t orc_obl_compact_rec2(void* recs, size_t np, int word, int bit, int inv, int n_threads);
+
+/* orc_filter_groupby's result (same contract) from the oblivious steps:
+ * predicate -> ORCompact of all next_pow2(n) rows -> network sort of all of
+ * them on the group key -> segmented sums into max_groups ranked slots. */
+size_t orc_obl_filter_groupby(size_t n, const int32_t* qty, const int64_t* price, const int32_t* disc,
+                              const int32_t* tax, const int32_t* shipdate, const uint8_t* flag1,
+                              const uint8_t* flag2, int32_t ship_lo, int32_t ship_hi, int32_t disc_lo,
+                              int32_t disc_hi, int32_t qty_lo, int32_t qty_hi, size_t max_groups,
+                              uint64_t* out_keys, int64_t* out_sums, int n_threads);
+
+/* orc_join_groupby_topk's result (same contract) from the oblivious steps:
+ * union -> network sort on (key, tag) -> forward fill -> ORCompact of the
+ * joined rows -> segmented sums -> ORCompact of the group records -> network
+ * sort of next_pow2(n_dim) group records on (sum desc, fk asc).  Keys must be
+ * below INT32_MAX (the pad key). */
+size_t orc_obl_join_groupby_topk(size_t n_dim, const int32_t* dim_key, const int32_t* dim_date, size_t n_fact,
+                                 const int32_t* fact_fk, const int64_t* fact_price, int32_t date_hi,
+                                 int64_t price_hi, size_t k, int32_t* out_fk, int64_t* out_sum, int64_t* out_cnt,
+                                 int n_threads);
+
 #ifdef __cplusplus
 }
 #endif

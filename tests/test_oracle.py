@@ -236,3 +236,52 @@ def test_workload_generators_are_deterministic():
     assert set(np.unique(li["flag1"])) == {0, 1, 2} and set(np.unique(li["flag2"])) == {0, 1}
     dim, fact = W.join_tables(1000, 4000)
     assert np.array_equal(np.sort(dim["key"]), np.arange(1, 1001))
+
+
+# ---- the oblivious CPU pipelines (the timed CPU baseline) ------------------
+
+@pytest.mark.parametrize("n", [1, 2, 1000, 50_000, 300_001])
+def test_oblivious_cpu_filter_groupby_equals_oracle(orc, n):
+    cols = W.lineitem(n, seed=W.SEED_LINEITEM + 5)
+    for pred in (W.LINEITEM_PRED, dict(ship_lo=0, ship_hi=2556, disc_lo=0, disc_hi=10, qty_lo=1, qty_hi=50),
+                 dict(ship_lo=9000, ship_hi=9001, disc_lo=0, disc_hi=10, qty_lo=1, qty_hi=50)):
+        a = orc.filter_groupby(cols, pred, 8)
+        b = orc.filter_groupby(cols, pred, 8, oblivious=True)
+        assert a[0] == b[0] and np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+
+
+@pytest.mark.parametrize("nd,nf", [(1, 1), (10, 40), (1000, 4000), (30_000, 120_000)])
+def test_oblivious_cpu_join_equals_oracle(orc, nd, nf):
+    dim, fact = W.join_tables(nd, nf, seed=W.SEED_JOIN + 9)
+    for pred in (W.JOIN_PRED, dict(date_hi=10**6, price_hi=10**12), dict(date_hi=-1, price_hi=10**12)):
+        a = orc.join_groupby_topk(dim, fact, pred, 10)
+        b = orc.join_groupby_topk(dim, fact, pred, 10, oblivious=True)
+        assert a[0] == b[0] and all(np.array_equal(x, y) for x, y in zip(a[1:], b[1:]))
+
+
+@pytest.mark.parametrize("n", [2, 64, 4096, 1 << 16])
+def test_oblivious_cpu_compaction_equals_restatement(orc, n):
+    rng = np.random.default_rng(n)
+    rec = np.zeros((n, 2), np.uint64)
+    rec[:, 0] = rng.integers(0, 2**62, n, dtype=np.uint64)
+    marks = rng.random(n) < 0.3
+    rec[:, 1] = (np.arange(n, dtype=np.uint64) << np.uint64(8)) | (marks.astype(np.uint64) << np.uint64(5))
+    got, cnt = orc.obl_compact_rec2(rec, 1, 5, 0)
+    d, _, c2 = orc.ocompact(rec.view(np.uint8).reshape(n, 16).copy(), marks.astype(np.uint8))
+    assert cnt == c2 == int(marks.sum())
+    assert np.array_equal(got, d.view(np.uint64).reshape(n, 2))
+    s = orc.obl_sort_rec2(rec, 2**64 - 1, 0)
+    assert np.array_equal(s[:, 0], np.sort(rec[:, 0]))
+
+
+def test_smj_pairs_equal_brute_force(orc):
+    rng = np.random.default_rng(3)
+    left = rng.integers(0, 30, 400)
+    right = rng.integers(0, 30, 300)
+    lm = rng.random(400) < 0.8
+    rm = rng.random(300) < 0.7
+    ol, orr, tot = orc.smj_pairs(left, lm, right, rm)
+    want = sorted((int(left[a]), a, b) for a in range(400) for b in range(300)
+                  if lm[a] and rm[b] and left[a] == right[b])
+    assert tot == len(want)
+    assert [(int(left[a]), int(a), int(b)) for a, b in zip(ol, orr)] == want

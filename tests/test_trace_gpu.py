@@ -356,3 +356,31 @@ def test_ogroupby_trace_is_data_independent(T):
              (np.arange(n, dtype=np.int32), 1.0),                  # every row its own group
              (np.zeros(n, np.int32), 0.0)]                         # one key, nothing selected
     assert_same_trace([trace_of(T, run(k, d)) for k, d in cases])
+
+
+def test_mn_join_trace_is_data_independent(T):
+    bn, pn, mp = 6_000, 20_000, 50_000
+    bk = torch.empty(bn, dtype=torch.int32, device="cuda")
+    pk = torch.empty(pn, dtype=torch.int32, device="cuda")
+    bm = torch.empty(bn, dtype=torch.uint8, device="cuda")
+    ob = torch.empty(mp, dtype=torch.int64, device="cuda")
+    op = torch.empty(mp, dtype=torch.int64, device="cuda")
+    jc = torch.empty(2, dtype=torch.int64, device="cuda")
+    sb = T.velo_ojoin_mn_scratch_bytes(bn, pn, mp)
+    s = torch.empty(sb, dtype=torch.uint8, device="cuda")
+
+    def join(seed, span, all_masked=False):
+        def f():
+            rng = np.random.default_rng(seed)
+            dev_copy(bk, rng.integers(0, span, bn).astype(np.int32))
+            dev_copy(pk, rng.integers(0, span, pn).astype(np.int32))
+            dev_copy(bm, np.zeros(bn, np.uint8) if all_masked else (rng.random(bn) < 0.7).astype(np.uint8))
+            torch.cuda.synchronize()
+            assert T.velo_ojoin_mn(bk.data_ptr(), bm.data_ptr(), bn, pk.data_ptr(), None, pn, 4, mp, ob.data_ptr(),
+                                   op.data_ptr(), jc.data_ptr(), s.data_ptr(), sb, None) == 0
+        return f
+
+    # many matches per key, one key only (overflowing the bound), no key
+    # matching at all, every build row left out
+    assert_same_trace([trace_of(T, join(x, sp, am)) for x, sp, am in
+                       ((1, 3000, False), (2, 3000, False), (3, 1, False), (4, 10**9, False), (5, 3000, True))])

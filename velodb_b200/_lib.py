@@ -18,6 +18,9 @@ PROTOS = {
     "velo_next_pow2": (sz, [sz]),
     "velo_last_error_text": (C.c_char_p, []),
     "velo_set_stage_timing": (None, [i32]),
+    "velo_set_pass_timing": (None, [i32]),
+    "velo_pass_times_clear": (None, []),
+    "velo_last_pass_times": (i32, [vp, i32]),
     "velo_trace_enabled": (i32, []),
     "velo_trace_begin": (i32, [u64, u64]),
     "velo_trace_end": (i32, [vp, vp, vp, u64, vp]),
@@ -56,6 +59,8 @@ PROTOS = {
     "velo_ogather_u64": (i32, [vp, sz, vp, sz, vp, vp, sz, vp]),
     "velo_ojoin_scratch_bytes": (sz, [sz, sz]),
     "velo_ojoin_pkfk": (i32, [vp, vp, sz, vp, vp, sz, u32, vp, vp, vp, vp, sz, vp]),
+    "velo_ojoin_mn_scratch_bytes": (sz, [sz, sz, sz]),
+    "velo_ojoin_mn": (i32, [vp, vp, sz, vp, vp, sz, u32, sz, vp, vp, vp, vp, sz, vp]),
     "velo_init": (i32, [vp, vp]),
     "velo_shutdown": (i32, [vp, u32]),
     "velo_submit": (i32, [vp, vp, vp]),
@@ -123,6 +128,10 @@ def last_error() -> str:
 def check(status: int, what: str) -> None:
     if status != 0:
         raise VeloError(status, what, last_error())
+
+
+class VeloPassTime(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("log_n", C.c_uint32), ("row_bytes", C.c_uint32), ("ms", C.c_float)]
 
 
 class VeloLineitem(C.Structure):

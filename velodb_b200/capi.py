@@ -5,6 +5,8 @@ operators is computed by the sm_100a kernels in libvelo_obl.so.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 
@@ -31,6 +33,30 @@ def last_stage_times() -> list:
     buf = np.zeros(8, dtype=np.float32)
     n = int(lib().velo_last_stage_times(buf.ctypes.data, 8))
     return [float(x) for x in buf[:n]]
+
+
+PASS_KINDS = {0: "tile_sort", 1: "merge", 2: "global", 3: "compact_tile", 4: "compact_global"}
+
+
+def set_pass_timing(on: bool) -> None:
+    """Switch per-pass CUDA-event timing of the network passes
+    (velo_set_pass_timing); clears this thread's pass list."""
+    lib().velo_set_pass_timing(1 if on else 0)
+
+
+def clear_pass_times() -> None:
+    lib().velo_pass_times_clear()
+
+
+def last_pass_times() -> list:
+    """(kind name, log2 rows, row bytes, ms) of every network pass this thread
+    launched since the list was last cleared."""
+    from ._lib import VeloPassTime
+
+    buf = (VeloPassTime * 1024)()
+    n = int(lib().velo_last_pass_times(C.cast(buf, C.c_void_p), 1024))
+    return [(PASS_KINDS.get(int(buf[i].kind), str(buf[i].kind)), int(buf[i].log_n), int(buf[i].row_bytes),
+             float(buf[i].ms)) for i in range(n)]
 
 
 def to_dev_u64(a: np.ndarray, capacity: int | None = None, device="cuda") -> torch.Tensor:
@@ -332,6 +358,22 @@ def ojoin_pkfk(build_keys, build_mask, probe_keys, probe_mask, key_type, stream=
     check(lib().velo_ojoin_pkfk(build_keys.data_ptr(), _ptr(build_mask), bn, probe_keys.data_ptr(), _ptr(probe_mask),
                                 pn, key_type, ob.data_ptr(), op.data_ptr(), cnt.data_ptr(), sc.data_ptr(), sc.numel(),
                                 _stream(stream)), "velo_ojoin_pkfk")
+    return ob, op, cnt
+
+
+def ojoin_mn(build_keys, build_mask, probe_keys, probe_mask, key_type, max_pairs, stream=None):
+    """Oblivious many-to-many equi-join (velo_ojoin_mn).  Returns (build
+    rowids, probe rowids, counts[2] = (pairs, overflow)) device tensors of
+    max_pairs rows; rows past the pair count are -1."""
+    bn, pn = build_keys.numel(), probe_keys.numel()
+    dev = build_keys.device
+    ob = torch.empty(max_pairs, dtype=torch.int64, device=dev)
+    op = torch.empty(max_pairs, dtype=torch.int64, device=dev)
+    cnt = torch.zeros(2, dtype=torch.int64, device=dev)
+    sc = _scratch(lib().velo_ojoin_mn_scratch_bytes(bn, pn, max_pairs), dev)
+    check(lib().velo_ojoin_mn(build_keys.data_ptr(), _ptr(build_mask), bn, probe_keys.data_ptr(), _ptr(probe_mask),
+                              pn, key_type, max_pairs, ob.data_ptr(), op.data_ptr(), cnt.data_ptr(), sc.data_ptr(),
+                              sc.numel(), _stream(stream)), "velo_ojoin_mn")
     return ob, op, cnt
 
 

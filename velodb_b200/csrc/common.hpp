@@ -58,6 +58,12 @@ constexpr int MAX_LOGN = 31;
 bool stage_timing_on();
 void store_stage_times(const float* ms, int n);
 
+// Pass timing (velo_set_pass_timing): while on, launch_net records an event
+// after each network pass and appends (kind, log2 rows, row bytes, ms) of
+// every pass to the calling thread's list.
+bool pass_timing_on();
+void store_pass_time(int kind, int log_n, int row_bytes, float ms);
+
 class StageTimer {
 public:
     static constexpr int MAX_STAGES = 8;

@@ -62,6 +62,61 @@ __global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<R, LOG_NT>())
     Net<R, LOG_NT, LOG_E>::template run<false>(c, g, p, tile_prefix, blockIdx.x, sm);
 }
 
+// bytes of one row that a pass reads and writes
+template <class R>
+struct RowBytes {
+    static constexpr int value = R::WORDS * 8;
+};
+template <>
+struct RowBytes<RowKP> {
+    static constexpr int value = 12;
+};
+template <>
+struct RowBytes<RowKPM> {
+    static constexpr int value = 13;
+};
+
+// Events around each pass while pass timing is on (velo_set_pass_timing);
+// inert otherwise.
+class PassTimer {
+public:
+    PassTimer(cudaStream_t st, size_t n) : st_(st), on_(pass_timing_on()), ev_(on_ ? n + 1 : 0, nullptr)
+    {
+        for (auto& e : ev_)
+            if (cudaEventCreate(&e) != cudaSuccess)
+                on_ = false;
+        if (on_)
+            cudaEventRecord(ev_[0], st_);
+    }
+    bool on() const { return on_; }
+    void mark(size_t i)
+    {
+        if (on_)
+            cudaEventRecord(ev_[i + 1], st_);
+    }
+    void finish(const std::vector<NetPass>& passes, int log_n, int row_bytes)
+    {
+        if (!on_ || cudaEventSynchronize(ev_.back()) != cudaSuccess)
+            return;
+        for (size_t i = 0; i < passes.size(); i++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev_[i], ev_[i + 1]);
+            store_pass_time(passes[i].kind, log_n, row_bytes, ms);
+        }
+    }
+    ~PassTimer()
+    {
+        for (auto e : ev_)
+            if (e)
+                cudaEventDestroy(e);
+    }
+
+private:
+    cudaStream_t st_;
+    bool on_;
+    std::vector<cudaEvent_t> ev_;
+};
+
 template <class R, int LOG_NT, int LOG_E>
 velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::vector<NetPass>& passes,
                        const uint32_t* tile_prefix, cudaStream_t st)
@@ -94,6 +149,7 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
+    PassTimer timer(st, passes.size());
     for (size_t i = 0; i < passes.size(); i++) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)grid);
@@ -101,10 +157,12 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
         cfg.dynamicSmemBytes = smem;
         cfg.stream = st;
         cfg.attrs = attr;
-        cfg.numAttrs = i > 0 ? 1 : 0;
+        cfg.numAttrs = (i > 0 && !timer.on()) ? 1 : 0;
         auto kern = compact ? k_comp : passes[i].kind == P_SORT_GLOBAL ? k_global : k_local;
         VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, c, g, passes[i], tile_prefix), "network pass launch");
+        timer.mark(i);
     }
+    timer.finish(passes, g.logN, RowBytes<R>::value);
     return VELO_OK;
 }
 

@@ -98,6 +98,35 @@ extern "C" int velo_last_stage_times(float* ms, int capacity)
     return ms ? n : g_stage_n;
 }
 
+static std::atomic<int> g_pass_timing { 0 };
+constexpr int PASS_LOG_CAP = 1024;
+static thread_local velo_pass_time g_pass_log[PASS_LOG_CAP];
+static thread_local int g_pass_n = 0;
+
+bool velo::pass_timing_on() { return g_pass_timing.load(std::memory_order_relaxed) != 0; }
+
+void velo::store_pass_time(int kind, int log_n, int row_bytes, float ms)
+{
+    if (g_pass_n < PASS_LOG_CAP)
+        g_pass_log[g_pass_n++] = velo_pass_time { (uint32_t)kind, (uint32_t)log_n, (uint32_t)row_bytes, ms };
+}
+
+extern "C" void velo_set_pass_timing(int on)
+{
+    g_pass_timing.store(on ? 1 : 0, std::memory_order_relaxed);
+    g_pass_n = 0;
+}
+
+extern "C" void velo_pass_times_clear(void) { g_pass_n = 0; }
+
+extern "C" int velo_last_pass_times(velo_pass_time* out, int capacity)
+{
+    const int n = capacity < g_pass_n ? capacity : g_pass_n;
+    for (int i = 0; out && i < n; i++)
+        out[i] = g_pass_log[i];
+    return out ? n : g_pass_n;
+}
+
 extern "C" const char* velo_last_error_text(void)
 {
     return g_last_error.c_str();

@@ -1,0 +1,230 @@
+// Building blocks of the union-sort operators (oblivious gather, joins):
+// the forward fill over a key-sorted record array and the scratch layout of
+// a union of 3-word records.  Included by the translation units that
+// implement those operators.
+#pragma once
+
+#include "net_impl.cuh"
+
+namespace velo {
+
+// ---------------------------------------------------------------------------
+// forward fill over a key-sorted record array: every row receives the
+// (key, value) of the last "source" row at or before it (segmented scan in
+// three passes; addresses never depend on the data)
+// ---------------------------------------------------------------------------
+
+struct FillCarry {
+    uint64_t key;
+    uint64_t val;
+    uint32_t has;
+    uint32_t valid;
+};
+
+__device__ __forceinline__ FillCarry fill_combine(const FillCarry& l, const FillCarry& r)
+{
+    return r.has ? r : l;
+}
+
+constexpr int FL_TS = 2048, FL_THREADS = 256, FL_RPT = FL_TS / FL_THREADS;
+
+__device__ __forceinline__ FillCarry fill_shfl(const FillCarry& c, int d, bool up)
+{
+    FillCarry r;
+    const uint32_t hv = c.has | (c.valid << 1);
+    const uint32_t x = up ? __shfl_up_sync(0xFFFFFFFFu, hv, d) : __shfl_xor_sync(0xFFFFFFFFu, hv, d);
+    r.key = up ? __shfl_up_sync(0xFFFFFFFFu, c.key, d) : __shfl_xor_sync(0xFFFFFFFFu, c.key, d);
+    r.val = up ? __shfl_up_sync(0xFFFFFFFFu, c.val, d) : __shfl_xor_sync(0xFFFFFFFFu, c.val, d);
+    r.has = x & 1u;
+    r.valid = (x >> 1) & 1u;
+    return r;
+}
+
+// block-wide exclusive "last source row" scan (warp shuffles, then one
+// shared-memory round over the warp totals); wsm holds 33 entries, the
+// block total is left in wsm[32]
+__device__ __forceinline__ FillCarry block_fill_scan_excl(const FillCarry& mine, FillCarry* wsm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const FillCarry zero { 0, 0, 0, 0 };
+    FillCarry inc = mine;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const FillCarry y = fill_shfl(inc, off, true);
+        if (lane >= off)
+            inc = fill_combine(y, inc);
+    }
+    __syncthreads(); // wsm may still be read by a previous call
+    if (lane == 31)
+        wsm[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        FillCarry z = lane < nw ? wsm[lane] : zero;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const FillCarry y = fill_shfl(z, off, true);
+            if (lane >= off)
+                z = fill_combine(y, z);
+        }
+        FillCarry ez = fill_shfl(z, 1, true);
+        if (lane == 0)
+            ez = zero;
+        __syncwarp();
+        if (lane < nw)
+            wsm[lane] = ez;
+        if (lane == nw - 1)
+            wsm[32] = z;
+    }
+    __syncthreads();
+    FillCarry ex = fill_shfl(inc, 1, true);
+    if (lane == 0)
+        ex = zero;
+    return fill_combine(wsm[warp], ex);
+}
+
+// Src: static FillCarry src(w0, w1, w2) -- has = row is a source
+//      static void apply(uint64_t& w0, uint64_t& w1, uint64_t& w2, const FillCarry& last)
+template <class F>
+__global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, const uint64_t* w1, const uint64_t* w2,
+                                                         FillCarry* tile_last)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_sum"));
+    __shared__ FillCarry sm[FL_THREADS / 32];
+    __shared__ int idx[FL_THREADS / 32];
+    const size_t base = (size_t)blockIdx.x * FL_TS;
+    FillCarry c { 0, 0, 0, 0 };
+    int last = -1;
+    for (int i = threadIdx.x; i < FL_TS; i += FL_THREADS) {
+        const size_t g = base + i;
+        VELO_TRACE_AT(TS_FILL, w0 + g);
+        const FillCarry d = F::src(w0[g], w1[g], w2[g]);
+        c = fill_combine(c, d);
+        last = d.has ? i : last;
+    }
+    // the source row with the largest index: warp shuffles, then warp 0
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const FillCarry oc = fill_shfl(c, off, false);
+        const int oi = __shfl_xor_sync(0xFFFFFFFFu, last, off);
+        const bool take = oi > last;
+        c = take ? oc : c;
+        last = take ? oi : last;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sm[threadIdx.x >> 5] = c;
+        idx[threadIdx.x >> 5] = last;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        FillCarry b = sm[0];
+        int bi = idx[0];
+        for (int w = 1; w < FL_THREADS / 32; w++) {
+            const bool take = idx[w] > bi;
+            b = take ? sm[w] : b;
+            bi = take ? idx[w] : bi;
+        }
+        VELO_TRACE_AT(TS_FILL, tile_last + blockIdx.x);
+        tile_last[blockIdx.x] = b;
+    }
+}
+
+// exclusive scan of the tile carries (one CTA of 1024 threads), defined in
+// ops.cu
+__global__ void k_fill_scan(const FillCarry* tile_last, int ntiles, FillCarry* carry);
+
+template <class F>
+__global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_t* w1, uint64_t* w2,
+                                                           const FillCarry* carry, unsigned long long* d_stat)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_apply"));
+    __shared__ FillCarry wsm[33];
+    __shared__ uint32_t tmp[33];
+    const size_t base = (size_t)blockIdx.x * FL_TS + (size_t)threadIdx.x * FL_RPT;
+    uint64_t a[FL_RPT], b[FL_RPT], c[FL_RPT];
+    FillCarry mine { 0, 0, 0, 0 };
+#pragma unroll
+    for (int r = 0; r < FL_RPT; r++) {
+        VELO_TRACE_AT(TS_FILL, w0 + base + r);
+        a[r] = w0[base + r];
+        b[r] = w1[base + r];
+        c[r] = w2[base + r];
+        mine = fill_combine(mine, F::src(a[r], b[r], c[r]));
+    }
+    FillCarry run = fill_combine(carry[blockIdx.x], block_fill_scan_excl(mine, wsm));
+    uint32_t stat = 0;
+#pragma unroll
+    for (int r = 0; r < FL_RPT; r++) {
+        stat += F::dup(a[r], b[r], c[r], run) ? 1u : 0u;
+        run = fill_combine(run, F::src(a[r], b[r], c[r]));
+        F::apply(a[r], b[r], c[r], run);
+        VELO_TRACE_AT(TS_FILL, w0 + base + r);
+        w0[base + r] = a[r];
+        w1[base + r] = b[r];
+        w2[base + r] = c[r];
+    }
+    // one counter update per CTA at a fixed address
+    uint32_t total;
+    block_exclusive_scan(stat, tmp, &total);
+    if (threadIdx.x == 0 && d_stat)
+        atomicAdd(d_stat, (unsigned long long)total);
+}
+
+template <class F>
+static velo_status run_fill(uint64_t* w0, uint64_t* w1, uint64_t* w2, size_t rows, FillCarry* tl, FillCarry* carry,
+                            unsigned long long* d_stat, cudaStream_t st)
+{
+    const int nt = (int)(rows / FL_TS);
+    k_fill_sum<F><<<nt, FL_THREADS, 0, st>>>(w0, w1, w2, tl);
+    k_fill_scan<<<1, 1024, 0, st>>>(tl, nt, carry);
+    k_fill_apply<F><<<nt, FL_THREADS, 0, st>>>(w0, w1, w2, carry, d_stat);
+    VELO_CUDA_TRY(cudaGetLastError(), "fill launch");
+    return VELO_OK;
+}
+
+using Rec3 = RowRec<3, 1, false>;
+using Rec3K2 = RowRec<3, 2, false>;
+constexpr int OP_LT = 12; // 4096-row tiles (CTA shape per record width: Tile12)
+constexpr int OP_LMAX = OP_LT - 5 < 8 ? OP_LT - 5 : 8;
+
+// scratch of the union-sort operators: 3 words x rows + fill carries + compaction
+inline size_t union_rows(size_t n)
+{
+    size_t r = next_pow2(n);
+    const size_t floor_rows = (size_t)1 << OP_LT;
+    return r < floor_rows ? floor_rows : r;
+}
+
+struct UnionScratch {
+    uint64_t* w[3];
+    FillCarry* tl;
+    FillCarry* carry;
+    uint32_t* counts;
+    uint32_t* prefix;
+    uint64_t* n_marked;
+    unsigned long long* stat;
+    size_t bytes;
+};
+
+inline UnionScratch union_layout(char* base, size_t rows)
+{
+    UnionScratch s {};
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        char* p = base ? base + off : nullptr;
+        off += align_up(b, 256);
+        return p;
+    };
+    for (int i = 0; i < 3; i++)
+        s.w[i] = reinterpret_cast<uint64_t*>(take(rows * 8));
+    const size_t nft = rows / FL_TS, nct = rows >> OP_LT;
+    s.tl = reinterpret_cast<FillCarry*>(take(nft * sizeof(FillCarry)));
+    s.carry = reinterpret_cast<FillCarry*>(take(nft * sizeof(FillCarry)));
+    s.counts = reinterpret_cast<uint32_t*>(take(nct * 4));
+    s.prefix = reinterpret_cast<uint32_t*>(take((nct + 1) * 4));
+    s.n_marked = reinterpret_cast<uint64_t*>(take(8));
+    s.stat = reinterpret_cast<unsigned long long*>(take(8));
+    s.bytes = off;
+    return s;
+}
+
+} // namespace velo
