@@ -943,6 +943,44 @@ def batch_plain(torch, wl, args):
             "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in wl.tune_ms.items()}}
 
 
+def measure_join_algorithms(torch, capi, W, steps):
+    """The three oblivious equi-joins on the 1.5 M-row dimension keys and the
+    6 M-row fact foreign keys (join only, no group-by): the union-sort PK-FK
+    join, the bin-padded hash join and the many-to-many sort-merge join
+    (bound 6 M pairs).  Each is timed with CUDA events over `steps` calls and
+    its pair set checked against numpy."""
+    dim, fact = W.join_tables()
+    bk = torch.from_numpy(dim["key"]).cuda()
+    pk = torch.from_numpy(fact["fk"]).cuda()
+    n = len(dim["key"]) + len(fact["fk"])
+    keyset = np.zeros(len(dim["key"]) + 2, np.int64) - 1
+    keyset[dim["key"]] = np.arange(len(dim["key"]))
+    want = int((keyset[fact["fk"]] >= 0).sum())
+    out = {}
+    algos = {"pkfk_union_sort": lambda: capi.ojoin_pkfk(bk, None, pk, None, 4),
+             "hash_bin_padded": lambda: capi.ohash_join(bk, None, pk, None, 4),
+             "many_to_many_sort_merge": lambda: capi.ojoin_mn(bk, None, pk, None, 4, len(fact["fk"]))}
+    for name, fn in algos.items():
+        try:
+            for _ in range(2):
+                fn()
+            torch.cuda.synchronize()
+            ts = time_steps(torch, fn, max(3, steps // 2))
+            ob, op, cnt = fn()
+            torch.cuda.synchronize()
+            m = int(cnt[0].item())
+            o_b, o_p = ob.cpu().numpy()[:m], op.cpu().numpy()[:m]
+            ok = m == want and bool(np.array_equal(keyset[fact["fk"][o_p]], o_b))
+            ms = float(np.mean(ts))
+            out[name] = {"ms": ms, "input_mrows_per_s": n / (ms / 1e3) / 1e6, "pairs": m, "checked": ok}
+        except Exception as e:  # noqa: BLE001
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+    out["note"] = ("times include each call's scratch allocation by the caching allocator (no cudaMalloc after "
+                   "the first call)")
+    return out
+
+
 def run_extras(torch, capi, W, device, args, peak, peak_kind, orc):
     """The other configurations, each measured and checked on its own (N = 1
     only).  A failure is recorded in its key instead of ending the run."""
@@ -979,6 +1017,10 @@ def run_extras(torch, capi, W, device, args, peak, peak_kind, orc):
         except Exception as e:  # noqa: BLE001
             out["batched"] = {"error": f"{type(e).__name__}: {e}"}
         torch.cuda.empty_cache()
+    try:
+        out["joins_1.5Mx6M"] = measure_join_algorithms(torch, capi, W, args.steps)
+    except Exception as e:  # noqa: BLE001
+        out["joins_1.5Mx6M"] = {"error": f"{type(e).__name__}: {e}"}
     try:
         out["served"] = measure_serve(torch)
     except Exception as e:  # noqa: BLE001

@@ -356,6 +356,26 @@ velo_status velo_ojoin_mn(const void* d_build_keys, const uint8_t* d_build_mask,
                           size_t max_pairs, int64_t* d_out_build_rowid, int64_t* d_out_probe_rowid,
                           uint64_t* d_counts, void* d_scratch, size_t scratch_bytes, void* stream);
 
+/* Oblivious bin-padded hash join, the HashJoinOperator's algorithm
+ * (replaces the chained hash table of include/cuda/hash_join.cuh:28-254 and
+ * src/operator/hash_join_operator.cpp:88-393): both sides are hashed into
+ * bins by a keyed Philox4x32-10 hash (hash_seed) and every bin is padded to a
+ * public capacity derived from build_n and probe_n, so bin occupancy never
+ * shows; each bin compares every probe slot with every build slot.  For a
+ * build side with unique keys (the PK-FK case) rows [0, pairs) of the outputs
+ * (probe_n rows) hold (build row id, probe row id) pairs in (bin, probe row
+ * id) order, the rest -1.  Rows with mask == 0 (NULL = all valid) do not join.
+ * d_counts: 3 u64 = (pairs, probe rows with more than one partner -- a
+ * repeated build key --, real rows that did not fit their bin).  When either
+ * of the last two is nonzero the pairs are incomplete: join with
+ * velo_ojoin_mn instead (HashJoinOperator does).  key_type: VELO_INTEGER or
+ * VELO_BIGINT.  d_scratch: velo_ohash_join_scratch_bytes() bytes. */
+size_t velo_ohash_join_scratch_bytes(size_t build_n, size_t probe_n);
+velo_status velo_ohash_join(const void* d_build_keys, const uint8_t* d_build_mask, size_t build_n,
+                            const void* d_probe_keys, const uint8_t* d_probe_mask, size_t probe_n, uint32_t key_type,
+                            uint64_t hash_seed, int64_t* d_out_build_rowid, int64_t* d_out_probe_rowid,
+                            uint64_t* d_counts, void* d_scratch, size_t scratch_bytes, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Batched form: one persistent launch for many independent commands        */
 /* ------------------------------------------------------------------------ */
@@ -514,7 +534,9 @@ typedef enum velo_opcode {
     VELO_OP_OGATHER = 0x104,
     VELO_OP_OSHUFFLE = 0x105,
     VELO_OP_FILTER_GROUPBY = 0x106,
-    VELO_OP_JOIN_GROUPBY_TOPK = 0x107
+    VELO_OP_JOIN_GROUPBY_TOPK = 0x107,
+    VELO_OP_OJOIN_MN = 0x108,
+    VELO_OP_OHASH_JOIN = 0x109
 } velo_opcode;
 
 /* A command: device pointers and public sizes only (the same arguments as
@@ -541,6 +563,14 @@ typedef struct velo_cmd {
         struct { const void* d_build_keys; const uint8_t* d_build_mask; size_t build_n; const void* d_probe_keys;
                  const uint8_t* d_probe_mask; size_t probe_n; uint32_t key_type; int64_t* d_out_build_rowid;
                  int64_t* d_out_probe_rowid; uint64_t* d_counts; void* d_scratch; size_t scratch_bytes; } ojoin;
+        struct { const void* d_build_keys; const uint8_t* d_build_mask; size_t build_n; const void* d_probe_keys;
+                 const uint8_t* d_probe_mask; size_t probe_n; uint32_t key_type; size_t max_pairs;
+                 int64_t* d_out_build_rowid; int64_t* d_out_probe_rowid; uint64_t* d_counts; void* d_scratch;
+                 size_t scratch_bytes; } ojoin_mn;
+        struct { const void* d_build_keys; const uint8_t* d_build_mask; size_t build_n; const void* d_probe_keys;
+                 const uint8_t* d_probe_mask; size_t probe_n; uint32_t key_type; uint64_t hash_seed;
+                 int64_t* d_out_build_rowid; int64_t* d_out_probe_rowid; uint64_t* d_counts; void* d_scratch;
+                 size_t scratch_bytes; } ohash;
         struct { const uint64_t* d_table; size_t table_n; const uint32_t* d_rids; size_t n_req; uint64_t* d_out;
                  void* d_scratch; size_t scratch_bytes; } ogather;
         struct { uint32_t* d_map; size_t n; uint64_t key; uint64_t counter; void* d_scratch; size_t scratch_bytes; }

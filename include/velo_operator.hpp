@@ -283,9 +283,12 @@ private:
 
 enum class JoinType { INNER, LEFT, RIGHT, FULL, CROSS };
 
-// Inner PK-FK equi-join: the left input is the key (build) side.  The output
-// holds the left columns then the right columns, one row per matching pair,
-// in key order.  A left side with repeated keys is rejected (failure).
+// Inner equi-join, the reference's sort-merge join: the left input is the
+// build side.  The output holds the left columns then the right columns, one
+// row per matching pair, in key order.  A left side with unique keys takes
+// the oblivious PK-FK join (velo_ojoin_pkfk); repeated left keys take the
+// oblivious many-to-many join (velo_ojoin_mn), which writes every pair, as
+// the reference's cross product of equal-key runs does.
 class SortMergeJoinOperator : public BinaryOperator {
 public:
     SortMergeJoinOperator(ExecutionContext& context, Schema output_schema, std::unique_ptr<AbstractOperator> left,
@@ -294,16 +297,21 @@ public:
     Result<RowBatch> next() override;
 
 protected:
-    // mask column indices of the build and probe inputs (-1: none)
-    Result<RowBatch> join(std::pair<long, long> mask_indices);
+    // mask column indices of the build and probe inputs (-1: none); hashed
+    // selects the bin-padded hash join, else the union-sort PK-FK join; both
+    // hand a build side with repeated keys to the many-to-many join
+    Result<RowBatch> join(std::pair<long, long> mask_indices, bool hashed);
     std::pair<size_t, size_t> join_key_indices_;
     JoinType join_type_;
     bool joined_ = false;
+    uint64_t hash_seed_ = 0;
 };
 
-// Same join with the reference's build/probe mask columns: rows whose mask
-// is zero do not join.  The reference builds a chained hash table; here the
-// join is the same oblivious union sort.
+// The join with the reference's build/probe mask columns (rows whose mask is
+// zero do not join), by the oblivious bin-padded hash join
+// (velo_ohash_join): both sides hashed into padded bins by a per-operator
+// keyed hash, every probe slot compared with every build slot of its bin.
+// The reference builds a chained hash table (hash_join_operator.cpp:88-393).
 class HashJoinOperator : public SortMergeJoinOperator {
 public:
     HashJoinOperator(ExecutionContext& context, Schema output_schema, std::unique_ptr<AbstractOperator> left,

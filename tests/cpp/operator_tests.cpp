@@ -438,7 +438,8 @@ static void run_join_test(ExecutionContext& ctx, bool hash, size_t nd, size_t nf
     for (size_t i = 0; i < gk.size(); i++) {
         EXPECT(gk[i] == gfk[i]);
         EXPECT(gdate[i] == j.ddate[dim_of[gk[i]]]);
-        if (i)
+        // the sort-merge join emits key order; the hash join bin order
+        if (i && !hash)
             EXPECT(gk[i - 1] <= gk[i]);
         got.insert({ gfk[i], gp[i] });
     }
@@ -458,20 +459,62 @@ static void test_hash_join_with_masks(ExecutionContext& ctx)
     run_join_test(ctx, true, 20000, 70001, 5);
 }
 
-static void test_join_rejects_repeated_build_keys(ExecutionContext& ctx)
+// repeated build keys: every pair, as the reference's sort-merge join writes
+// the cross product of each run of equal keys
+static void run_many_to_many(ExecutionContext& ctx, bool hash)
 {
-    Schema s = schema_of({ { "k", VELO_INTEGER } });
+    Schema s = schema_of({ { "k", VELO_INTEGER }, { "v", VELO_BIGINT } });
+    std::vector<int32_t> lk, rk;
+    std::vector<int64_t> lv, rv;
+    std::mt19937_64 rng(hash ? 11 : 12);
+    for (int i = 0; i < 3000; i++) {
+        lk.push_back((int32_t)(rng() % 400));
+        lv.push_back(i);
+    }
+    for (int i = 0; i < 5000; i++) {
+        rk.push_back((int32_t)(rng() % 400));
+        rv.push_back(100000 + i);
+    }
     RowBatch lb, rb;
-    lb.addColumn(Column::fromHost(ctx, VELO_INTEGER, std::vector<int32_t> { 1, 2, 2 }));
-    rb.addColumn(Column::fromHost(ctx, VELO_INTEGER, std::vector<int32_t> { 2, 1 }));
+    lb.addColumn(Column::fromHost(ctx, VELO_INTEGER, lk));
+    lb.addColumn(Column::fromHost(ctx, VELO_BIGINT, lv));
+    rb.addColumn(Column::fromHost(ctx, VELO_INTEGER, rk));
+    rb.addColumn(Column::fromHost(ctx, VELO_BIGINT, rv));
     std::vector<RowBatch> li, ri;
     li.push_back(std::move(lb));
     ri.push_back(std::move(rb));
-    SortMergeJoinOperator op(ctx, schema_of({ { "l.k", VELO_INTEGER }, { "r.k", VELO_INTEGER } }),
-                             std::make_unique<BatchSource>(ctx, s, std::move(li)),
-                             std::make_unique<BatchSource>(ctx, s, std::move(ri)), { 0, 0 });
-    auto r = op.next();
-    EXPECT(!r);
+    Schema os = schema_of({ { "l.k", VELO_INTEGER }, { "l.v", VELO_BIGINT }, { "r.k", VELO_INTEGER },
+                            { "r.v", VELO_BIGINT } });
+    std::unique_ptr<AbstractOperator> op;
+    auto L = std::make_unique<BatchSource>(ctx, s, std::move(li));
+    auto R = std::make_unique<BatchSource>(ctx, s, std::move(ri));
+    if (hash)
+        op = std::make_unique<HashJoinOperator>(ctx, os, std::move(L), std::move(R), std::make_pair(0ul, 0ul),
+                                                std::make_pair(-1l, -1l));
+    else
+        op = std::make_unique<SortMergeJoinOperator>(ctx, os, std::move(L), std::move(R), std::make_pair(0ul, 0ul));
+    auto out = drain(*op);
+    std::multiset<std::pair<int64_t, int64_t>> expect, got;
+    for (size_t a = 0; a < lk.size(); a++)
+        for (size_t b = 0; b < rk.size(); b++)
+            if (lk[a] == rk[b])
+                expect.insert({ lv[a], rv[b] });
+    auto gl = col_host<int64_t>(ctx, out, 1);
+    auto gr = col_host<int64_t>(ctx, out, 3);
+    auto gkl = col_host<int32_t>(ctx, out, 0);
+    auto gkr = col_host<int32_t>(ctx, out, 2);
+    EXPECT(gl.size() == expect.size());
+    for (size_t i = 0; i < gl.size(); i++) {
+        EXPECT(gkl[i] == gkr[i]);
+        got.insert({ gl[i], gr[i] });
+    }
+    EXPECT(got == expect);
+}
+
+static void test_join_many_to_many(ExecutionContext& ctx)
+{
+    run_many_to_many(ctx, false);
+    run_many_to_many(ctx, true);
 }
 
 static void test_join_empty_side(ExecutionContext& ctx)
@@ -702,7 +745,7 @@ int main(int argc, char** argv)
         { "filter_propagates_child_failure", test_filter_propagates_child_failure },
         { "sort_merge_join_cardinality", test_sort_merge_join_cardinality },
         { "hash_join_with_masks", test_hash_join_with_masks },
-        { "join_rejects_repeated_build_keys", test_join_rejects_repeated_build_keys },
+        { "join_many_to_many", test_join_many_to_many },
         { "join_empty_side", test_join_empty_side },
         { "materialization", test_materialization },
         { "limit_offset", test_limit_offset },

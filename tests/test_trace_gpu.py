@@ -384,3 +384,27 @@ def test_mn_join_trace_is_data_independent(T):
     # matching at all, every build row left out
     assert_same_trace([trace_of(T, join(x, sp, am)) for x, sp, am in
                        ((1, 3000, False), (2, 3000, False), (3, 1, False), (4, 10**9, False), (5, 3000, True))])
+
+
+def test_hash_join_trace_is_data_independent(T):
+    bn, pn = 5_000, 20_000
+    bk = torch.empty(bn, dtype=torch.int64, device="cuda")
+    pk = torch.empty(pn, dtype=torch.int64, device="cuda")
+    ob = torch.empty(pn, dtype=torch.int64, device="cuda")
+    op = torch.empty(pn, dtype=torch.int64, device="cuda")
+    jc = torch.empty(3, dtype=torch.int64, device="cuda")
+    sb = T.velo_ohash_join_scratch_bytes(bn, pn)
+    s = torch.empty(sb, dtype=torch.uint8, device="cuda")
+
+    def join(seed, miss):
+        def f():
+            rng = np.random.default_rng(seed)
+            dev_copy(bk, rng.permutation(bn).astype(np.int64))
+            fk = rng.integers(bn, 2 * bn, pn) if miss else rng.integers(0, bn, pn)
+            dev_copy(pk, fk.astype(np.int64))
+            torch.cuda.synchronize()
+            assert T.velo_ohash_join(bk.data_ptr(), None, bn, pk.data_ptr(), None, pn, 5, 99, ob.data_ptr(),
+                                     op.data_ptr(), jc.data_ptr(), s.data_ptr(), sb, None) == 0
+        return f
+
+    assert_same_trace([trace_of(T, join(x, mm)) for x, mm in ((6, False), (7, False), (8, True))])

@@ -61,6 +61,8 @@ PROTOS = {
     "velo_ojoin_pkfk": (i32, [vp, vp, sz, vp, vp, sz, u32, vp, vp, vp, vp, sz, vp]),
     "velo_ojoin_mn_scratch_bytes": (sz, [sz, sz, sz]),
     "velo_ojoin_mn": (i32, [vp, vp, sz, vp, vp, sz, u32, sz, vp, vp, vp, vp, sz, vp]),
+    "velo_ohash_join_scratch_bytes": (sz, [sz, sz]),
+    "velo_ohash_join": (i32, [vp, vp, sz, vp, vp, sz, u32, u64, vp, vp, vp, vp, sz, vp]),
     "velo_init": (i32, [vp, vp]),
     "velo_shutdown": (i32, [vp, u32]),
     "velo_submit": (i32, [vp, vp, vp]),
@@ -168,6 +170,8 @@ class VeloCmdArgs(C.Union):
         ("ocompact_kpm", _args(vp, vp, vp, sz, sz, vp, vp, sz)),
         ("ogather", _args(vp, sz, vp, sz, vp, vp, sz)),
         ("ojoin", _args(vp, vp, sz, vp, vp, sz, u32, vp, vp, vp, vp, sz)),
+        ("ojoin_mn", _args(vp, vp, sz, vp, vp, sz, u32, sz, vp, vp, vp, vp, sz)),
+        ("ohash", _args(vp, vp, sz, vp, vp, sz, u32, u64, vp, vp, vp, vp, sz)),
     ]
 
 
@@ -181,7 +185,7 @@ class VeloConfig(C.Structure):
 
 OP = dict(NOP=0, SCATTER=1, GATHER=2, SORT=3, PERMUTE=4, COMPARE_EQ=10, COMPOSE_POSITION_MAP=11, ENRICH_POSITIONS=12,
           OSORT_KP=0x100, OCOMPACT_KPM=0x101, OSORT_RECORDS=0x102, OJOIN_PKFK=0x103, OGATHER=0x104, OSHUFFLE=0x105,
-          FILTER_GROUPBY=0x106, JOIN_GROUPBY_TOPK=0x107)
+          FILTER_GROUPBY=0x106, JOIN_GROUPBY_TOPK=0x107, OJOIN_MN=0x108, OHASH_JOIN=0x109)
 
 
 class VeloServedTables(C.Structure):

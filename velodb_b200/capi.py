@@ -377,6 +377,22 @@ def ojoin_mn(build_keys, build_mask, probe_keys, probe_mask, key_type, max_pairs
     return ob, op, cnt
 
 
+def ohash_join(build_keys, build_mask, probe_keys, probe_mask, key_type, hash_seed=0x5EED, stream=None):
+    """Oblivious bin-padded hash join (velo_ohash_join).  Returns (build
+    rowids, probe rowids, counts[3] = (pairs, repeated build keys, overflowed
+    rows)) device tensors of probe_n rows."""
+    bn, pn = build_keys.numel(), probe_keys.numel()
+    dev = build_keys.device
+    ob = torch.empty(max(pn, 1), dtype=torch.int64, device=dev)
+    op = torch.empty(max(pn, 1), dtype=torch.int64, device=dev)
+    cnt = torch.zeros(3, dtype=torch.int64, device=dev)
+    sc = _scratch(lib().velo_ohash_join_scratch_bytes(bn, pn), dev)
+    check(lib().velo_ohash_join(build_keys.data_ptr(), _ptr(build_mask), bn, probe_keys.data_ptr(),
+                                _ptr(probe_mask), pn, key_type, hash_seed, ob.data_ptr(), op.data_ptr(),
+                                cnt.data_ptr(), sc.data_ptr(), sc.numel(), _stream(stream)), "velo_ohash_join")
+    return ob, op, cnt
+
+
 def ogroupby(keys: torch.Tensor, key_type: int, n: int, sums=(), with_count: bool = True, mask=None,
              group_bound: int | None = None, stream=None):
     """Oblivious GROUP BY key with SUM/COUNT (velo_ogroupby).  keys: int32

@@ -33,10 +33,34 @@
 // id, build row id) order; the rest hold -1.  Every launch, address and
 // branch depends only on build_n, probe_n and max_pairs.
 #include <algorithm>
+#include <cmath>
 
 #include "union.cuh"
 
 namespace velo {
+
+// exclusive scan of run summaries of tiles: one CTA of 1024 threads, rounds of
+// 1024 consecutive tiles chained through the running total
+__global__ void __launch_bounds__(1024) k_run_scan(const RunSum* tiles, int ntiles, RunSum* carry)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_run_scan"));
+    __shared__ RunSum sm[1024];
+    RunSum run {};
+    for (int base = 0; base < ntiles; base += blockDim.x) {
+        const int t = base + (int)threadIdx.x;
+        RunSum x {};
+        if (t < ntiles) {
+            VELO_TRACE_AT(TS_FILL, tiles + t);
+            x = tiles[t];
+        }
+        RunSum total;
+        const RunSum ex = run_block_scan_excl(x, sm, &total);
+        if (t < ntiles)
+            carry[t] = run_combine(run, ex);
+        run = run_combine(run, total);
+    }
+}
+
 
 constexpr uint64_t MN_OUT = 1ull << 63, MN_TAG = 1ull << 62, MN_VB = 1ull << 61;
 constexpr uint64_t MN_ROWID = 0xFFFFFFFFull;
@@ -71,100 +95,22 @@ __global__ void k_mn_pack(const void* bk, const uint8_t* bm, size_t bn, const vo
 
 // ---- scan 1: segmented count of valid build rows over key runs ---------------
 
-// summary of a range of rows: first/last key, valid build rows in it, valid
-// build rows in its trailing key run, whether it is one key run
-struct MnSum {
-    uint64_t first_key, last_key;
-    uint64_t nb, tail_nb;
-    uint32_t uniform, has;
-};
-
-// a then b (a the earlier range); associative
-__device__ __forceinline__ MnSum mn_combine(const MnSum& a, const MnSum& b)
-{
-    if (!a.has)
-        return b;
-    if (!b.has)
-        return a;
-    const bool join = a.last_key == b.first_key;
-    MnSum r;
-    r.first_key = a.first_key;
-    r.last_key = b.last_key;
-    r.nb = a.nb + b.nb;
-    r.tail_nb = b.tail_nb + ((b.uniform && join) ? a.tail_nb : 0ull);
-    r.uniform = (a.uniform && b.uniform && join) ? 1u : 0u;
-    r.has = 1u;
-    return r;
-}
-
-__device__ __forceinline__ MnSum mn_row(uint64_t key, uint64_t w1)
-{
-    const uint64_t vb = mn_valid_build(w1) ? 1ull : 0ull;
-    return MnSum { key, key, vb, vb, 1u, 1u };
-}
-
-// block-wide exclusive scan of MnSum (shared-memory Hillis-Steele over the
-// threads' summaries); the block total is returned in *total
-__device__ MnSum mn_block_scan_excl(const MnSum& mine, MnSum* sm, MnSum* total)
-{
-    const int t = threadIdx.x, n = blockDim.x;
-    MnSum x = mine;
-    for (int off = 1; off < n; off <<= 1) {
-        __syncthreads();
-        sm[t] = x;
-        __syncthreads();
-        if (t >= off)
-            x = mn_combine(sm[t - off], x);
-    }
-    __syncthreads();
-    sm[t] = x;
-    __syncthreads();
-    *total = sm[n - 1];
-    MnSum ex {};
-    if (t > 0)
-        ex = sm[t - 1];
-    __syncthreads();
-    return ex;
-}
-
-__global__ void __launch_bounds__(MN_THREADS) k_mn_sum1(const uint64_t* w0, const uint64_t* w1, MnSum* tiles)
+__global__ void __launch_bounds__(MN_THREADS) k_mn_sum1(const uint64_t* w0, const uint64_t* w1, RunSum* tiles)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_mn_sum1"));
-    __shared__ MnSum sm[MN_THREADS];
+    __shared__ RunSum sm[MN_THREADS];
     const size_t base = (size_t)blockIdx.x * MN_TS + (size_t)threadIdx.x * MN_RPT;
-    MnSum s {};
+    RunSum s {};
 #pragma unroll
     for (int r = 0; r < MN_RPT; r++) {
         VELO_TRACE_AT(TS_FILL, w0 + base + r);
-        s = mn_combine(s, mn_row(w0[base + r], w1[base + r]));
+        s = run_combine(s, run_row(w0[base + r], mn_valid_build(w1[base + r]) ? 1ull : 0ull));
     }
-    MnSum total;
-    mn_block_scan_excl(s, sm, &total);
+    RunSum total;
+    run_block_scan_excl(s, sm, &total);
     if (threadIdx.x == 0) {
         VELO_TRACE_AT(TS_FILL, tiles + blockIdx.x);
         tiles[blockIdx.x] = total;
-    }
-}
-
-// exclusive scan of the tile summaries: one CTA of 1024 threads, rounds of
-// 1024 consecutive tiles chained through the running total
-__global__ void __launch_bounds__(1024) k_mn_scan1(const MnSum* tiles, int ntiles, MnSum* carry)
-{
-    VELO_TRACE_KERNEL(velo_site_hash("k_mn_scan1"));
-    __shared__ MnSum sm[1024];
-    MnSum run {};
-    for (int base = 0; base < ntiles; base += blockDim.x) {
-        const int t = base + (int)threadIdx.x;
-        MnSum x {};
-        if (t < ntiles) {
-            VELO_TRACE_AT(TS_FILL, tiles + t);
-            x = tiles[t];
-        }
-        MnSum total;
-        const MnSum ex = mn_block_scan_excl(x, sm, &total);
-        if (t < ntiles)
-            carry[t] = mn_combine(run, ex);
-        run = mn_combine(run, total);
     }
 }
 
@@ -173,23 +119,23 @@ __global__ void __launch_bounds__(1024) k_mn_scan1(const MnSum* tiles, int ntile
 // over valid probe rows replaces w0 (the key is no longer needed); the tile's
 // total of c goes to csum.
 __global__ void __launch_bounds__(MN_THREADS) k_mn_apply1(uint64_t* w0, uint64_t* w1, uint64_t* w2,
-                                                          const MnSum* carry, uint64_t* csum)
+                                                          const RunSum* carry, uint64_t* csum)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_mn_apply1"));
-    __shared__ MnSum sm[MN_THREADS];
+    __shared__ RunSum sm[MN_THREADS];
     __shared__ uint64_t s64[MN_THREADS];
     const size_t base = (size_t)blockIdx.x * MN_TS + (size_t)threadIdx.x * MN_RPT;
     uint64_t k[MN_RPT], b[MN_RPT];
-    MnSum s {};
+    RunSum s {};
 #pragma unroll
     for (int r = 0; r < MN_RPT; r++) {
         VELO_TRACE_AT(TS_FILL, w0 + base + r);
         k[r] = w0[base + r];
         b[r] = w1[base + r];
-        s = mn_combine(s, mn_row(k[r], b[r]));
+        s = run_combine(s, run_row(k[r], mn_valid_build(b[r]) ? 1ull : 0ull));
     }
-    MnSum total;
-    MnSum run = mn_combine(carry[blockIdx.x], mn_block_scan_excl(s, sm, &total));
+    RunSum total;
+    RunSum run = run_combine(carry[blockIdx.x], run_block_scan_excl(s, sm, &total));
     uint64_t cs[MN_RPT], c_thread = 0;
 #pragma unroll
     for (int r = 0; r < MN_RPT; r++) {
@@ -201,7 +147,7 @@ __global__ void __launch_bounds__(MN_THREADS) k_mn_apply1(uint64_t* w0, uint64_t
         cs[r] = probe ? c : 0ull;
         c_thread += cs[r];
         w2[base + r] = probe ? (((P - c) << 32) | c) : 0ull;
-        run = mn_combine(run, mn_row(k[r], b[r]));
+        run = run_combine(run, run_row(k[r], mn_valid_build(b[r]) ? 1ull : 0ull));
     }
     // tile-local exclusive prefix of c over the threads (then within each)
     uint64_t x = c_thread;
@@ -366,8 +312,8 @@ struct MnScratch {
     UnionScratch u;    // sorted union
     UnionScratch e;    // expansion (its area is reused by the gather)
     size_t e_off, e_bytes;
-    MnSum* tiles;
-    MnSum* carry;
+    RunSum* tiles;
+    RunSum* carry;
     uint64_t* csum;
     uint64_t* cbase;
     uint64_t* pairs;
@@ -400,8 +346,8 @@ static MnScratch mn_layout(char* base, size_t build_n, size_t probe_n, size_t ma
     s.e_bytes = eb;
     s.e = union_layout(static_cast<char*>(take(eb)), s.E);
     const size_t nt = s.U / MN_TS;
-    s.tiles = reinterpret_cast<MnSum*>(take(nt * sizeof(MnSum)));
-    s.carry = reinterpret_cast<MnSum*>(take(nt * sizeof(MnSum)));
+    s.tiles = reinterpret_cast<RunSum*>(take(nt * sizeof(RunSum)));
+    s.carry = reinterpret_cast<RunSum*>(take(nt * sizeof(RunSum)));
     s.csum = reinterpret_cast<uint64_t*>(take(nt * 8));
     s.cbase = reinterpret_cast<uint64_t*>(take(nt * 8));
     s.pairs = reinterpret_cast<uint64_t*>(take(8));
@@ -490,7 +436,7 @@ extern "C" velo_status velo_ojoin_mn(const void* d_build_keys, const uint8_t* d_
     // 3-4. the two scans
     const int nt = (int)(U / MN_TS);
     k_mn_sum1<<<nt, MN_THREADS, 0, st>>>(w[0], w[1], s.tiles);
-    k_mn_scan1<<<1, 1024, 0, st>>>(s.tiles, nt, s.carry);
+    k_run_scan<<<1, 1024, 0, st>>>(s.tiles, nt, s.carry);
     k_mn_apply1<<<nt, MN_THREADS, 0, st>>>(w[0], w[1], w[2], s.carry, s.csum);
     k_mn_scan2<<<1, 1024, 0, st>>>(s.csum, nt, s.cbase, s.pairs);
     VELO_CUDA_TRY(cudaGetLastError(), "ojoin_mn scan launch");
@@ -545,5 +491,421 @@ extern "C" velo_status velo_ojoin_mn(const void* d_build_keys, const uint8_t* d_
     k_mn_out<<<mn_grid(max_pairs), 256, 0, st>>>(s.gathered, d_out_probe_rowid, max_pairs, d_out_build_rowid, s.pairs,
                                                  d_counts);
     VELO_CUDA_TRY(cudaGetLastError(), "ojoin_mn out launch");
+    return VELO_OK;
+}
+
+// ===========================================================================
+// Oblivious bin-padded hash join (velo_ohash_join)
+//
+// The reference's hash join (include/cuda/hash_join.cuh:28-254,
+// src/operator/hash_join_operator.cpp:88-393) chains build rows into a hash
+// table and walks the chains for every probe row; its addresses follow the
+// keys.  Here both sides are hashed into B bins by a keyed Philox4x32-10 hash
+// and every bin is padded to a public capacity (C_b build slots, C_p probe
+// slots, set from the public sizes), so a bin's occupancy never shows:
+//
+//   1. union   R = next_pow2(build_n + probe_n + B (C_b + C_p)) records
+//              w0 = [63] not kept | bin << 33 | side << 32 | dummy << 31
+//                   | row id (dummy: slot index), w1 = key; rows left out
+//              by their mask take bin B (no bin); every bin also gets C_b
+//              build dummies and C_p probe dummies
+//   2. sort    bitonic network on w0: each (bin, side) group holds its real
+//              rows in row id order, then its dummies
+//   3. rank    a run-count scan gives each row its rank in its group; the
+//              first C rows of every group are kept (real rows first), real
+//              rows past the capacity are counted as overflow
+//   4. place   ORCompact of the kept rows: slot b (C_b + C_p) + i is bin b's
+//              i-th build slot, then its probe slots
+//   5. bins    one CTA per bin holds the C_b build slots in shared memory and
+//              compares every probe slot with every build slot, reading the
+//              build slots in the same order for every bin (a broadcast
+//              read, no data-dependent address); a probe slot with two or
+//              more partners counts a repeated build key
+//   6. output  ORCompact of the joined probe slots; the first `pairs` rows
+//              are (build row id, probe row id) in (bin, probe row id) order,
+//              the rest up to probe_n are -1
+//
+// Every launch, address and branch depends only on build_n, probe_n and the
+// hash seed.  Overflow (a bin holding more rows than its capacity) and a
+// repeated build key are reported in d_counts; the caller then joins with the
+// sort-merge join (velo_ojoin_mn), which has no such limit.
+// ===========================================================================
+
+namespace velo {
+
+constexpr uint64_t HJ_DROP = 1ull << 63, HJ_SIDE = 1ull << 32, HJ_DUMMY = 1ull << 31;
+constexpr uint64_t HJ_ID = (1ull << 31) - 1;
+constexpr int HJ_THREADS = 512;
+
+struct HjGeom {
+    uint32_t B, log_b, cb, cp; // bins, log2 bins, build / probe slots per bin
+    size_t rows;               // padded union rows
+    size_t slots;              // B (cb + cp)
+    size_t probe_slots;        // B cp
+    size_t out_rows;           // padded probe slot records (>= B cp)
+};
+
+static uint32_t hj_cap(size_t mean, double sigmas)
+{
+    const double c = (double)mean + sigmas * std::sqrt((double)mean) + 16.0;
+    return (uint32_t)((((uint64_t)std::ceil(c)) + 31) / 32 * 32);
+}
+
+// mean build rows per bin in [1024, 2048) (a single bin below); the build
+// capacity allows 8 standard deviations of a Poisson count, the probe side
+// 16, because foreign keys repeat and their bin counts spread wider
+static HjGeom hj_geometry(size_t build_n, size_t probe_n)
+{
+    HjGeom g {};
+    uint32_t B = 1, lb = 0;
+    while ((size_t)B * 2 * 1024 <= build_n && lb < 20) {
+        B *= 2;
+        lb++;
+    }
+    g.B = B;
+    g.log_b = lb;
+    g.cb = hj_cap((build_n + B - 1) / B, 8.0);
+    g.cp = hj_cap((probe_n + B - 1) / B, 16.0);
+    g.slots = (size_t)B * (g.cb + g.cp);
+    g.probe_slots = (size_t)B * g.cp;
+    g.rows = union_rows(build_n + probe_n + g.slots);
+    g.out_rows = union_rows(g.probe_slots);
+    return g;
+}
+
+__device__ __forceinline__ uint64_t hj_key(const void* keys, size_t j, int key64)
+{
+    return key64 ? ((uint64_t) static_cast<const int64_t*>(keys)[j] ^ 0x8000000000000000ull)
+                 : (uint64_t)((uint32_t) static_cast<const int32_t*>(keys)[j] ^ 0x80000000u);
+}
+
+__global__ void k_hj_pack(const void* bk, const uint8_t* bm, size_t bn, const void* pk, const uint8_t* pm, size_t pn,
+                          int key64, HjGeom g, uint64_t seed, uint64_t* w0, uint64_t* w1)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_hj_pack"));
+    const size_t real = bn + pn, bdum = (size_t)g.B * g.cb;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, g.rows);
+         i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t a = ~0ull, b = ~0ull;
+        if (i < real) {
+            const bool build = i < bn;
+            const size_t j = build ? i : i - bn;
+            const uint64_t key = hj_key(build ? bk : pk, j, key64);
+            const uint8_t* mask = build ? bm : pm;
+            const bool valid = mask == nullptr || mask[j] != 0;
+            const uint64_t bin = valid ? (philox_u64(key, 0x4A4F494Eull, seed) & (g.B - 1ull)) : (uint64_t)g.B;
+            a = (bin << 33) | (build ? 0ull : HJ_SIDE) | (uint64_t)j;
+            b = key;
+        } else if (i < real + g.slots) {
+            const size_t d = i - real;
+            const bool build = d < bdum;
+            const size_t e = build ? d : d - bdum;
+            const uint32_t cap = build ? g.cb : g.cp;
+            const uint64_t bin = e / cap, slot = e - bin * cap;
+            a = (bin << 33) | (build ? 0ull : HJ_SIDE) | HJ_DUMMY | slot;
+            b = 0;
+        }
+        VELO_TRACE_AT(TS_ROW_STORE, w0 + i);
+        w0[i] = a;
+        w1[i] = b;
+    }
+}
+
+// group key of a placement record: (bin, side); pads have their own
+__device__ __forceinline__ uint64_t hj_group(uint64_t w0) { return (w0 & ~HJ_DROP) >> 32; }
+
+__global__ void __launch_bounds__(MN_THREADS) k_hj_sum(const uint64_t* w0, RunSum* tiles)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_hj_sum"));
+    __shared__ RunSum sm[MN_THREADS];
+    const size_t base = (size_t)blockIdx.x * MN_TS + (size_t)threadIdx.x * MN_RPT;
+    RunSum s {};
+#pragma unroll
+    for (int r = 0; r < MN_RPT; r++) {
+        VELO_TRACE_AT(TS_FILL, w0 + base + r);
+        s = run_combine(s, run_row(hj_group(w0[base + r]), 1ull));
+    }
+    RunSum total;
+    run_block_scan_excl(s, sm, &total);
+    if (threadIdx.x == 0) {
+        VELO_TRACE_AT(TS_FILL, tiles + blockIdx.x);
+        tiles[blockIdx.x] = total;
+    }
+}
+
+// rank in the (bin, side) group: keep the first C rows of every bin's group,
+// count real rows past the capacity (one counter update per CTA)
+__global__ void __launch_bounds__(MN_THREADS) k_hj_rank(uint64_t* w0, const RunSum* carry, uint32_t B, uint32_t cb,
+                                                        uint32_t cp, unsigned long long* overflow)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_hj_rank"));
+    __shared__ RunSum sm[MN_THREADS];
+    __shared__ uint32_t tmp[33];
+    const size_t base = (size_t)blockIdx.x * MN_TS + (size_t)threadIdx.x * MN_RPT;
+    uint64_t a[MN_RPT];
+    RunSum s {};
+#pragma unroll
+    for (int r = 0; r < MN_RPT; r++) {
+        VELO_TRACE_AT(TS_FILL, w0 + base + r);
+        a[r] = w0[base + r];
+        s = run_combine(s, run_row(hj_group(a[r]), 1ull));
+    }
+    RunSum total;
+    RunSum run = run_combine(carry[blockIdx.x], run_block_scan_excl(s, sm, &total));
+    uint32_t over = 0;
+#pragma unroll
+    for (int r = 0; r < MN_RPT; r++) {
+        const uint64_t grp = hj_group(a[r]);
+        const uint64_t rank = (run.has && run.last_key == grp) ? run.tail_nb : 0ull;
+        const uint64_t bin = grp >> 1;
+        const uint32_t cap = (grp & 1ull) ? cp : cb;
+        const bool pad = a[r] == ~0ull;
+        const bool keep = !pad & (bin < B) & (rank < cap);
+        over += (!pad & (bin < B) & ((a[r] & HJ_DUMMY) == 0) & (rank >= cap)) ? 1u : 0u;
+        VELO_TRACE_AT(TS_FILL, w0 + base + r);
+        w0[base + r] = keep ? (a[r] & ~HJ_DROP) : (a[r] | HJ_DROP);
+        run = run_combine(run, run_row(grp, 1ull));
+    }
+    uint32_t t;
+    block_exclusive_scan(over, tmp, &t);
+    if (threadIdx.x == 0 && t)
+        atomicAdd(overflow, (unsigned long long)t);
+}
+
+// one CTA per bin: every probe slot against every build slot of the bin
+// probe slot record: o0 = [63] not joined | probe row id, o1 = build row id
+__global__ void __launch_bounds__(HJ_THREADS) k_hj_bins(const uint64_t* w0, const uint64_t* w1, HjGeom g,
+                                                        size_t out_rows, uint64_t* o0, uint64_t* o1,
+                                                        unsigned long long* dups)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_hj_bins"));
+    extern __shared__ __align__(16) char smem[];
+    uint64_t* bkey = reinterpret_cast<uint64_t*>(smem);
+    uint64_t* brow = bkey + g.cb; // row id, or ~0 for a dummy
+    __shared__ uint32_t tmp[33];
+    const size_t bin = blockIdx.x;
+    const size_t base = bin * (size_t)(g.cb + g.cp);
+    for (uint32_t i = threadIdx.x; i < g.cb; i += blockDim.x) {
+        VELO_TRACE_AT(TS_ROW_LOAD, w0 + base + i);
+        const uint64_t a = w0[base + i];
+        bkey[i] = w1[base + i];
+        brow[i] = (a & HJ_DUMMY) ? ~0ull : (a & HJ_ID);
+    }
+    __syncthreads();
+    uint32_t dup = 0;
+    for (uint32_t p0 = threadIdx.x; p0 < g.cp; p0 += 4 * blockDim.x) {
+        uint64_t pkey[4], prow[4], hit[4];
+        uint32_t cnt[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t p = p0 + q * blockDim.x;
+            const bool in = p < g.cp;
+            const size_t gi = base + g.cb + (in ? p : 0);
+            VELO_TRACE_AT(TS_ROW_LOAD, w0 + gi);
+            const uint64_t a = w0[gi];
+            pkey[q] = w1[gi];
+            prow[q] = (!in || (a & HJ_DUMMY)) ? ~0ull : (a & HJ_ID);
+            hit[q] = ~0ull;
+            cnt[q] = 0;
+        }
+        for (uint32_t j = 0; j < g.cb; j++) {
+            const uint64_t k = bkey[j], r = brow[j];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const bool eq = (k == pkey[q]) & (r != ~0ull);
+                hit[q] = eq ? r : hit[q];
+                cnt[q] += eq ? 1u : 0u;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const uint32_t p = p0 + q * blockDim.x;
+            const bool joined = (prow[q] != ~0ull) & (cnt[q] != 0);
+            dup += (prow[q] != ~0ull && cnt[q] > 1) ? 1u : 0u;
+            if (p < g.cp) {
+                const size_t o = bin * (size_t)g.cp + p;
+                VELO_TRACE_AT(TS_ROW_STORE, o0 + o);
+                o0[o] = joined ? (prow[q] & HJ_ID) : (HJ_DROP | (prow[q] & HJ_ID));
+                o1[o] = joined ? hit[q] : ~0ull;
+            }
+        }
+    }
+    uint32_t t;
+    block_exclusive_scan(dup, tmp, &t);
+    if (threadIdx.x == 0 && t)
+        atomicAdd(dups, (unsigned long long)t);
+    // the pad records after the last bin's slots
+    if (blockIdx.x == 0)
+        for (size_t i = g.probe_slots + threadIdx.x; i < out_rows; i += blockDim.x) {
+            o0[i] = ~0ull;
+            o1[i] = ~0ull;
+        }
+}
+
+__global__ void k_hj_out(const uint64_t* o0, const uint64_t* o1, size_t pn, const uint64_t* pairs,
+                         const unsigned long long* dups, const unsigned long long* overflow, int64_t* ob, int64_t* op,
+                         uint64_t* d_counts)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_hj_out"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, pn);
+         i += (size_t)gridDim.x * blockDim.x) {
+        VELO_TRACE_AT(TS_ROW_LOAD, o0 + i);
+        const uint64_t a = o0[i];
+        const bool j = (a & HJ_DROP) == 0;
+        ob[i] = j ? (int64_t)o1[i] : -1;
+        op[i] = j ? (int64_t)(a & HJ_ID) : -1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        d_counts[0] = *pairs;
+        d_counts[1] = *dups;
+        d_counts[2] = *overflow;
+    }
+}
+
+struct HjScratch {
+    HjGeom g;
+    uint64_t* w[2];
+    uint64_t* o[2];
+    RunSum* tiles;
+    RunSum* carry;
+    uint32_t* counts;
+    uint32_t* prefix;
+    uint64_t* n_marked;
+    uint32_t* ocounts;
+    uint32_t* oprefix;
+    uint64_t* pairs;
+    unsigned long long* stat; // [0] repeated build keys, [1] overflow
+    size_t bytes;
+};
+
+static HjScratch hj_layout(char* base, size_t build_n, size_t probe_n)
+{
+    HjScratch s {};
+    s.g = hj_geometry(build_n, probe_n);
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        char* p = base ? base + off : nullptr;
+        off += align_up(b ? b : 1, 256);
+        return p;
+    };
+    for (int i = 0; i < 2; i++)
+        s.w[i] = reinterpret_cast<uint64_t*>(take(s.g.rows * 8));
+    for (int i = 0; i < 2; i++)
+        s.o[i] = reinterpret_cast<uint64_t*>(take(s.g.out_rows * 8));
+    const size_t nt = s.g.rows / MN_TS;
+    s.tiles = reinterpret_cast<RunSum*>(take(nt * sizeof(RunSum)));
+    s.carry = reinterpret_cast<RunSum*>(take(nt * sizeof(RunSum)));
+    s.counts = reinterpret_cast<uint32_t*>(take((s.g.rows >> OP_LT) * 4));
+    s.prefix = reinterpret_cast<uint32_t*>(take(((s.g.rows >> OP_LT) + 1) * 4));
+    s.n_marked = reinterpret_cast<uint64_t*>(take(8));
+    s.ocounts = reinterpret_cast<uint32_t*>(take((s.g.out_rows >> OP_LT) * 4));
+    s.oprefix = reinterpret_cast<uint32_t*>(take(((s.g.out_rows >> OP_LT) + 1) * 4));
+    s.pairs = reinterpret_cast<uint64_t*>(take(8));
+    s.stat = reinterpret_cast<unsigned long long*>(take(16));
+    s.bytes = off;
+    return s;
+}
+
+using HjRec = RowRec<2, 1, false, KEY_FULL>;
+
+} // namespace velo
+
+extern "C" size_t velo_ohash_join_scratch_bytes(size_t build_n, size_t probe_n)
+{
+    return hj_layout(nullptr, build_n, probe_n).bytes;
+}
+
+extern "C" velo_status velo_ohash_join(const void* d_build_keys, const uint8_t* d_build_mask, size_t build_n,
+                                       const void* d_probe_keys, const uint8_t* d_probe_mask, size_t probe_n,
+                                       uint32_t key_type, uint64_t hash_seed, int64_t* d_out_build_rowid,
+                                       int64_t* d_out_probe_rowid, uint64_t* d_counts, void* d_scratch,
+                                       size_t scratch_bytes, void* stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!d_counts)
+        return einval("velo_ohash_join: null counts");
+    if (key_type != VELO_INTEGER && key_type != VELO_BIGINT)
+        return einval("velo_ohash_join: join keys must be INTEGER or BIGINT");
+    if (build_n >= 0x80000000ull || probe_n >= 0x80000000ull)
+        return einval("velo_ohash_join: sizes must be below 2^31");
+    if (probe_n == 0 || build_n == 0) {
+        VELO_CUDA_TRY(cudaMemsetAsync(d_counts, 0, 24, st), "cudaMemsetAsync");
+        if (probe_n) {
+            VELO_CUDA_TRY(cudaMemsetAsync(d_out_build_rowid, 0xFF, probe_n * 8, st), "cudaMemsetAsync");
+            VELO_CUDA_TRY(cudaMemsetAsync(d_out_probe_rowid, 0xFF, probe_n * 8, st), "cudaMemsetAsync");
+        }
+        return VELO_OK;
+    }
+    if (!d_build_keys || !d_probe_keys || !d_out_build_rowid || !d_out_probe_rowid)
+        return einval("velo_ohash_join: null buffer");
+    HjScratch s = hj_layout(static_cast<char*>(d_scratch), build_n, probe_n);
+    const HjGeom& g = s.g;
+    const int logR = ilog2_floor(g.rows), logO = ilog2_floor(g.out_rows);
+    if (logR > MAX_LOGN)
+        return einval("velo_ohash_join: too large");
+    if ((size_t)g.cb * 16 > MAX_SMEM_BYTES)
+        return einval("velo_ohash_join: bins too large");
+    if (!d_scratch || scratch_bytes < s.bytes) {
+        set_error("velo_ohash_join: scratch must hold velo_ohash_join_scratch_bytes() bytes");
+        return VELO_ENOMEM;
+    }
+    VELO_CUDA_TRY(cudaMemsetAsync(s.stat, 0, 16, st), "cudaMemsetAsync");
+    k_hj_pack<<<mn_grid(g.rows), 256, 0, st>>>(d_build_keys, d_build_mask, build_n, d_probe_keys, d_probe_mask,
+                                               probe_n, key_type == VELO_BIGINT, g, hash_seed, s.w[0], s.w[1]);
+    VELO_CUDA_TRY(cudaGetLastError(), "ohash_join pack launch");
+    HjRec::Cols c;
+    for (int i = 0; i < 2; i++) {
+        c.w[i] = s.w[i];
+        c.pad[i] = ~0ull;
+    }
+    c.mask[0] = ~0ull;
+    c.mark_word = 0;
+    c.mark_bit = 63;
+    c.mark_inv = 1; // kept rows (bit 63 clear) are marked
+    std::vector<NetPass> passes;
+    plan_sort(logR, OP_LT, OP_LMAX, passes);
+    velo_status rc = launch_net12<HjRec>(c, NetGeom { g.rows, logR, 0 }, passes, nullptr, st);
+    if (rc != VELO_OK)
+        return rc;
+    const int nt = (int)(g.rows / MN_TS);
+    k_hj_sum<<<nt, MN_THREADS, 0, st>>>(s.w[0], s.tiles);
+    k_run_scan<<<1, 1024, 0, st>>>(s.tiles, nt, s.carry);
+    k_hj_rank<<<nt, MN_THREADS, 0, st>>>(s.w[0], s.carry, g.B, g.cb, g.cp, s.stat + 1);
+    VELO_CUDA_TRY(cudaGetLastError(), "ohash_join rank launch");
+    const int nct = (int)(g.rows >> OP_LT);
+    k_count_marks<HjRec><<<nct, 256, 0, st>>>(c, g.rows, OP_LT, s.counts);
+    k_scan_tiles<<<1, 1024, 0, st>>>(s.counts, nct, s.prefix, s.n_marked);
+    passes.clear();
+    plan_compact(logR, OP_LT, OP_LMAX, passes);
+    rc = launch_net12<HjRec>(c, NetGeom { g.rows, logR, 0 }, passes, s.prefix, st);
+    if (rc != VELO_OK)
+        return rc;
+    const size_t smem = (size_t)g.cb * 16;
+    static int done[64] = {};
+    rc = ensure_smem(k_hj_bins, MAX_SMEM_BYTES, done);
+    if (rc != VELO_OK)
+        return rc;
+    k_hj_bins<<<g.B, HJ_THREADS, smem, st>>>(s.w[0], s.w[1], g, g.out_rows, s.o[0], s.o[1], s.stat);
+    VELO_CUDA_TRY(cudaGetLastError(), "ohash_join bins launch");
+    HjRec::Cols oc;
+    for (int i = 0; i < 2; i++) {
+        oc.w[i] = s.o[i];
+        oc.pad[i] = ~0ull;
+    }
+    oc.mask[0] = ~0ull;
+    oc.mark_word = 0;
+    oc.mark_bit = 63;
+    oc.mark_inv = 1; // joined probe slots
+    const int nco = (int)(g.out_rows >> OP_LT);
+    k_count_marks<HjRec><<<nco, 256, 0, st>>>(oc, g.out_rows, OP_LT, s.ocounts);
+    k_scan_tiles<<<1, 1024, 0, st>>>(s.ocounts, nco, s.oprefix, s.pairs);
+    passes.clear();
+    plan_compact(logO, OP_LT, OP_LMAX, passes);
+    rc = launch_net12<HjRec>(oc, NetGeom { g.out_rows, logO, 0 }, passes, s.oprefix, st);
+    if (rc != VELO_OK)
+        return rc;
+    k_hj_out<<<mn_grid(probe_n), 256, 0, st>>>(s.o[0], s.o[1], probe_n, s.pairs, s.stat, s.stat + 1,
+                                               d_out_build_rowid, d_out_probe_rowid, d_counts);
+    VELO_CUDA_TRY(cudaGetLastError(), "ohash_join out launch");
     return VELO_OK;
 }

@@ -123,37 +123,6 @@ __global__ void __launch_bounds__(256) k_scatter_write(const uint8_t* mask, size
     }
 }
 
-// ---------------------------------------------------------------------------
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), counter-based PRF used
-// to draw the shuffle keys on the device
-// ---------------------------------------------------------------------------
-
-__host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo)
-{
-    const uint64_t p = (uint64_t)a * b;
-    hi = (uint32_t)(p >> 32);
-    lo = (uint32_t)p;
-}
-
-__host__ __device__ __forceinline__ uint64_t philox_u64(uint64_t idx, uint64_t counter, uint64_t key)
-{
-    uint32_t c0 = (uint32_t)idx, c1 = (uint32_t)(idx >> 32), c2 = (uint32_t)counter, c3 = (uint32_t)(counter >> 32);
-    uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
-    for (int r = 0; r < 10; r++) {
-        uint32_t hi0, lo0, hi1, lo1;
-        mulhilo32(0xD2511F53u, c0, hi0, lo0);
-        mulhilo32(0xCD9E8D57u, c2, hi1, lo1);
-        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
-        c0 = n0;
-        c1 = lo1;
-        c2 = n2;
-        c3 = lo0;
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
-    }
-    return ((uint64_t)c1 << 32) | c0;
-}
-
 __global__ void k_shuffle_pack(const uint32_t* map, size_t n, size_t np, uint64_t counter, uint64_t key, uint64_t* k,
                                uint32_t* p)
 {

@@ -85,6 +85,16 @@ velo_status dispatch(velo_ctx* c, const velo_cmd& m)
                                a.ojoin.d_probe_mask, a.ojoin.probe_n, a.ojoin.key_type, a.ojoin.d_out_build_rowid,
                                a.ojoin.d_out_probe_rowid, a.ojoin.d_counts, a.ojoin.d_scratch, a.ojoin.scratch_bytes,
                                st);
+    case VELO_OP_OJOIN_MN:
+        return velo_ojoin_mn(a.ojoin_mn.d_build_keys, a.ojoin_mn.d_build_mask, a.ojoin_mn.build_n,
+                             a.ojoin_mn.d_probe_keys, a.ojoin_mn.d_probe_mask, a.ojoin_mn.probe_n, a.ojoin_mn.key_type,
+                             a.ojoin_mn.max_pairs, a.ojoin_mn.d_out_build_rowid, a.ojoin_mn.d_out_probe_rowid,
+                             a.ojoin_mn.d_counts, a.ojoin_mn.d_scratch, a.ojoin_mn.scratch_bytes, st);
+    case VELO_OP_OHASH_JOIN:
+        return velo_ohash_join(a.ohash.d_build_keys, a.ohash.d_build_mask, a.ohash.build_n, a.ohash.d_probe_keys,
+                               a.ohash.d_probe_mask, a.ohash.probe_n, a.ohash.key_type, a.ohash.hash_seed,
+                               a.ohash.d_out_build_rowid, a.ohash.d_out_probe_rowid, a.ohash.d_counts,
+                               a.ohash.d_scratch, a.ohash.scratch_bytes, st);
     case VELO_OP_OGATHER:
         return velo_ogather_u64(a.ogather.d_table, a.ogather.table_n, a.ogather.d_rids, a.ogather.n_req,
                                 a.ogather.d_out, a.ogather.d_scratch, a.ogather.scratch_bytes, st);

@@ -9,6 +9,37 @@
 namespace velo {
 
 // ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), counter-based PRF used
+// to draw the shuffle keys on the device
+// ---------------------------------------------------------------------------
+
+__host__ __device__ __forceinline__ void mulhilo32(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo)
+{
+    const uint64_t p = (uint64_t)a * b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+}
+
+__host__ __device__ __forceinline__ uint64_t philox_u64(uint64_t idx, uint64_t counter, uint64_t key)
+{
+    uint32_t c0 = (uint32_t)idx, c1 = (uint32_t)(idx >> 32), c2 = (uint32_t)counter, c3 = (uint32_t)(counter >> 32);
+    uint32_t k0 = (uint32_t)key, k1 = (uint32_t)(key >> 32);
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo32(0xD2511F53u, c0, hi0, lo0);
+        mulhilo32(0xCD9E8D57u, c2, hi1, lo1);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return ((uint64_t)c1 << 32) | c0;
+}
+
+// ---------------------------------------------------------------------------
 // forward fill over a key-sorted record array: every row receives the
 // (key, value) of the last "source" row at or before it (segmented scan in
 // three passes; addresses never depend on the data)
@@ -226,5 +257,65 @@ inline UnionScratch union_layout(char* base, size_t rows)
     s.bytes = off;
     return s;
 }
+
+// Run counts over a key-sorted array (the scans of the joins): summary of a
+// range of rows = first/last key, counted rows in it, counted rows in its
+// trailing key run, whether it is one key run
+struct RunSum {
+    uint64_t first_key, last_key;
+    uint64_t nb, tail_nb;
+    uint32_t uniform, has;
+};
+
+// a then b (a the earlier range); associative
+__device__ __forceinline__ RunSum run_combine(const RunSum& a, const RunSum& b)
+{
+    if (!a.has)
+        return b;
+    if (!b.has)
+        return a;
+    const bool join = a.last_key == b.first_key;
+    RunSum r;
+    r.first_key = a.first_key;
+    r.last_key = b.last_key;
+    r.nb = a.nb + b.nb;
+    r.tail_nb = b.tail_nb + ((b.uniform && join) ? a.tail_nb : 0ull);
+    r.uniform = (a.uniform && b.uniform && join) ? 1u : 0u;
+    r.has = 1u;
+    return r;
+}
+
+__device__ __forceinline__ RunSum run_row(uint64_t key, uint64_t counted)
+{
+    return RunSum { key, key, counted, counted, 1u, 1u };
+}
+
+// block-wide exclusive scan of RunSum (shared-memory Hillis-Steele over the
+// threads' summaries); the block total is returned in *total
+__device__ __forceinline__ RunSum run_block_scan_excl(const RunSum& mine, RunSum* sm, RunSum* total)
+{
+    const int t = threadIdx.x, n = blockDim.x;
+    RunSum x = mine;
+    for (int off = 1; off < n; off <<= 1) {
+        __syncthreads();
+        sm[t] = x;
+        __syncthreads();
+        if (t >= off)
+            x = run_combine(sm[t - off], x);
+    }
+    __syncthreads();
+    sm[t] = x;
+    __syncthreads();
+    *total = sm[n - 1];
+    RunSum ex {};
+    if (t > 0)
+        ex = sm[t - 1];
+    __syncthreads();
+    return ex;
+}
+
+// exclusive scan of run summaries of tiles (one CTA of 1024 threads),
+// defined in joins.cu
+__global__ void k_run_scan(const RunSum* tiles, int ntiles, RunSum* carry);
 
 } // namespace velo

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <random>
 
 namespace velo_b200 {
 
@@ -477,10 +478,10 @@ Result<RowBatch> SortMergeJoinOperator::next()
 {
     if (joined_)
         return Result<RowBatch>::success(RowBatch());
-    return join({ -1, -1 });
+    return join({ -1, -1 }, false);
 }
 
-Result<RowBatch> SortMergeJoinOperator::join(std::pair<long, long> mask_indices)
+Result<RowBatch> SortMergeJoinOperator::join(std::pair<long, long> mask_indices, bool hashed)
 {
     joined_ = true;
     if (join_type_ != JoinType::INNER)
@@ -507,31 +508,87 @@ Result<RowBatch> SortMergeJoinOperator::join(std::pair<long, long> mask_indices)
         ? static_cast<const uint8_t*>(right.getColumn((size_t)mask_indices.second).rawData())
         : nullptr;
     std::shared_ptr<void> brow = device_alloc(context_, pn * 8), prow = device_alloc(context_, pn * 8);
-    std::shared_ptr<void> counts = device_alloc(context_, 16);
-    const size_t sb = velo_ojoin_scratch_bytes(bn, pn);
-    std::shared_ptr<void> scratch = device_alloc(context_, sb);
+    std::shared_ptr<void> counts = device_alloc(context_, 24);
+    uint64_t hc[3] = { 0, 0, 0 };
     velo_cmd cmd;
     std::memset(&cmd, 0, sizeof cmd);
-    cmd.opcode = VELO_OP_OJOIN_PKFK;
-    cmd.args.ojoin.d_build_keys = lk.rawData();
-    cmd.args.ojoin.d_build_mask = bmask;
-    cmd.args.ojoin.build_n = bn;
-    cmd.args.ojoin.d_probe_keys = rk.rawData();
-    cmd.args.ojoin.d_probe_mask = pmask;
-    cmd.args.ojoin.probe_n = pn;
-    cmd.args.ojoin.key_type = lk.getType();
-    cmd.args.ojoin.d_out_build_rowid = static_cast<int64_t*>(brow.get());
-    cmd.args.ojoin.d_out_probe_rowid = static_cast<int64_t*>(prow.get());
-    cmd.args.ojoin.d_counts = static_cast<uint64_t*>(counts.get());
-    cmd.args.ojoin.d_scratch = scratch.get();
-    cmd.args.ojoin.scratch_bytes = sb;
-    context_.run(cmd);
-    uint64_t hc[2] = { 0, 0 };
-    check(velo_copy(hc, counts.get(), 16, VELO_COPY_D2H, context_.stream()), "join counts");
-    context_.sync();
-    if (hc[1] != 0)
-        return Result<RowBatch>::failure("the left (build) input repeats join keys; the oblivious join needs a key "
-                                         "on the build side");
+    if (hashed) {
+        // the oblivious bin-padded hash join; a repeated build key or a bin
+        // overflow sends the join to the many-to-many sort-merge join below
+        const size_t sb = velo_ohash_join_scratch_bytes(bn, pn);
+        std::shared_ptr<void> scratch = device_alloc(context_, sb);
+        cmd.opcode = VELO_OP_OHASH_JOIN;
+        cmd.args.ohash.d_build_keys = lk.rawData();
+        cmd.args.ohash.d_build_mask = bmask;
+        cmd.args.ohash.build_n = bn;
+        cmd.args.ohash.d_probe_keys = rk.rawData();
+        cmd.args.ohash.d_probe_mask = pmask;
+        cmd.args.ohash.probe_n = pn;
+        cmd.args.ohash.key_type = lk.getType();
+        cmd.args.ohash.hash_seed = hash_seed_;
+        cmd.args.ohash.d_out_build_rowid = static_cast<int64_t*>(brow.get());
+        cmd.args.ohash.d_out_probe_rowid = static_cast<int64_t*>(prow.get());
+        cmd.args.ohash.d_counts = static_cast<uint64_t*>(counts.get());
+        cmd.args.ohash.d_scratch = scratch.get();
+        cmd.args.ohash.scratch_bytes = sb;
+        context_.run(cmd);
+        check(velo_copy(hc, counts.get(), 24, VELO_COPY_D2H, context_.stream()), "join counts");
+        context_.sync();
+    } else {
+        // the oblivious PK-FK join; a repeated build key sends the join to the
+        // many-to-many join below
+        const size_t sb = velo_ojoin_scratch_bytes(bn, pn);
+        std::shared_ptr<void> scratch = device_alloc(context_, sb);
+        cmd.opcode = VELO_OP_OJOIN_PKFK;
+        cmd.args.ojoin.d_build_keys = lk.rawData();
+        cmd.args.ojoin.d_build_mask = bmask;
+        cmd.args.ojoin.build_n = bn;
+        cmd.args.ojoin.d_probe_keys = rk.rawData();
+        cmd.args.ojoin.d_probe_mask = pmask;
+        cmd.args.ojoin.probe_n = pn;
+        cmd.args.ojoin.key_type = lk.getType();
+        cmd.args.ojoin.d_out_build_rowid = static_cast<int64_t*>(brow.get());
+        cmd.args.ojoin.d_out_probe_rowid = static_cast<int64_t*>(prow.get());
+        cmd.args.ojoin.d_counts = static_cast<uint64_t*>(counts.get());
+        cmd.args.ojoin.d_scratch = scratch.get();
+        cmd.args.ojoin.scratch_bytes = sb;
+        context_.run(cmd);
+        check(velo_copy(hc, counts.get(), 16, VELO_COPY_D2H, context_.stream()), "join counts");
+        context_.sync();
+    }
+    if (hc[1] != 0 || hc[2] != 0) {
+        // many-to-many: every pair, first bounded by the probe side; a larger
+        // pair count (revealed, as the reference's SMJ count step does) sizes
+        // a second run
+        size_t bound = pn;
+        for (int attempt = 0; attempt < 2; attempt++) {
+            brow = device_alloc(context_, bound * 8);
+            prow = device_alloc(context_, bound * 8);
+            const size_t sb = velo_ojoin_mn_scratch_bytes(bn, pn, bound);
+            std::shared_ptr<void> scratch = device_alloc(context_, sb);
+            std::memset(&cmd, 0, sizeof cmd);
+            cmd.opcode = VELO_OP_OJOIN_MN;
+            cmd.args.ojoin_mn.d_build_keys = lk.rawData();
+            cmd.args.ojoin_mn.d_build_mask = bmask;
+            cmd.args.ojoin_mn.build_n = bn;
+            cmd.args.ojoin_mn.d_probe_keys = rk.rawData();
+            cmd.args.ojoin_mn.d_probe_mask = pmask;
+            cmd.args.ojoin_mn.probe_n = pn;
+            cmd.args.ojoin_mn.key_type = lk.getType();
+            cmd.args.ojoin_mn.max_pairs = bound;
+            cmd.args.ojoin_mn.d_out_build_rowid = static_cast<int64_t*>(brow.get());
+            cmd.args.ojoin_mn.d_out_probe_rowid = static_cast<int64_t*>(prow.get());
+            cmd.args.ojoin_mn.d_counts = static_cast<uint64_t*>(counts.get());
+            cmd.args.ojoin_mn.d_scratch = scratch.get();
+            cmd.args.ojoin_mn.scratch_bytes = sb;
+            context_.run(cmd);
+            check(velo_copy(hc, counts.get(), 16, VELO_COPY_D2H, context_.stream()), "join counts");
+            context_.sync();
+            if (hc[1] == 0)
+                break;
+            bound = (size_t)hc[0];
+        }
+    }
     const size_t pairs = (size_t)hc[0];
     std::vector<Column> out;
     auto gather_side = [&](RowBatch& side, const std::shared_ptr<void>& rowids) {
@@ -574,13 +631,17 @@ HashJoinOperator::HashJoinOperator(ExecutionContext& context, Schema output_sche
                             join_type)
     , mask_indices_(mask_indices)
 {
+    // the bin hash is keyed per operator, so bin assignments cannot be
+    // chosen ahead by whoever supplies the keys
+    std::random_device rd;
+    hash_seed_ = ((uint64_t)rd() << 32) ^ (uint64_t)rd();
 }
 
 Result<RowBatch> HashJoinOperator::next()
 {
     if (joined_)
         return Result<RowBatch>::success(RowBatch());
-    return join(mask_indices_);
+    return join(mask_indices_, true);
 }
 
 // ---- materialization ---------------------------------------------------------
