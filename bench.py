@@ -52,7 +52,7 @@ METRIC = "obliv sort & join Mrows/s (frac of HBM peak); p50/p99 latency served v
 # DRAM bytes (read + write) per launch of the dominant kernel from one ncu
 # capture of the same pipeline (the mean over its sort passes), or None when
 # no capture of that launch exists.
-TRAFFIC = {"groupby": 210.1e6, "sort": 12.65e6, "join": None, "batch": None}
+TRAFFIC = {"groupby": 210.1e6, "sort": 12.65e6, "join": 210.6e6, "batch": None}
 
 # warm-up runs at least this long (seconds) so that the clock samples taken
 # from the end of the warm-up through the timed steps show the GPU under load

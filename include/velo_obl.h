@@ -285,12 +285,11 @@ velo_status velo_ogather_column(const void* d_table_col, uint32_t type, const ui
 /* Oblivious GROUP BY key with SUM / COUNT: one or two aggregates a call
  * (n_sums int64 columns summed mod 2^64, plus COUNT when with_count; n_sums +
  * with_count is 1 or 2).  Rows with mask == 0 (NULL = all rows) are left out.
- * Keys: VELO_INTEGER, or VELO_BIGINT in [-2^62, 2^62) (other BIGINT keys are
- * left out and counted).  Writes the first group_bound groups in key order --
- * d_out_keys[j], d_out_sums[s][j], d_out_counts[j] -- and zeros past the
- * number of groups; d_counts (2 u64) = (groups, rows left out for their key).
- * Sort, segmented sums and ORCompact of one record per group; every address
- * depends only on n and group_bound.  The reference engine declares an
+ * Keys: VELO_INTEGER or VELO_BIGINT, every value of either.  Writes the first
+ * group_bound groups in key order -- d_out_keys[j], d_out_sums[s][j],
+ * d_out_counts[j] -- and zeros past the number of groups; d_counts (2 u64) =
+ * (groups, 0).  Sort, segmented sums and ORCompact of one record per group;
+ * every address depends only on n, group_bound and the key type.  The reference engine declares an
  * aggregate plan node (include/planner/abstract_plan_node.hpp:31) without an
  * operator; the algorithm is obliviator/operator_2/enclave/
  * scalable_oblivious_join.c:105-262. */

@@ -53,16 +53,43 @@ def test_ogroupby_matches_exact_sums(cuda, n, combo):
     assert not ok[g:].any() and all(not a[g:].any() for a in osum)
 
 
-def test_ogroupby_bigint_keys_and_range(cuda):
+EXTREMES = np.array([-(2**63), -(2**63) + 1, -(2**62) - 1, -(2**62), -5, 0, 7, 2**62 - 1, 2**62, 2**63 - 2,
+                     2**63 - 1], np.int64)
+
+
+@pytest.mark.parametrize("combo", [(0, True), (1, True), (1, False), (2, False)])
+def test_ogroupby_bigint_full_range(cuda, combo):
+    # every BIGINT value is a key, the extremes included, with and without a
+    # mask; a key whose rows are all left out forms no group
+    ns, with_count = combo
     n = 50_000
-    rng = np.random.default_rng(3)
-    keys = rng.choice(np.array([-(2**62), -5, 0, 7, 2**62 - 1, 2**62, -(2**62) - 1, 2**63 - 1], np.int64), n)
-    vals = [rng.integers(0, 1000, n).astype(np.int64)]
-    ok, osum, ocnt, cnt = run(keys, BIGINT, vals, True)
-    inr = (keys >= -(2**62)) & (keys < 2**62)
-    ek, es, ec = expected(keys, vals, inr)
+    rng = np.random.default_rng(3 + ns)
+    keys = rng.choice(EXTREMES, n)
+    vals = [rng.integers(-10**12, 10**12, n).astype(np.int64) for _ in range(ns)]
+    for mask in (None, rng.random(n) < 0.6, keys != 2**63 - 1):
+        ok, osum, ocnt, cnt = run(keys, BIGINT, vals, with_count, mask)
+        ek, es, ec = expected(keys, vals, np.ones(n, bool) if mask is None else mask)
+        g = len(ek)
+        assert int(cnt[0]) == g and int(cnt[1]) == 0
+        assert np.array_equal(ok[:g], ek)
+        for a, b in zip(osum, es):
+            assert np.array_equal(a[:g], b)
+        if with_count:
+            assert np.array_equal(ocnt[:g], ec)
+        assert not ok[g:].any()
+
+
+@pytest.mark.parametrize("n", [1, 4097, 300_000])
+def test_ogroupby_bigint_random(cuda, n):
+    rng = np.random.default_rng(n)
+    keys = (rng.integers(-(2**63), 2**63 - 1, n, dtype=np.int64) // (2**60)) * (2**60)  # 16 distinct values
+    keys[: n // 3] = rng.integers(-(2**63), 2**63 - 1, n // 3, dtype=np.int64)
+    vals = [rng.integers(-10**9, 10**9, n).astype(np.int64)]
+    mask = rng.random(n) < 0.8
+    ok, osum, ocnt, cnt = run(keys, BIGINT, vals, True, mask)
+    ek, es, ec = expected(keys, vals, mask)
     g = len(ek)
-    assert int(cnt[0]) == g and int(cnt[1]) == int((~inr).sum())
+    assert int(cnt[0]) == g
     assert np.array_equal(ok[:g], ek) and np.array_equal(osum[0][:g], es[0]) and np.array_equal(ocnt[:g], ec)
 
 

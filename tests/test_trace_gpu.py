@@ -408,3 +408,37 @@ def test_hash_join_trace_is_data_independent(T):
         return f
 
     assert_same_trace([trace_of(T, join(x, mm)) for x, mm in ((6, False), (7, False), (8, True))])
+
+
+def test_ogroupby_bigint_trace_is_data_independent(T):
+    n = 40_001
+    keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    vals = torch.empty(n, dtype=torch.int64, device="cuda")
+    mask = torch.empty(n, dtype=torch.uint8, device="cuda")
+    bound = 500
+    ok = torch.empty(bound, dtype=torch.int64, device="cuda")
+    os_ = torch.empty(bound, dtype=torch.int64, device="cuda")
+    oc = torch.empty(bound, dtype=torch.int64, device="cuda")
+    cnt = torch.empty(2, dtype=torch.int64, device="cuda")
+    sb = T.velo_ogroupby_scratch_bytes(n)
+    s = torch.empty(sb, dtype=torch.uint8, device="cuda")
+    sums = (C.c_void_p * 2)(vals.data_ptr(), None)
+    outs = (C.c_void_p * 2)(os_.data_ptr(), None)
+
+    def run(k, dens):
+        def f():
+            rng = np.random.default_rng(int(dens * 100) + 1)
+            dev_copy(keys, k)
+            dev_copy(vals, rng.integers(0, 1000, n).astype(np.int64))
+            dev_copy(mask, (rng.random(n) < dens).astype(np.uint8))
+            torch.cuda.synchronize()
+            assert T.velo_ogroupby(keys.data_ptr(), 5, sums, 1, 1, mask.data_ptr(), n, bound, ok.data_ptr(), outs,
+                                   oc.data_ptr(), cnt.data_ptr(), s.data_ptr(), sb, None) == 0, \
+                T.velo_last_error_text()
+        return f
+
+    rng = np.random.default_rng(1)
+    cases = [(rng.integers(-(2**63), 2**63 - 1, n, dtype=np.int64), 0.5),              # distinct, extreme range
+             (np.full(n, 2**63 - 1, np.int64), 1.0),                                    # one key, the maximum
+             (rng.choice(np.array([-(2**63), 0, 2**63 - 1], np.int64), n), 0.0)]        # nothing selected
+    assert_same_trace([trace_of(T, run(k, d)) for k, d in cases])

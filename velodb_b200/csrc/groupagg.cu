@@ -14,8 +14,12 @@
 //   4. compact  ORCompact of the group records: groups first, in key order
 //   5. out      the first group_bound group records, decoded (zeros past the
 //               number of groups)
-// Every address depends only on n and group_bound.  Keys: INTEGER (any
-// value) or BIGINT in [-2^62, 2^62) (others are excluded and counted).
+// Every address depends only on n, group_bound and the key type.  INTEGER
+// keys share word 0 with the exclusion bit.  BIGINT keys use all 64 bits of
+// word 0 (key ^ 2^63), so their records carry the row's validity in a word of
+// its own, sorted after the key: within a key the rows left out come first,
+// so a key run ends on a valid row exactly when it holds one; their group
+// records carry the group flag in a word of its own too (segagg FLAG_WORD).
 #include "net_impl.cuh"
 #include "segagg.cuh"
 
@@ -47,6 +51,34 @@ struct GbAgg {
     }
     __device__ __forceinline__ static int64_t out_key_from(uint64_t key) { return (int64_t)(key & ~GB_EXCL); }
     __device__ __forceinline__ static uint64_t out_bits(uint64_t key) { return key & ~GB_EXCL; }
+};
+
+// BIGINT keys: records (key ^ 2^63, validity, sum 0, sum 1); aggregates
+// (count, sum 0, sum 1) -- the ones not asked for are computed on zeros and
+// dropped at the output
+struct GbAggWide {
+    static constexpr int W = 4;
+    static constexpr int V = 3;
+    static constexpr bool FLAG_WORD = true;
+    struct Params { };
+    __device__ __forceinline__ static uint64_t key(const uint64_t* w) { return w[0]; }
+    __device__ __forceinline__ static bool valid(const uint64_t* w) { return (w[1] & 1ull) != 0; }
+    __device__ __forceinline__ static void values(const uint64_t* w, int64_t (&v)[V], const Params&)
+    {
+        const bool ok = valid(w);
+        v[0] = ok ? 1 : 0;
+        v[1] = ok ? (int64_t)w[2] : 0;
+        v[2] = ok ? (int64_t)w[3] : 0;
+    }
+    __device__ __forceinline__ static int64_t out_key_from(uint64_t key) { return (int64_t)(key ^ (1ull << 63)); }
+    __device__ __forceinline__ static uint64_t out_bits(uint64_t key) { return key; }
+};
+
+struct GbTypesWide {
+    using Agg = GbAggWide;
+    using Seg = SegAgg<Agg>;
+    using Rec = RowRec<4, 2, false, KEY_FULL>; // sorted on (key, validity)
+    using Grp = RowRec<5, 1, false>;           // key, flag, count, sum 0, sum 1
 };
 
 template <int NS, int CNT>
@@ -116,6 +148,51 @@ __global__ void __launch_bounds__(256) k_gb_pack(GbIn in, size_t n, size_t np, u
         atomicAdd(d_rejected, (unsigned long long)total);
 }
 
+__global__ void __launch_bounds__(256) k_gb_pack_wide(GbIn in, int n_sums, size_t n, size_t np, uint64_t* w0,
+                                                      uint64_t* w1, uint64_t* w2, uint64_t* w3)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_gb_pack_wide"));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, np);
+         i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t k = ~0ull, f = 0, s0 = 0, s1 = 0;
+        if (i < n) {
+            k = (uint64_t) static_cast<const int64_t*>(in.keys)[i] ^ (1ull << 63);
+            f = (in.mask ? in.mask[i] != 0 : true) ? 1ull : 0ull;
+            s0 = n_sums >= 1 ? (uint64_t)in.sums[0][i] : 0ull;
+            s1 = n_sums >= 2 ? (uint64_t)in.sums[1][i] : 0ull;
+        }
+        VELO_TRACE_AT(TS_ROW_STORE, w0 + i);
+        w0[i] = k;
+        w1[i] = f;
+        w2[i] = s0;
+        w3[i] = s1;
+    }
+}
+
+__global__ void __launch_bounds__(SEG_THREADS) k_gbw_summary(GbTypesWide::Rec::Cols c, SegTileAgg* aggs, int64_t* runs)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_gbw_summary"));
+    extern __shared__ __align__(16) char sm[];
+    GbTypesWide::Seg::tile_summary(c.w, blockIdx.x, aggs, runs, {}, sm);
+}
+
+__global__ void __launch_bounds__(1024) k_gbw_carries(const SegTileAgg* aggs, const int64_t* runs, int ntiles,
+                                                      int64_t* carry_in, uint32_t* tail_prefix, uint64_t* n_groups)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_gbw_carries"));
+    extern __shared__ __align__(16) char sm[];
+    GbTypesWide::Seg::carries(aggs, runs, ntiles, carry_in, tail_prefix, n_groups, sm);
+}
+
+__global__ void __launch_bounds__(SEG_THREADS) k_gbw_emit_rows(GbTypesWide::Rec::Cols c, int ntiles,
+                                                               const SegTileAgg* aggs, const int64_t* carry_in,
+                                                               GbTypesWide::Grp::Cols g)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_gbw_emit_rows"));
+    extern __shared__ __align__(16) char sm[];
+    GbTypesWide::Seg::emit_rows(c.w, blockIdx.x, ntiles, aggs, carry_in, g.w, {}, sm);
+}
+
 template <int NS, int CNT>
 __global__ void __launch_bounds__(SEG_THREADS) k_gb_summary(typename GbTypes<NS, CNT>::Rec::Cols c, SegTileAgg* aggs,
                                                             int64_t* runs)
@@ -179,9 +256,35 @@ __global__ void k_gb_out(const uint64_t* g0, const uint64_t* g1, const uint64_t*
     }
 }
 
+// wide group records: g[0] = key ^ 2^63, g[1] = flag, g[2] count, g[3..4] sums
+struct GbwWords {
+    const uint64_t* g[5];
+};
+
+__global__ void k_gbw_out(GbwWords g, size_t bound, int n_sums, int with_count, GbOut out,
+                          const uint64_t* n_groups, uint64_t* d_counts)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_gbw_out"));
+    const uint64_t ng = *n_groups;
+    for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(j, bound);
+         j += (size_t)gridDim.x * blockDim.x) {
+        const bool ok = j < ng;
+        VELO_TRACE_AT(TS_ROW_LOAD, g.g[0] + j);
+        out.keys[j] = ok ? (int64_t)(g.g[0][j] ^ (1ull << 63)) : 0;
+        if (with_count)
+            out.counts[j] = ok ? (int64_t)g.g[2][j] : 0;
+        for (int s = 0; s < n_sums; s++)
+            out.sums[s][j] = ok ? (int64_t)g.g[3 + s][j] : 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        d_counts[0] = ng;
+        d_counts[1] = 0;
+    }
+}
+
 struct GbScratch {
-    uint64_t* r[3];      // sort records
-    uint64_t* g[3];      // group records
+    uint64_t* r[4];      // sort records
+    uint64_t* g[5];      // group records
     uint32_t* counts;
     uint32_t* prefix;
     uint64_t* n_grp_rows;
@@ -209,9 +312,9 @@ static GbScratch gb_layout(char* base, size_t n)
         off += align_up(bytes ? bytes : 1, 256);
         return p;
     };
-    for (int i = 0; i < 3; i++)
+    for (int i = 0; i < 4; i++)
         s.r[i] = reinterpret_cast<uint64_t*>(take(np * 8));
-    for (int i = 0; i < 3; i++)
+    for (int i = 0; i < 5; i++)
         s.g[i] = reinterpret_cast<uint64_t*>(take(np * 8));
     s.counts = reinterpret_cast<uint32_t*>(take(ntc * 4));
     s.prefix = reinterpret_cast<uint32_t*>(take((ntc + 1) * 4));
@@ -302,6 +405,76 @@ static velo_status gb_run(const GbScratch& s, const GbIn& in, size_t n, size_t b
     return VELO_OK;
 }
 
+// BIGINT keys over their whole range: the same steps on wide records
+static velo_status gb_run_wide(const GbScratch& s, const GbIn& in, int n_sums, int with_count, size_t n, size_t bound,
+                               GbOut out, uint64_t* d_counts, cudaStream_t st)
+{
+    using T = GbTypesWide;
+    using Seg = T::Seg;
+    static int done[64] = {};
+    int dev = 0;
+    VELO_CUDA_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64 || !done[dev]) {
+        VELO_CUDA_TRY(cudaFuncSetAttribute(k_gbw_summary, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)Seg::SMEM_IN),
+                      "cudaFuncSetAttribute");
+        VELO_CUDA_TRY(cudaFuncSetAttribute(k_gbw_emit_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)Seg::SMEM),
+                      "cudaFuncSetAttribute");
+        if (dev >= 0 && dev < 64)
+            done[dev] = 1;
+    }
+    const size_t np = s.n_rec;
+    const int logN = ilog2_floor(np);
+    k_gb_pack_wide<<<gb_grid(np), 256, 0, st>>>(in, n_sums, n, np, s.r[0], s.r[1], s.r[2], s.r[3]);
+    VELO_CUDA_TRY(cudaGetLastError(), "group-by pack launch");
+    T::Rec::Cols rc;
+    for (int i = 0; i < 4; i++) {
+        rc.w[i] = s.r[i];
+        rc.pad[i] = ~0ull;
+    }
+    rc.pad[1] = 0; // network pads, if any, are rows left out
+    rc.mask[0] = ~0ull;
+    rc.mask[1] = ~0ull;
+    rc.mark_bit = 0;
+    rc.mark_inv = 0;
+    rc.mark_word = 1;
+    std::vector<NetPass> passes;
+    plan_sort(logN, GB_LT, GB_LMAX, passes);
+    velo_status rc2 = launch_net12<T::Rec>(rc, NetGeom { np, logN, 0 }, passes, nullptr, st);
+    if (rc2 != VELO_OK)
+        return rc2;
+    const int nts = (int)(np / SEG_TS);
+    T::Grp::Cols gc;
+    for (int i = 0; i < 5; i++) {
+        gc.w[i] = s.g[i];
+        gc.pad[i] = ~0ull;
+    }
+    gc.mask[0] = ~0ull;
+    gc.mark_bit = 63;
+    gc.mark_inv = 1;
+    gc.mark_word = 1;
+    k_gbw_summary<<<nts, SEG_THREADS, Seg::SMEM_IN, st>>>(rc, s.aggs, s.runs);
+    k_gbw_carries<<<1, 1024, 3 * 1024 * 8 + 2 * 1024 * 4, st>>>(s.aggs, s.runs, nts, s.carry, s.tail_prefix,
+                                                                s.n_groups);
+    k_gbw_emit_rows<<<nts, SEG_THREADS, Seg::SMEM, st>>>(rc, nts, s.aggs, s.carry, gc);
+    VELO_CUDA_TRY(cudaGetLastError(), "group-by aggregation launch");
+    const int ntc = (int)(np >> GB_LT);
+    k_count_marks<T::Grp><<<ntc, 256, 0, st>>>(gc, np, GB_LT, s.counts);
+    k_scan_tiles<<<1, 1024, 0, st>>>(s.counts, ntc, s.prefix, s.n_grp_rows);
+    passes.clear();
+    plan_compact(logN, GB_LT, GB_LMAX, passes);
+    rc2 = launch_net12<T::Grp>(gc, NetGeom { np, logN, 0 }, passes, s.prefix, st);
+    if (rc2 != VELO_OK)
+        return rc2;
+    GbwWords gw;
+    for (int i = 0; i < 5; i++)
+        gw.g[i] = s.g[i];
+    k_gbw_out<<<gb_grid(bound), 256, 0, st>>>(gw, bound, n_sums, with_count, out, s.n_groups, d_counts);
+    VELO_CUDA_TRY(cudaGetLastError(), "group-by output launch");
+    return VELO_OK;
+}
+
 } // namespace velo
 
 using namespace velo;
@@ -345,6 +518,8 @@ extern "C" velo_status velo_ogroupby(const void* d_keys, uint32_t key_type, cons
         out.sums[i] = d_out_sums[i];
     }
     cudaStream_t st = (cudaStream_t)stream;
+    if (key_type == VELO_BIGINT)
+        return gb_run_wide(s, in, (int)n_sums, with_count ? 1 : 0, n, group_bound, out, d_counts, st);
     if (with_count && n_sums == 0)
         return gb_run<0, 1>(s, in, n, group_bound, out, d_counts, st);
     if (with_count && n_sums == 1)

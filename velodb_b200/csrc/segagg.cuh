@@ -20,6 +20,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "trace.cuh"
 
@@ -109,6 +110,18 @@ __device__ __forceinline__ void warp_reduce_scatter32(int64_t (&a)[32], int lane
     }
 }
 
+// Group records with a separate flag word (Agg::FLAG_WORD = true): o0 = the
+// whole 64-bit out_bits(key), o1 = [63] not the last row of a valid group,
+// then the sums; otherwise the flag shares word 0 with a key of at most 63 bits.
+template <class A, class = void>
+struct SegFlagWord {
+    static constexpr bool value = false;
+};
+template <class A>
+struct SegFlagWord<A, std::void_t<decltype(A::FLAG_WORD)>> {
+    static constexpr bool value = A::FLAG_WORD;
+};
+
 // Agg: static constexpr int W (record words), V (values); struct Params
 //      (public decoding parameters passed to every pass);
 //      static uint64_t key(const uint64_t* w)      -- run key (includes validity)
@@ -119,8 +132,11 @@ template <class Agg>
 struct SegAgg {
     static constexpr int W = Agg::W;
     static constexpr int V = Agg::V;
-    // the tile area holds the W input words, later the 1+V output words
-    static constexpr int TW = W > 1 + V ? W : 1 + V;
+    // group record words of emit_rows: key (and flag), then the V sums
+    static constexpr int FW = SegFlagWord<Agg>::value ? 1 : 0;
+    static constexpr int OW = 1 + FW + V;
+    // the tile area holds the W input words, later the OW output words
+    static constexpr int TW = W > OW ? W : OW;
     using Params = typename Agg::Params;
     // emit_rows stages 1+V output words in the tile area; the other passes
     // only the W input words (smaller footprint, more CTAs per SM)
@@ -523,12 +539,12 @@ struct SegAgg {
         for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS) {
             VELO_TRACE_AT(TS_SEG_OUT, out[0] + base + i);
 #pragma unroll
-            for (int x = 0; x <= V; x++)
+            for (int x = 0; x < OW; x++)
                 out[x][base + i] = so[(size_t)x * SEG_TS_PAD + seg_slot(i)];
         }
     }
 
-    // emit_rows without the stores: leaves the tile's 1+V output words of
+    // emit_rows without the stores: leaves the tile's OW output words of
     // row i at smem word x * SEG_TS_PAD + seg_slot(i) (after a barrier)
     __device__ static void emit_stage(uint64_t* const* words, int tile, int ntiles, const SegTileAgg* aggs,
                                       const int64_t* carry_in, const Params& prm, char* smem)
@@ -611,10 +627,15 @@ struct SegAgg {
             if (r > 0)
                 lead = lead & (keys[r] == keys[r - 1]);
             const bool first_run_of_tile = (keys[r] == head_key);
-            so[seg_slot(r0 + r)] = ((uint64_t)(!tail[r]) << 63) | Agg::out_bits(keys[r]);
+            if constexpr (FW == 1) {
+                so[seg_slot(r0 + r)] = Agg::out_bits(keys[r]);
+                so[(size_t)SEG_TS_PAD + seg_slot(r0 + r)] = (uint64_t)(!tail[r]) << 63;
+            } else {
+                so[seg_slot(r0 + r)] = ((uint64_t)(!tail[r]) << 63) | Agg::out_bits(keys[r]);
+            }
 #pragma unroll
             for (int i = 0; i < V; i++)
-                so[(size_t)(1 + i) * SEG_TS_PAD + seg_slot(r0 + r)] =
+                so[(size_t)(1 + FW + i) * SEG_TS_PAD + seg_slot(r0 + r)] =
                     (uint64_t)(pref[r][i] + (lead ? cin[i] : 0) + (first_run_of_tile ? tc[i] : 0));
         }
         __syncthreads();
