@@ -341,6 +341,28 @@ __global__ void __launch_bounds__(SEG_THREADS) k_jseg_emit_topk(JRec::Cols c, in
     const uint64_t* so = reinterpret_cast<const uint64_t*>(sm);
     uint64_t* k0 = reinterpret_cast<uint64_t*>(sm + JSEG_KEYS_OFF);
     uint64_t* k1 = k0 + SEG_TS;
+    if (cand == 16) {
+        // the 16 best in registers and warp shuffles (rows 4t .. 4t + 3 of
+        // thread t), then through 2 x 128 words of shared memory
+        static_assert(SEG_TS == 4 * SEG_THREADS && SEG_THREADS == 256, "4 rows a thread, 8 warps");
+        uint64_t x0[4], x1[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int i = 4 * threadIdx.x + e;
+            topk_key(so[seg_slot(i)], so[SEG_TS_PAD + seg_slot(i)], so[2 * SEG_TS_PAD + seg_slot(i)], x0[e], x1[e]);
+        }
+        topk16_block(x0, x1, k0, TK_M1);
+        if (threadIdx.x < 4) {
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const size_t o = (size_t)blockIdx.x * 16 + 4 * threadIdx.x + e;
+                VELO_TRACE_AT(TS_TOPK, out0 + o);
+                out0[o] = x0[e];
+                out1[o] = x1[e];
+            }
+        }
+        return;
+    }
     for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS)
         topk_key(so[seg_slot(i)], so[SEG_TS_PAD + seg_slot(i)], so[2 * SEG_TS_PAD + seg_slot(i)], k0[i], k1[i]);
     topk_net<SEG_TS / 2 / SEG_THREADS>(k0, k1, SEG_TS, cand, TK_M1, false);

@@ -96,4 +96,129 @@ __device__ void topk_net(uint64_t* k0, uint64_t* k1, int n, int c, uint64_t m1, 
     }
 }
 
+// ---- top 16 of a CTA's rows in registers and warp shuffles ------------------
+// Lane l of a warp holds rows 4l .. 4l + 3 of the warp's 128 rows (x0[e],
+// x1[e] = row 4l + e).  Every exchange partner (register or lane) and every
+// direction depends only on the lane and the register, never on the data.
+
+// compare-exchange of registers a (lower row) and b
+__device__ __forceinline__ void tk_cx_reg(uint64_t& a0, uint64_t& a1, uint64_t& b0, uint64_t& b1, bool asc,
+                                          uint64_t m1)
+{
+    const bool sw = asc ? tk_gt(a0, a1, b0, b1, m1) : tk_gt(b0, b1, a0, a1, m1);
+    const uint64_t n0 = sw ? b0 : a0, n1 = sw ? b1 : a1;
+    b0 = sw ? a0 : b0;
+    b1 = sw ? a1 : b1;
+    a0 = n0;
+    a1 = n1;
+}
+
+// compare-exchange with lane ^ d: keep the smaller (keep_min) or the larger
+// of the two rows; on equal keys each lane keeps its own row
+__device__ __forceinline__ void tk_cx_lane(uint64_t& x0, uint64_t& x1, int d, bool keep_min, uint64_t m1)
+{
+    const uint64_t p0 = __shfl_xor_sync(0xFFFFFFFFu, x0, d), p1 = __shfl_xor_sync(0xFFFFFFFFu, x1, d);
+    const bool take = keep_min ? tk_gt(x0, x1, p0, p1, m1) : tk_gt(p0, p1, x0, x1, m1);
+    x0 = take ? p0 : x0;
+    x1 = take ? p1 : x1;
+}
+
+// levels j = 8, 4 (lanes ^ 2, ^ 1) and 2, 1 (registers) of a 16-row run, in
+// direction asc
+__device__ __forceinline__ void tk_merge16(uint64_t (&x0)[4], uint64_t (&x1)[4], int lane, bool asc, uint64_t m1)
+{
+#pragma unroll
+    for (int d = 2; d >= 1; d >>= 1) {
+        const bool lower = (lane & d) == 0;
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            tk_cx_lane(x0[e], x1[e], d, lower == asc, m1);
+    }
+    tk_cx_reg(x0[0], x1[0], x0[2], x1[2], asc, m1);
+    tk_cx_reg(x0[1], x1[1], x0[3], x1[3], asc, m1);
+    tk_cx_reg(x0[0], x1[0], x0[1], x1[1], asc, m1);
+    tk_cx_reg(x0[2], x1[2], x0[3], x1[3], asc, m1);
+}
+
+// Runs of 16 rows (lanes 4q .. 4q + 3 hold run q) sorted ascending for even
+// q, descending for odd q, are halved three times (lanes ^ 4, ^ 8, ^ 16: the
+// element-wise minimum of a run pair holds its 16 best rows as a bitonic
+// sequence, merged again); afterwards every 4-lane group holds the warp's 16
+// best rows ascending.
+__device__ __forceinline__ void tk_warp_rounds16(uint64_t (&x0)[4], uint64_t (&x1)[4], int lane, uint64_t m1)
+{
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        const int d = 4 << r;
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            tk_cx_lane(x0[e], x1[e], d, true, m1);
+        // the merged run's index is the lane's bits above d; even ascending
+        const bool asc = r == 2 ? true : ((lane >> (3 + r)) & 1) == 0;
+        tk_merge16(x0, x1, lane, asc, m1);
+    }
+}
+
+// Sorts the warp's runs of 16 rows, even runs ascending and odd descending
+// (bitonic phases 1..4 of the row index 4 * lane + e).
+__device__ __forceinline__ void tk_warp_runs16(uint64_t (&x0)[4], uint64_t (&x1)[4], int lane, uint64_t m1)
+{
+    // phase 1 (pairs): direction from bit 1 of the row = register bit 1
+    tk_cx_reg(x0[0], x1[0], x0[1], x1[1], true, m1);
+    tk_cx_reg(x0[2], x1[2], x0[3], x1[3], false, m1);
+    // phase 2: direction from bit 2 of the row = lane bit 0
+    {
+        const bool asc = (lane & 1) == 0;
+        tk_cx_reg(x0[0], x1[0], x0[2], x1[2], asc, m1);
+        tk_cx_reg(x0[1], x1[1], x0[3], x1[3], asc, m1);
+        tk_cx_reg(x0[0], x1[0], x0[1], x1[1], asc, m1);
+        tk_cx_reg(x0[2], x1[2], x0[3], x1[3], asc, m1);
+    }
+    // phase 3: direction from lane bit 1; level 4 across lanes ^ 1
+    {
+        const bool asc = (lane & 2) == 0;
+        const bool lower = (lane & 1) == 0;
+#pragma unroll
+        for (int e = 0; e < 4; e++)
+            tk_cx_lane(x0[e], x1[e], 1, lower == asc, m1);
+        tk_cx_reg(x0[0], x1[0], x0[2], x1[2], asc, m1);
+        tk_cx_reg(x0[1], x1[1], x0[3], x1[3], asc, m1);
+        tk_cx_reg(x0[0], x1[0], x0[1], x1[1], asc, m1);
+        tk_cx_reg(x0[2], x1[2], x0[3], x1[3], asc, m1);
+    }
+    // phase 4: direction from lane bit 2
+    tk_merge16(x0, x1, lane, (lane & 4) == 0, m1);
+}
+
+// The 16 best of the CTA's rows (4 a thread, blockDim.x = 256) ascending in
+// lanes 0..3 of warp 0 (x0/x1 of those lanes on return; other threads' rows
+// are unspecified).  scratch: 2 x 128 u64 of shared memory.
+__device__ __forceinline__ void topk16_block(uint64_t (&x0)[4], uint64_t (&x1)[4], uint64_t* scratch, uint64_t m1)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    tk_warp_runs16(x0, x1, lane, m1);
+    tk_warp_rounds16(x0, x1, lane, m1);
+    // the 8 warps' results: warp w's 16 rows to rows 16w .. 16w + 15, odd
+    // warps reversed so that neighbouring runs form bitonic sequences
+    __syncthreads();
+    if (lane < 4) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int r = 4 * lane + e;
+            const int slot = 16 * warp + ((warp & 1) ? 15 - r : r);
+            scratch[slot] = x0[e];
+            scratch[128 + slot] = x1[e];
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            x0[e] = scratch[4 * lane + e];
+            x1[e] = scratch[128 + 4 * lane + e];
+        }
+        tk_warp_rounds16(x0, x1, lane, m1);
+    }
+}
+
 } // namespace velo
