@@ -74,6 +74,9 @@ struct GbAggWide {
     __device__ __forceinline__ static uint64_t out_bits(uint64_t key) { return key; }
 };
 
+// the per-tile run and carry arrays of the scratch hold 3 values a tile
+static_assert(GbAggWide::V <= 3 && GbAgg<2, 0>::V <= 3 && GbAgg<1, 1>::V <= 3, "aggregates a tile in scratch");
+
 struct GbTypesWide {
     using Agg = GbAggWide;
     using Seg = SegAgg<Agg>;
@@ -320,8 +323,10 @@ static GbScratch gb_layout(char* base, size_t n)
     s.prefix = reinterpret_cast<uint32_t*>(take((ntc + 1) * 4));
     s.n_grp_rows = reinterpret_cast<uint64_t*>(take(8));
     s.aggs = reinterpret_cast<SegTileAgg*>(take(nts * sizeof(SegTileAgg)));
-    s.runs = reinterpret_cast<int64_t*>(take(nts * 2 * 8));
-    s.carry = reinterpret_cast<int64_t*>(take(nts * 2 * 8));
+    // per tile: one value per aggregate (at most 3: the BIGINT path's
+    // count and two sums)
+    s.runs = reinterpret_cast<int64_t*>(take(nts * 3 * 8));
+    s.carry = reinterpret_cast<int64_t*>(take(nts * 3 * 8));
     s.tail_prefix = reinterpret_cast<uint32_t*>(take(nts * 4));
     s.n_groups = reinterpret_cast<uint64_t*>(take(8));
     s.rejected = reinterpret_cast<unsigned long long*>(take(8));

@@ -329,41 +329,50 @@ struct Net {
     // Pair (l, l + 2^b) inside block S; the block's offset is P[S] mod 2^(b+1)
     // and its left-half mark count is P[S + 2^b] - P[S] (P = exclusive prefix
     // of the original marks; block counts are invariant under the
-    // permutations of lower levels).
+    // permutations of lower levels).  Level b is register bit Q of layout s
+    // (b = s + Q): the registers whose bits above Q agree lie in one block, so
+    // each of the thread's E >> (Q + 1) blocks is looked up once and its
+    // 2^Q pairs share the offset, the count and the threshold.
     template <int Q>
     __device__ __forceinline__ static void compact_level_tile(R (&v)[E], const Cols& c, int s, int b, uint32_t p_tile,
                                                               const uint32_t* pre)
     {
         const int tp = tidpart(s);
         const uint32_t half = 1u << b;
+        const int tblk = tp & ~(int)(2 * half - 1); // the thread's bits above b
+        const uint32_t ti = (uint32_t)tp & (half - 1u); // its bits below b (all below s)
+        constexpr int NB = E >> (Q + 1);
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            if (e & (1 << Q))
-                continue;
-            const int e2 = e | (1 << Q);
-            const int l = tp | (e << s);
-            const int blk = l & ~(int)(2 * half - 1);
-            const uint32_t ps = p_tile + pre[ppos(blk)];
-            bool sw;
+        for (int hb = 0; hb < NB; hb++) {
+            const int blk = tblk | (hb << (b + 1));
+            const uint32_t pb = pre[ppos(blk)];
+            const uint32_t ps = p_tile + pb;
             if (b == 0) {
-                // compact_offset, n == 2 (algorithms.c:123-128)
+                // compact_offset, n == 2 (algorithms.c:123-128): one pair a block
+                const int e = hb << 1, e2 = e | 1;
                 const bool ml = MarkOf<R>::get(v[e], c), mr = MarkOf<R>::get(v[e2], c);
-                sw = ((!ml) & mr) != ((ps & 1u) == 1u);
+                R::cswap(v[e], v[e2], ((!ml) & mr) != ((ps & 1u) == 1u));
             } else {
                 // compact_offset, n > 2 (algorithms.c:130-152)
-                const uint32_t left = pre[ppos(blk + (int)half)] - pre[ppos(blk)];
+                const uint32_t left = pre[ppos(blk + (int)half)] - pb;
                 const uint32_t off = ps & (2 * half - 1);
-                const uint32_t i = (uint32_t)(l - blk);
                 const bool sb = (((off & (half - 1)) + left) >= half) != (off >= half);
-                sw = sb != (i >= ((off + left) & (half - 1)));
+                const uint32_t thr = (off + left) & (half - 1);
+#pragma unroll
+                for (int lo = 0; lo < (1 << Q); lo++) {
+                    const int e = (hb << (Q + 1)) | lo, e2 = e | (1 << Q);
+                    const uint32_t i = ti | ((uint32_t)lo << s);
+                    R::cswap(v[e], v[e2], sb != (i >= thr));
+                }
             }
-            R::cswap(v[e], v[e2], sw);
         }
     }
 
     // `gpre[m]` holds P at the tile whose bits b_lo..b_hi are m (the CTA's
     // other tile bits fixed, its bits below b_lo zero): every block start and
-    // block middle of a global level is such a tile boundary.
+    // block middle of a global level is such a tile boundary.  Global level b
+    // is register bit Q of layout s, so as in the tile levels the thread's
+    // E >> (Q + 1) blocks are looked up once each.
     template <int Q>
     __device__ __forceinline__ static void compact_level_global(R (&v)[E], const Cols& c, int s, int b,
                                                                 const uint32_t* gpre, int C, int b_lo,
@@ -377,22 +386,25 @@ struct Net {
         const uint32_t mmask = (1u << L) - 1u;
         const uint32_t cb = (uint32_t)cta_bits;
         const uint32_t cm = (1u << C) - 1u;
+        constexpr int NB = E >> (Q + 1);
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            if (e & (1 << Q))
-                continue;
-            const int e2 = e | (1 << Q);
-            const uint32_t l = tp | ((uint32_t)e << s);
-            const uint32_t g = (l & cm) | ((l >> C) << b_lo) | cb;
-            const uint32_t mb = ((g & ~bm) >> b_lo) & mmask;
+        for (int hb = 0; hb < NB; hb++) {
+            // the block of the block's first pair
+            const uint32_t l0 = tp | ((uint32_t)(hb << (Q + 1)) << s);
+            const uint32_t g0 = (l0 & cm) | ((l0 >> C) << b_lo) | cb;
+            const uint32_t mb = ((g0 & ~bm) >> b_lo) & mmask;
             const uint32_t ps = gpre[mb];
-            const uint32_t pm = gpre[mb | (1u << (b - b_lo))];
-            const uint32_t left = pm - ps;
+            const uint32_t left = gpre[mb | (1u << (b - b_lo))] - ps;
             const uint32_t off = ps & bm;
-            const uint32_t i = g & bm;
             const bool sb = (((off & (half - 1u)) + left) >= half) != (off >= half);
-            const bool sw = sb != (i >= ((off + left) & (half - 1u)));
-            R::cswap(v[e], v[e2], sw);
+            const uint32_t thr = (off + left) & (half - 1u);
+#pragma unroll
+            for (int lo = 0; lo < (1 << Q); lo++) {
+                const int e = (hb << (Q + 1)) | lo, e2 = e | (1 << Q);
+                const uint32_t l = tp | ((uint32_t)e << s);
+                const uint32_t g = (l & cm) | ((l >> C) << b_lo) | cb;
+                R::cswap(v[e], v[e2], sb != ((g & bm) >= thr));
+            }
         }
     }
 
