@@ -45,28 +45,56 @@ struct SegTileAgg {
 };
 
 // Block-wide inclusive segmented scan (flag = "a new run starts at this
-// thread's first row"; the operator resets at flags).  V int64 values.
+// thread's first row"; the operator resets at flags).  V int64 values.  Warp
+// shuffles scan each warp; the warps' totals go through shared memory
+// (sm_vals[i * 32 + warp], sm_flags[warp]) and each thread adds the carry
+// of the warps before its own.  Ends with a barrier, so the caller may reuse
+// sm_vals at once.
 template <int V>
 __device__ __forceinline__ void block_seg_scan(bool& flag, int64_t (&x)[V], int64_t* sm_vals, uint32_t* sm_flags)
 {
-    const int t = threadIdx.x;
-    for (int off = 1; off < SEG_THREADS; off <<= 1) {
-        __syncthreads();
-        sm_flags[t] = flag ? 1u : 0u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    bool f = flag;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        int64_t y[V];
 #pragma unroll
         for (int i = 0; i < V; i++)
-            sm_vals[i * SEG_THREADS + t] = x[i];
-        __syncthreads();
-        if (t >= off) {
-            const bool pf = sm_flags[t - off] != 0;
-            if (!flag) {
+            y[i] = __shfl_up_sync(0xFFFFFFFFu, x[i], off);
+        const bool fy = __shfl_up_sync(0xFFFFFFFFu, f ? 1 : 0, off) != 0;
+        if (lane >= off) {
 #pragma unroll
-                for (int i = 0; i < V; i++)
-                    x[i] += sm_vals[i * SEG_THREADS + t - off];
-            }
-            flag = flag | pf;
+            for (int i = 0; i < V; i++)
+                x[i] = f ? x[i] : x[i] + y[i];
+            f = f | fy;
         }
     }
+    __syncthreads(); // the caller may still read sm_vals
+    if (lane == 31) {
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            sm_vals[i * 32 + warp] = x[i];
+        sm_flags[warp] = f ? 1u : 0u;
+    }
+    __syncthreads();
+    // the inclusive value at the end of the previous warp (the warp index is
+    // public, so the loop bound is too)
+    int64_t c[V];
+#pragma unroll
+    for (int i = 0; i < V; i++)
+        c[i] = 0;
+    bool cf = false;
+    for (int w = 0; w < warp; w++) {
+        const bool fw = sm_flags[w] != 0;
+#pragma unroll
+        for (int i = 0; i < V; i++)
+            c[i] = fw ? sm_vals[i * 32 + w] : c[i] + sm_vals[i * 32 + w];
+        cf = cf | fw;
+    }
+#pragma unroll
+    for (int i = 0; i < V; i++)
+        x[i] = f ? x[i] : x[i] + c[i];
+    flag = f | cf;
     __syncthreads();
 }
 
@@ -494,6 +522,9 @@ struct SegAgg {
 #pragma unroll
             for (int q = 0; q < 32; q++)
                 acc[q] = 0;
+            // the ranks of a thread's tails are distinct, so each slot takes
+            // at most one of its rows: a select, not an add (the block sum
+            // below adds the threads' slots, all but one zero)
             uint32_t rank = rank0;
 #pragma unroll
             for (int r = 0; r < SEG_RPT; r++) {
@@ -501,10 +532,10 @@ struct SegAgg {
 #pragma unroll
                 for (int jj = 0; jj < 4; jj++) {
                     const bool hit = tail[r] & (rank == (uint32_t)(j0 + jj));
-                    acc[jj * 8] += hit ? kv : 0;
+                    acc[jj * 8] = hit ? kv : acc[jj * 8];
 #pragma unroll
                     for (int i = 0; i < V; i++)
-                        acc[jj * 8 + 1 + i] += hit ? pref[r][i] : 0;
+                        acc[jj * 8 + 1 + i] = hit ? pref[r][i] : acc[jj * 8 + 1 + i];
                 }
                 rank += tail[r] ? 1u : 0u;
             }
