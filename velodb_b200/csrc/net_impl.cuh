@@ -16,18 +16,30 @@ namespace velo {
 template <class R, int LOG_NT>
 constexpr int net_min_blocks() { return LOG_NT <= 8 ? 2 : 1; }
 // rows of at most 12 bytes, and two-word records keyed on 32 bits (the
-// group-by's: 2^23-row sort 1.78 -> 1.63 ms); two-word records compared on a
-// whole word need their 128 registers (measured 1 % slower at 85)
+// group-by's: 2^23-row sort 1.78 -> 1.63 ms), in both the in-tile and the
+// global kernels.  Two-word records compared on a whole word (the join's
+// union) only in the global kernel: their in-tile passes need 128 registers
+// (2^23 union sort: tile 353 -> 390 us at 85), while their global passes gain
+// from the third CTA (56.4 -> 53.2 us a pass).
 template <class R>
 struct NetWide {
     static constexpr bool ok = sizeof(R) <= 12;
+    static constexpr bool ok_global = ok;
 };
 template <bool S>
 struct NetWide<RowRec<2, 1, S, KEY_HI32>> {
     static constexpr bool ok = true;
+    static constexpr bool ok_global = true;
+};
+template <bool S>
+struct NetWide<RowRec<2, 1, S, KEY_FULL>> {
+    static constexpr bool ok = false;
+    static constexpr bool ok_global = true;
 };
 template <class R, int LOG_NT>
 constexpr bool net_has_wide() { return LOG_NT <= 8 && NetWide<R>::ok; }
+template <class R, int LOG_NT>
+constexpr bool net_has_wide_global() { return LOG_NT <= 8 && NetWide<R>::ok_global; }
 constexpr int NET_WIDE_LOGN = 21; // sorts of 2^21 rows and more take the three-CTA form
 
 // Passes of one sequence are launched with programmatic stream serialization:
@@ -127,10 +139,12 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
     const bool compact = passes[0].kind == P_COMPACT_TILE || passes[0].kind == P_COMPACT_GLOBAL;
     constexpr int MB = net_min_blocks<R, LOG_NT>();
     constexpr int MBW = net_has_wide<R, LOG_NT>() ? 3 : MB;
+    constexpr int MBG = net_has_wide_global<R, LOG_NT>() ? 3 : MB;
     const bool wide = MBW != MB && g.logN >= NET_WIDE_LOGN;
+    const bool wide_g = MBG != MB && g.logN >= NET_WIDE_LOGN;
     auto k_local = wide ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_LOCAL, MBW> : k_sort_pass<R, LOG_NT, LOG_E, N::PK_LOCAL, MB>;
-    auto k_global = wide ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MBW>
-                         : k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MB>;
+    auto k_global = wide_g ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MBG>
+                           : k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MB>;
     auto k_comp = k_compact_pass<R, LOG_NT, LOG_E>;
     const size_t smem = compact ? N::smem_bytes_compact() : N::smem_bytes_sort();
     if (smem > MAX_SMEM_BYTES)
@@ -139,7 +153,7 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
     velo_status rc = compact ? ensure_smem(k_comp, MAX_SMEM_BYTES, done_compact)
                              : ensure_smem(k_local, MAX_SMEM_BYTES, done_local[wide ? 1 : 0]);
     if (rc == VELO_OK && !compact)
-        rc = ensure_smem(k_global, MAX_SMEM_BYTES, done_global[wide ? 1 : 0]);
+        rc = ensure_smem(k_global, MAX_SMEM_BYTES, done_global[wide_g ? 1 : 0]);
     if (rc != VELO_OK)
         return rc;
     const int lt = N::LT;
