@@ -576,7 +576,10 @@ struct Net {
             }
         }
 
-        if (s < 5) {
+        // stores need 32 consecutive rows a warp, or (global passes) the
+        // layout the rows were loaded in: there the lanes cover whole
+        // 2^C-row segments, which are whole lines of every word array
+        if (s < 5 && !(is_global && s == smin)) {
             transpose<CT, BOFF>(v, s, S0, sm);
             s = S0;
         }
