@@ -583,15 +583,42 @@ typedef struct velo_cmd {
 
 typedef struct velo_ctx velo_ctx;
 
+/* velo_config.flags */
+#define VELO_QUEUE_PERSISTENT 1u /* commands run on a persistent device-side consumer */
+
+/* velo_cmd.flags: with VELO_QUEUE_PERSISTENT, the command need not wait for
+ * the commands submitted before it (it may run beside them) */
+#define VELO_CMD_UNORDERED 0x100u
+
 typedef struct velo_config {
     int32_t device;          /* CUDA device ordinal */
     uint32_t queue_capacity; /* tickets in flight before submit waits (0 = 1024) */
+    uint32_t flags;          /* VELO_QUEUE_PERSISTENT or 0 */
+    uint32_t idle_us;        /* persistent consumer: idle time before it exits (0 = 1000 us) */
 } velo_config;
 
-/* Creates a context: a non-blocking stream on `device` and a ring of
- * completion events (replaces TaskManager::start, which launches a
- * cooperative persistent kernel that polls a host-mapped ring forever; here
- * nothing runs while the queue is empty). */
+/* Creates a context on `device` (replaces TaskManager::start,
+ * src/cuda/task_manager.cu:26-78).
+ *
+ * Default: a non-blocking stream and a ring of completion events; each
+ * command is dispatched to its kernels on the stream; nothing runs while the
+ * queue is empty.
+ *
+ * VELO_QUEUE_PERSISTENT: like the reference, a persistent kernel consumes
+ * the commands from a host-mapped ring (src/cuda/persistent_kernel.cu:76-124),
+ * but every command is planned on the host into a job of tile-sized work
+ * items, and several jobs run at once: the consumer's CTAs claim items of
+ * all published jobs in publication order, each item waiting (bounded) only
+ * for the earlier steps of its own job.  Commands keep submission order
+ * unless they carry VELO_CMD_UNORDERED; a velo_batch_submit batch runs
+ * unordered among itself.  The consumer exits after idle_us without work and
+ * is relaunched by the next submission or wait; while it runs it holds the
+ * SMs, so work on other streams shares the GPU with it.  The queue is not
+ * ordered after work on other streams: a command's inputs (and buffers that
+ * other streams fill) must be complete before it is submitted.  Opcodes:
+ * NOP, PERMUTE, SCATTER, GATHER, COMPARE_EQ, COMPOSE_POSITION_MAP,
+ * ENRICH_POSITIONS, OSORT_KP, OCOMPACT_KPM, OSHUFFLE, OJOIN_PKFK, OGATHER,
+ * FILTER_GROUPBY, JOIN_GROUPBY_TOPK; the others return VELO_ENOTSUP. */
 velo_status velo_init(const velo_config* config, velo_ctx** out);
 /* Waits up to timeout_ms for outstanding commands, then releases the
  * context.  Never resets the device (the reference calls cudaDeviceReset on
@@ -601,9 +628,12 @@ velo_status velo_shutdown(velo_ctx* ctx, uint32_t timeout_ms);
 /* Enqueues one command; *ticket identifies its completion.  Thread-safe
  * (the reference's push is single-producer, src/cuda/commands.cpp:47-67). */
 velo_status velo_submit(velo_ctx* ctx, const velo_cmd* cmd, uint64_t* ticket);
-/* Enqueues n commands; the VELO_OP_OSORT_KP / VELO_OP_OCOMPACT_KPM commands
- * among them run as ONE persistent batched launch (velo_batch_*), the others
- * in order after it.  tickets[i] completes with the whole submission. */
+/* Enqueues n commands.  Stream queue: the VELO_OP_OSORT_KP /
+ * VELO_OP_OCOMPACT_KPM commands among them run as ONE persistent batched
+ * launch (velo_batch_*), the others in order after it, and tickets[i]
+ * completes with the whole submission.  Persistent queue: every command is a
+ * job of its own, the batch's jobs run beside each other after the commands
+ * submitted before the batch, and tickets[i] completes with command i. */
 velo_status velo_batch_submit(velo_ctx* ctx, const velo_cmd* cmds, size_t n, uint64_t* tickets);
 /* Waits for a ticket, at most timeout_ns (VELO_ETIMEDOUT instead of
  * spinning forever, cf. src/cuda/commands.cpp:69-91). */
@@ -615,6 +645,10 @@ velo_status velo_last_error(velo_ctx* ctx, char* buf, size_t len);
 void* velo_ctx_stream(velo_ctx* ctx);
 /* sizeof(velo_cmd), for bindings that lay out command arrays themselves. */
 size_t velo_cmd_size(void);
+/* Launches of a persistent context's consumer kernel so far (the first one
+ * and every relaunch after an idle exit); 0 for a stream context.  No
+ * reference counterpart (the reference's kernel never exits). */
+uint64_t velo_ctx_launches(velo_ctx* ctx);
 
 /* ------------------------------------------------------------------------ */
 /* Serving layer: continuous admission of queries over resident tables      */
@@ -664,10 +698,15 @@ typedef struct velo_query_result {
     uint64_t counts[2];
 } velo_query_result;
 
+/* velo_server_config.flags */
+#define VELO_SERVE_PERSISTENT 1u /* queries run as jobs of one persistent command queue */
+
 typedef struct velo_server_config {
     int32_t device;
-    uint32_t slots;            /* queries on the device at once (one stream each), 1..64 */
+    uint32_t slots;            /* queries on the device at once (one stream or job each), 1..64 */
     uint64_t hbm_budget_bytes; /* arena for all in-flight queries' scratch, allocated once */
+    uint32_t flags;            /* VELO_SERVE_PERSISTENT or 0 (per-slot streams) */
+    uint32_t idle_us;          /* persistent queue: idle time before its consumer exits (0 = 1000 us) */
 } velo_server_config;
 
 typedef struct velo_server_stats_t {
@@ -678,7 +717,10 @@ typedef struct velo_server velo_server;
 
 /* Starts the request loop.  Queries are admitted in arrival order whenever a
  * slot is free and their scratch fits in the budget; admitted queries run
- * concurrently on their own streams.  With slots = 1 the server runs one
+ * concurrently on their own streams, or with VELO_SERVE_PERSISTENT as jobs
+ * of one persistent command queue (see velo_init), whose consumer runs the
+ * work items of every admitted query as they become ready and copies each
+ * result straight into host memory.  With slots = 1 the server runs one
  * query at a time (the plain path). */
 velo_status velo_server_create(const velo_server_config* cfg, const velo_served_tables* tables, velo_server** out);
 /* Thread-safe; returns immediately with the query id. */

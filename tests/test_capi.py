@@ -66,8 +66,13 @@ def test_compact_scratch_size():
     small = L.velo_compact_scratch_bytes(1000, None)
     big = L.velo_compact_scratch_bytes(1 << 23, None)
     assert 0 < small <= big
-    # one u32 count and one u32 prefix per 8192-row tile, 256-byte aligned
-    assert big == 2 * ((1 << 10) * 4) + 256
+    # one u32 count and one u32 prefix per 4096-row tile (the persistent
+    # queue's tiles; the plain path's 8192-row tiles need half), 256-byte
+    # aligned
+    assert big == 2 * ((1 << 11) * 4) + 256
+    # with an explicit tune: that tune's tiles only (8192 rows here)
+    t = _lib.VeloTune(13, 512)
+    assert L.velo_compact_scratch_bytes(1 << 23, C.byref(t)) == 2 * ((1 << 10) * 4) + 256
 
 
 def test_queue_init_without_device_fails_cleanly():

@@ -30,6 +30,23 @@ def test_results_identical_alone_and_in_the_mix(tables):
         assert S.result_key(a) == S.result_key(m)
 
 
+def test_persistent_queue_results_identical_alone_and_in_the_mix(tables):
+    # the same stream served through one persistent command queue: every
+    # query's result equals its result alone on the stream path
+    qs = S.query_stream(tables, 40, seed=6, lo_log2=10, hi_log2=17)
+    alone = S.Server(tables, slots=1, budget_bytes=2 << 30)
+    ra, _ = S.run_closed_one_at_a_time(alone, qs)
+    alone.close()
+    mix = S.Server(tables, slots=16, budget_bytes=2 << 30, persistent=True)
+    rm, _ = S.run_open_loop(mix, qs, np.zeros(len(qs)))
+    st = mix.stats()
+    mix.close()
+    assert st["peak_inflight"] > 1
+    for a, m in zip(ra, rm):
+        assert a.status == 0 and m.status == 0
+        assert S.result_key(a) == S.result_key(m)
+
+
 def test_results_match_oracle(tables, orc):
     qs = [q for q in S.query_stream(tables, 12, seed=9, lo_log2=12, hi_log2=16)]
     srv = S.Server(tables, slots=4, budget_bytes=1 << 30)

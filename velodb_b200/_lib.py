@@ -71,6 +71,7 @@ PROTOS = {
     "velo_last_error": (i32, [vp, vp, sz]),
     "velo_ctx_stream": (vp, [vp]),
     "velo_cmd_size": (sz, []),
+    "velo_ctx_launches": (u64, [vp]),
     "velo_server_create": (i32, [vp, vp, vp]),
     "velo_server_submit": (i32, [vp, vp, vp]),
     "velo_server_wait": (i32, [vp, u64, u64, vp]),
@@ -172,6 +173,13 @@ class VeloCmdArgs(C.Union):
         ("ojoin", _args(vp, vp, sz, vp, vp, sz, u32, vp, vp, vp, vp, sz)),
         ("ojoin_mn", _args(vp, vp, sz, vp, vp, sz, u32, sz, vp, vp, vp, vp, sz)),
         ("ohash", _args(vp, vp, sz, vp, vp, sz, u32, u64, vp, vp, vp, vp, sz)),
+        ("scatter", _args(vp, sz, vp, vp, vp, sz)),
+        ("gather", _args(vp, vp, vp, vp, sz, u32)),
+        ("compose", _args(vp, vp, vp, sz)),
+        ("enrich", _args(vp, vp, vp, sz)),
+        ("oshuffle", _args(vp, sz, u64, u64, vp, sz)),
+        ("filter_groupby", _args(vp, sz, vp, u32, vp, vp, vp, sz)),
+        ("join_topk", _args(vp, vp, u32, vp, vp, vp, sz)),
     ]
 
 
@@ -180,7 +188,8 @@ class VeloCmd(C.Structure):
 
 
 class VeloConfig(C.Structure):
-    _fields_ = [("device", C.c_int32), ("queue_capacity", C.c_uint32)]
+    _fields_ = [("device", C.c_int32), ("queue_capacity", C.c_uint32), ("flags", C.c_uint32),
+                ("idle_us", C.c_uint32)]
 
 
 OP = dict(NOP=0, SCATTER=1, GATHER=2, SORT=3, PERMUTE=4, COMPARE_EQ=10, COMPOSE_POSITION_MAP=11, ENRICH_POSITIONS=12,
@@ -206,7 +215,8 @@ class VeloQueryResult(C.Structure):
 
 
 class VeloServerConfig(C.Structure):
-    _fields_ = [("device", C.c_int32), ("slots", C.c_uint32), ("hbm_budget_bytes", C.c_uint64)]
+    _fields_ = [("device", C.c_int32), ("slots", C.c_uint32), ("hbm_budget_bytes", C.c_uint64),
+                ("flags", C.c_uint32), ("idle_us", C.c_uint32)]
 
 
 class VeloServerStats(C.Structure):

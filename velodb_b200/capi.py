@@ -417,3 +417,91 @@ def ogroupby(keys: torch.Tensor, key_type: int, n: int, sums=(), with_count: boo
                               out_counts.data_ptr() if out_counts is not None else None, counts.data_ptr(),
                               scratch.data_ptr(), scratch.numel(), _stream(stream)), "velo_ogroupby")
     return out_keys, out_sums, out_counts, counts
+
+
+# ---- command queue (velo_init / velo_submit / velo_wait) ----------------------------
+
+QUEUE_PERSISTENT = 1
+CMD_UNORDERED = 0x100
+
+
+def make_cmd(opcode: str, *fields, flags: int = 0):
+    """A velo_cmd for `opcode` (a key of _lib.OP) with the union member's
+    fields in declaration order (pointers as ints or tensors)."""
+    from ._lib import OP, VeloCmd
+
+    member = {"OSORT_KP": "osort_kp", "OCOMPACT_KPM": "ocompact_kpm", "PERMUTE": "permute", "GATHER": "gather",
+              "COMPARE_EQ": "compare_eq", "COMPOSE_POSITION_MAP": "compose", "ENRICH_POSITIONS": "enrich",
+              "SCATTER": "scatter", "OSHUFFLE": "oshuffle", "OJOIN_PKFK": "ojoin", "OGATHER": "ogather",
+              "FILTER_GROUPBY": "filter_groupby", "JOIN_GROUPBY_TOPK": "join_topk", "OJOIN_MN": "ojoin_mn",
+              "OHASH_JOIN": "ohash"}.get(opcode)
+    m = VeloCmd()
+    m.opcode = OP[opcode]
+    m.flags = flags
+    if member is not None:
+        a = getattr(m.args, member)
+        for i, v in enumerate(fields):
+            if torch.is_tensor(v):
+                v = v.data_ptr()
+            setattr(a, f"f{i}", 0 if v is None else v)
+    return m
+
+
+class Queue:
+    """A command queue context (velo_init): the stream queue, or with
+    persistent=True the persistent device consumer.  The queue is not ordered
+    after torch's streams: tensors a command reads or writes must be ready
+    (e.g. torch.cuda.synchronize()) before it is submitted."""
+
+    def __init__(self, device: int = 0, persistent: bool = False, idle_us: int = 0, capacity: int = 0):
+        import ctypes as C
+
+        from ._lib import VeloConfig
+
+        self._c = C.c_void_p()
+        cfg = VeloConfig(device, capacity, QUEUE_PERSISTENT if persistent else 0, idle_us)
+        check(lib().velo_init(C.byref(cfg), C.byref(self._c)), "velo_init")
+
+    def submit(self, cmd) -> int:
+        import ctypes as C
+
+        t = C.c_uint64()
+        check(lib().velo_submit(self._c, C.byref(cmd), C.byref(t)), "velo_submit")
+        return t.value
+
+    def submit_raw(self, cmd) -> int:
+        """velo_submit's status, for tests of rejected commands."""
+        import ctypes as C
+
+        t = C.c_uint64()
+        return int(lib().velo_submit(self._c, C.byref(cmd), C.byref(t)))
+
+    def submit_batch(self, cmds) -> list:
+        import ctypes as C
+
+        from ._lib import VeloCmd
+
+        arr = (VeloCmd * len(cmds))(*cmds)
+        tix = (C.c_uint64 * len(cmds))()
+        check(lib().velo_batch_submit(self._c, arr, len(cmds), tix), "velo_batch_submit")
+        return list(tix)
+
+    def wait(self, ticket: int, timeout_s: float = 30.0) -> None:
+        check(lib().velo_wait(self._c, ticket, int(timeout_s * 1e9)), "velo_wait")
+
+    def wait_raw(self, ticket: int, timeout_ns: int) -> int:
+        return int(lib().velo_wait(self._c, ticket, timeout_ns))
+
+    def launches(self) -> int:
+        return int(lib().velo_ctx_launches(self._c))
+
+    def close(self, timeout_ms: int = 30_000) -> None:
+        if self._c:
+            c, self._c = self._c, None
+            check(lib().velo_shutdown(c, timeout_ms), "velo_shutdown")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -21,27 +21,6 @@ namespace velo {
 using ColRec = RowRec<3, 1, false>;
 constexpr int COL_LT = 12; // 4096-row tiles (CTA shape per record width: Tile12)
 
-static int type_bytes(uint32_t t)
-{
-    switch (t) {
-    case VELO_BOOLEAN:
-    case VELO_TINYINT:
-        return 1;
-    case VELO_SMALLINT:
-        return 2;
-    case VELO_INTEGER:
-    case VELO_FLOAT:
-    case VELO_DATE:
-        return 4;
-    case VELO_BIGINT:
-    case VELO_DOUBLE:
-    case VELO_VARCHAR:
-        return 8;
-    default:
-        return 0;
-    }
-}
-
 __device__ __forceinline__ uint64_t load_bits(const void* p, int bytes, size_t i)
 {
     switch (bytes) {

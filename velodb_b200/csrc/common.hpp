@@ -48,6 +48,28 @@ inline size_t next_pow2(size_t x)
     return x + 1;
 }
 
+// bytes of one value of a velo_type (0: not a fixed-width type)
+inline int type_bytes(uint32_t t)
+{
+    switch (t) {
+    case VELO_BOOLEAN:
+    case VELO_TINYINT:
+        return 1;
+    case VELO_SMALLINT:
+        return 2;
+    case VELO_INTEGER:
+    case VELO_FLOAT:
+    case VELO_DATE:
+        return 4;
+    case VELO_BIGINT:
+    case VELO_DOUBLE:
+    case VELO_VARCHAR:
+        return 8;
+    default:
+        return 0;
+    }
+}
+
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Largest supported padded size: the mark prefix counts are u32.

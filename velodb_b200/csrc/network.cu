@@ -160,7 +160,12 @@ extern "C" size_t velo_compact_scratch_bytes(size_t capacity, const velo_tune* t
     int log_nt = 9, log_e = 4;
     if (resolve_tune(tune, 9, 4, &log_nt, &log_e) != VELO_OK)
         return 0;
-    return compact_scratch_for(capacity, log_nt + log_e);
+    const size_t b = compact_scratch_for(capacity, log_nt + log_e);
+    if (tune && tune->tile_log2 != 0)
+        return b;
+    // the default also covers the persistent command queue's 4096-row tiles
+    const size_t q = compact_scratch_for(capacity, 12);
+    return b > q ? b : q;
 }
 
 extern "C" velo_status velo_ocompact_kpm(uint64_t* d_keys, uint32_t* d_payload, uint8_t* d_marks, size_t n,

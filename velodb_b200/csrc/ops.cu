@@ -6,30 +6,9 @@
 //   oblivious:   position-map shuffle (device PRF + bitonic network),
 //                oblivious gather (union sort + fill + sort back),
 //                PK-FK equi-join producing (build rowid, probe rowid) pairs
-#include "union.cuh"
+#include "ops.cuh"
 
 namespace velo {
-
-static int type_bytes(uint32_t t)
-{
-    switch (t) {
-    case VELO_BOOLEAN:
-    case VELO_TINYINT:
-        return 1;
-    case VELO_SMALLINT:
-        return 2;
-    case VELO_INTEGER:
-    case VELO_FLOAT:
-    case VELO_DATE:
-        return 4;
-    case VELO_BIGINT:
-    case VELO_DOUBLE:
-    case VELO_VARCHAR:
-        return 8;
-    default:
-        return 0;
-    }
-}
 
 static unsigned grid_for(size_t n)
 {
@@ -37,255 +16,97 @@ static unsigned grid_for(size_t n)
     return (unsigned)(b < 148 * 16 ? (b ? b : 1) : 148 * 16);
 }
 
-#define VELO_GRID_STRIDE(i, n)                                                                                         \
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; VELO_GRID_COND(i, (n));                          \
-         i += (size_t)gridDim.x * blockDim.x)
-
 // ---------------------------------------------------------------------------
-// compat operators (include/cuda/permute.cuh:24-40, gather.cuh:28-45,
-// scatter.cuh:16-81, compare.cuh:25-91, oblivious_shuffle.cuh:10-34)
+// kernels of the plain path: each runs the body of ops.cuh / union.cuh over
+// its grid
 // ---------------------------------------------------------------------------
 
 template <typename T>
 __global__ void k_permute(T* out, const T* in, const int64_t* idx, size_t n)
 {
-    VELO_GRID_STRIDE(i, n)
-    out[i] = in[idx[i]];
+    permute_body(out, in, idx, n, blockIdx.x, gridDim.x);
 }
 
 template <typename T>
 __global__ void k_gather(T* out, const T* in, const int32_t* idx, const uint8_t* mask, size_t n)
 {
-    VELO_GRID_STRIDE(i, n)
-    {
-        if (mask == nullptr || mask[i] != 0)
-            out[idx[i]] = in[i];
-    }
+    gather_body(out, in, idx, mask, n, blockIdx.x, gridDim.x);
 }
 
 template <typename T>
 __global__ void k_compare_eq(const T* l, const T* r, uint8_t* out, size_t n)
 {
-    VELO_GRID_STRIDE(i, n)
-    out[i] = (l[i] == r[i]) ? 1 : 0;
+    compare_eq_body(l, r, out, n, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_fill_u8(uint8_t* out, uint8_t v, size_t n)
 {
-    VELO_GRID_STRIDE(i, n)
-    out[i] = v;
+    fill_u8_body(out, v, n, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_compose(const uint32_t* old_map, const uint32_t* sigma, uint32_t* new_map, size_t n)
 {
-    VELO_GRID_STRIDE(i, n)
-    new_map[i] = old_map[sigma[i]];
+    compose_body(old_map, sigma, new_map, n, blockIdx.x, gridDim.x);
 }
 
-// stable scatter: per-tile kept counts, their scan, then ranks
-constexpr int SC_LT = 11;
 __global__ void __launch_bounds__(256) k_scatter_count(const uint8_t* mask, size_t n, uint32_t* counts)
 {
     __shared__ uint32_t tmp[33];
-    const size_t base = (size_t)blockIdx.x << SC_LT;
-    uint32_t c = 0;
-    for (int i = threadIdx.x; i < (1 << SC_LT); i += blockDim.x) {
-        const size_t g = base + i;
-        c += (g < n && mask[g] != 0) ? 1u : 0u;
-    }
-    uint32_t total;
-    block_exclusive_scan(c, tmp, &total);
-    if (threadIdx.x == 0)
-        counts[blockIdx.x] = total;
+    scatter_count_tile(mask, n, counts, blockIdx.x, tmp);
 }
 
 __global__ void __launch_bounds__(256) k_scatter_write(const uint8_t* mask, size_t n, const uint32_t* prefix,
                                                        int32_t* out_idx)
 {
     __shared__ uint32_t tmp[33];
-    // each thread owns 8 consecutive rows of the 2048-row tile
-    const size_t base = ((size_t)blockIdx.x << SC_LT) + (size_t)threadIdx.x * 8;
-    uint32_t m[8], c = 0;
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-        const size_t g = base + r;
-        m[r] = (g < n && mask[g] != 0) ? 1u : 0u;
-        c += m[r];
-    }
-    uint32_t total;
-    uint32_t rank = prefix[blockIdx.x] + block_exclusive_scan(c, tmp, &total);
-#pragma unroll
-    for (int r = 0; r < 8; r++) {
-        const size_t g = base + r;
-        if (m[r])
-            out_idx[g] = (int32_t)rank;
-        rank += m[r];
-    }
+    scatter_write_tile(mask, n, prefix, out_idx, blockIdx.x, tmp);
 }
 
 __global__ void k_shuffle_pack(const uint32_t* map, size_t n, size_t np, uint64_t counter, uint64_t key, uint64_t* k,
                                uint32_t* p)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_shuffle_pack"));
-    VELO_GRID_STRIDE(i, np)
-    {
-        k[i] = i < n ? philox_u64(i, counter, key) : ~0ull;
-        p[i] = i < n ? map[i] : ~0u;
-    }
+    shuffle_pack_body(map, n, np, counter, key, k, p, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_copy_u32(uint32_t* dst, const uint32_t* src, size_t n)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_copy_u32"));
-    VELO_GRID_STRIDE(i, n)
-    dst[i] = src[i];
+    copy_u32_body(dst, src, n, blockIdx.x, gridDim.x);
 }
 
-// exclusive scan of the tile carries; one CTA of 1024 threads, rounds of
-// 1024 consecutive tiles chained through the running carry
+// exclusive scan of the tile carries; one CTA of 1024 threads
 __global__ void __launch_bounds__(1024) k_fill_scan(const FillCarry* tile_last, int ntiles, FillCarry* carry)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_fill_scan"));
     __shared__ FillCarry wsm[33];
-    FillCarry run { 0, 0, 0, 0 };
-    for (int base = 0; base < ntiles; base += blockDim.x) {
-        const int t = base + (int)threadIdx.x;
-        FillCarry x { 0, 0, 0, 0 };
-        if (t < ntiles) {
-            VELO_TRACE_AT(TS_FILL, tile_last + t);
-            x = tile_last[t];
-        }
-        const FillCarry ex = block_fill_scan_excl(x, wsm);
-        if (t < ntiles)
-            carry[t] = fill_combine(run, ex);
-        run = fill_combine(run, wsm[32]);
-    }
+    fill_scan_body(tile_last, ntiles, carry, wsm);
 }
-
-// ---------------------------------------------------------------------------
-// oblivious gather: out[j] = table[rid[j]]
-// union row layout (3 words):
-//   table row i : w0 = i << 32 | tag 0      w1 = table[i]   w2 = 0
-//   request j   : w0 = rid << 32 | tag 1    w1 = 0          w2 = j
-// sort 1 on (index, tag); fill gives each request the value of its table
-// row; the requests' w0 becomes (0, j), every other row (1, ...); sort 2 on
-// w0 puts the requests first in request order.
-// ---------------------------------------------------------------------------
-
-struct GatherFill {
-    __device__ __forceinline__ static FillCarry src(uint64_t a, uint64_t b, uint64_t)
-    {
-        const bool table = ((a >> 31) & 1ull) == 0 && a != ~0ull;
-        return FillCarry { a >> 32, b, table ? 1u : 0u, 1u };
-    }
-    __device__ __forceinline__ static bool dup(uint64_t, uint64_t, uint64_t, const FillCarry&) { return false; }
-    __device__ __forceinline__ static void apply(uint64_t& a, uint64_t& b, uint64_t& c, const FillCarry& last)
-    {
-        const bool req = ((a >> 31) & 1ull) == 1 && a != ~0ull;
-        const bool hit = req & (last.has != 0) & (last.key == (a >> 32));
-        b = req ? (hit ? last.val : 0ull) : b;
-        a = req ? (c & 0xFFFFFFFFull) : (1ull << 63);
-    }
-};
 
 __global__ void k_ogather_pack(const uint64_t* table, size_t tn, const uint32_t* rids, size_t rn, size_t rows,
                                uint64_t* w0, uint64_t* w1, uint64_t* w2)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_ogather_pack"));
-    VELO_GRID_STRIDE(g, rows)
-    {
-        uint64_t a = ~0ull, b = ~0ull, c = ~0ull;
-        if (g < tn) {
-            a = (uint64_t)g << 32;
-            b = table[g];
-            c = 0;
-        } else if (g < tn + rn) {
-            const size_t j = g - tn;
-            a = ((uint64_t)rids[j] << 32) | (1ull << 31);
-            b = 0;
-            c = j;
-        }
-        w0[g] = a;
-        w1[g] = b;
-        w2[g] = c;
-    }
+    ogather_pack_body(table, tn, rids, rn, rows, w0, w1, w2, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_ogather_out(const uint64_t* w1, size_t rn, uint64_t* out)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_ogather_out"));
-    VELO_GRID_STRIDE(j, rn)
-    out[j] = w1[j];
+    ogather_out_body(w1, rn, out, blockIdx.x, gridDim.x);
 }
-
-// ---------------------------------------------------------------------------
-// oblivious PK-FK join producing rowid pairs
-// union row layout (3 words):
-//   w0 = key (order-preserving u64)
-//   w1 = [63] tag (0 build, 1 probe) | [62] row valid | [61] joined | [60:0] rowid
-//   w2 = build rowid of a joined probe row
-// ---------------------------------------------------------------------------
-
-constexpr uint64_t OJ_TAG = 1ull << 63, OJ_VALID = 1ull << 62, OJ_JOINED = 1ull << 61;
-constexpr uint64_t OJ_ROWID = (1ull << 61) - 1;
-
-struct JoinFill {
-    __device__ __forceinline__ static bool is_pad(uint64_t a, uint64_t b) { return a == ~0ull && b == ~0ull; }
-    __device__ __forceinline__ static FillCarry src(uint64_t a, uint64_t b, uint64_t)
-    {
-        const bool build = (b & OJ_TAG) == 0 && !is_pad(a, b);
-        return FillCarry { a, b & OJ_ROWID, build ? 1u : 0u, (b & OJ_VALID) ? 1u : 0u };
-    }
-    // a build row whose key equals the preceding build row's key
-    __device__ __forceinline__ static bool dup(uint64_t a, uint64_t b, uint64_t, const FillCarry& last)
-    {
-        const bool build = (b & OJ_TAG) == 0 && !is_pad(a, b);
-        return build & (last.has != 0) & (last.key == a);
-    }
-    __device__ __forceinline__ static void apply(uint64_t& a, uint64_t& b, uint64_t& c, const FillCarry& last)
-    {
-        const bool probe = (b & OJ_TAG) != 0 && !is_pad(a, b);
-        const bool joined = probe & ((b & OJ_VALID) != 0) & (last.has != 0) & (last.valid != 0) & (last.key == a);
-        b = (b & ~OJ_JOINED) | (joined ? OJ_JOINED : 0ull);
-        c = joined ? last.val : ~0ull;
-    }
-};
 
 __global__ void k_ojoin_pack(const void* bk, const uint8_t* bm, size_t bn, const void* pk, const uint8_t* pm, size_t pn,
                              int key64, size_t rows, uint64_t* w0, uint64_t* w1, uint64_t* w2)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_ojoin_pack"));
-    VELO_GRID_STRIDE(g, rows)
-    {
-        uint64_t a = ~0ull, b = ~0ull, c = ~0ull;
-        if (g < bn + pn) {
-            const bool build = g < bn;
-            const size_t j = build ? g : g - bn;
-            const void* keys = build ? bk : pk;
-            const uint8_t* mask = build ? bm : pm;
-            const uint64_t key = key64 ? ((uint64_t) static_cast<const int64_t*>(keys)[j] ^ 0x8000000000000000ull)
-                                       : (uint64_t)((uint32_t) static_cast<const int32_t*>(keys)[j] ^ 0x80000000u);
-            const bool valid = mask == nullptr || mask[j] != 0;
-            a = key;
-            b = (build ? 0ull : OJ_TAG) | (valid ? OJ_VALID : 0ull) | ((uint64_t)j & OJ_ROWID);
-            c = ~0ull;
-        }
-        w0[g] = a;
-        w1[g] = b;
-        w2[g] = c;
-    }
+    ojoin_pack_body(bk, bm, bn, pk, pm, pn, key64, rows, w0, w1, w2, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_ojoin_out(const uint64_t* w1, const uint64_t* w2, size_t pn, int64_t* ob, int64_t* op)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_ojoin_out"));
-    VELO_GRID_STRIDE(i, pn)
-    {
-        const uint64_t b = w1[i];
-        const bool j = (b & OJ_JOINED) != 0 && b != ~0ull;
-        ob[i] = j ? (int64_t)w2[i] : -1;
-        op[i] = j ? (int64_t)(b & OJ_ROWID) : -1;
-    }
+    ojoin_out_body(w1, w2, pn, ob, op, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_zero_u64(unsigned long long* p, int n)
@@ -298,8 +119,7 @@ __global__ void k_zero_u64(unsigned long long* p, int n)
 __global__ void k_join_counts(const uint64_t* n_joined, const unsigned long long* dups, uint64_t* d_counts)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_join_counts"));
-    d_counts[0] = *n_joined;
-    d_counts[1] = *dups;
+    join_counts_body(n_joined, dups, d_counts);
 }
 
 } // namespace velo

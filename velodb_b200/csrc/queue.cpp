@@ -1,5 +1,6 @@
-// Command queue over a CUDA stream: velo_init / velo_submit /
-// velo_batch_submit / velo_wait / velo_shutdown.
+// Command queue: velo_init / velo_submit / velo_batch_submit / velo_wait /
+// velo_shutdown, over a CUDA stream (default) or over the persistent device
+// consumer (VELO_QUEUE_PERSISTENT, dq.cu / dq_kernel.cu).
 //
 // The reference's TaskManager keeps one cooperative persistent kernel polling
 // a host-mapped ring and runs commands strictly one at a time with a
@@ -21,6 +22,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "dq_host.hpp"
 
 struct velo_ctx {
     int device = 0;
@@ -34,6 +36,8 @@ struct velo_ctx {
     std::deque<std::pair<uint64_t, velo_batch*>> plans; // batch plans kept alive until their ticket completes
     std::deque<uint64_t> failed;                        // tickets whose batch reported a device wait timeout
     std::string last_error;
+    velo::DqEngine* dq = nullptr; // VELO_QUEUE_PERSISTENT: tickets are job numbers of this queue
+    uint64_t dq_last = 0;         // the last job published
 };
 
 namespace {
@@ -178,6 +182,16 @@ extern "C" velo_status velo_init(const velo_config* config, velo_ctx** out)
     velo_ctx* c = new velo_ctx();
     c->device = config ? config->device : 0;
     c->capacity = (config && config->queue_capacity) ? config->queue_capacity : 1024;
+    if (config && (config->flags & VELO_QUEUE_PERSISTENT)) {
+        const velo_status rc = velo::dq_create(c->device, config->idle_us, &c->dq);
+        if (rc != VELO_OK) {
+            delete c;
+            return rc;
+        }
+        c->stream = (cudaStream_t)velo::dq_stream(c->dq);
+        *out = c;
+        return VELO_OK;
+    }
     cudaError_t err = cudaSetDevice(c->device);
     if (err == cudaSuccess)
         err = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
@@ -193,6 +207,11 @@ extern "C" velo_status velo_shutdown(velo_ctx* c, uint32_t timeout_ms)
 {
     if (!c)
         return VELO_OK;
+    if (c->dq) {
+        const velo_status rq = velo::dq_destroy(c->dq, timeout_ms);
+        delete c;
+        return rq;
+    }
     velo_status rc = VELO_OK;
     const auto t0 = std::chrono::steady_clock::now();
     for (;;) {
@@ -230,6 +249,19 @@ extern "C" velo_status velo_submit(velo_ctx* c, const velo_cmd* cmd, uint64_t* t
     if (!c || !cmd)
         return velo::einval("velo_submit: null argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    if (c->dq) {
+        velo::DqPlan plan;
+        velo_status rc = velo::dq_plan_cmd(plan, *cmd);
+        uint64_t seq = 0;
+        if (rc == VELO_OK)
+            rc = velo::dq_publish(c->dq, plan, (cmd->flags & VELO_CMD_UNORDERED) ? 0 : c->dq_last, &seq);
+        if (rc != VELO_OK)
+            return ctx_fail(c, rc);
+        c->dq_last = seq;
+        if (ticket)
+            *ticket = seq;
+        return VELO_OK;
+    }
     velo_status rc = dispatch(c, *cmd);
     if (rc != VELO_OK)
         return ctx_fail(c, rc);
@@ -241,6 +273,28 @@ extern "C" velo_status velo_batch_submit(velo_ctx* c, const velo_cmd* cmds, size
     if (!c || (!cmds && n))
         return velo::einval("velo_batch_submit: null argument");
     std::lock_guard<std::mutex> lock(c->mu);
+    if (c->dq) {
+        // every command a job of its own, ordered after what came before the
+        // batch and unordered among the batch
+        const uint64_t after = c->dq_last;
+        uint64_t last = after;
+        for (size_t i = 0; i < n; i++) {
+            velo::DqPlan plan;
+            velo_status rc = velo::dq_plan_cmd(plan, cmds[i]);
+            uint64_t seq = 0;
+            if (rc == VELO_OK)
+                rc = velo::dq_publish(c->dq, plan, after, &seq);
+            if (rc != VELO_OK) {
+                c->dq_last = last;
+                return ctx_fail(c, rc);
+            }
+            last = seq;
+            if (tickets)
+                tickets[i] = seq;
+        }
+        c->dq_last = last;
+        return VELO_OK;
+    }
     std::vector<velo_batch_item> items;
     std::vector<size_t> others;
     for (size_t i = 0; i < n; i++) {
@@ -312,6 +366,14 @@ extern "C" velo_status velo_wait(velo_ctx* c, uint64_t ticket, uint64_t timeout_
 {
     if (!c)
         return velo::einval("velo_wait: null context");
+    if (c->dq) {
+        const velo_status rc = velo::dq_wait(c->dq, ticket, timeout_ns);
+        if (rc != VELO_OK) {
+            std::lock_guard<std::mutex> lock(c->mu);
+            ctx_fail(c, rc);
+        }
+        return rc;
+    }
     const auto t0 = std::chrono::steady_clock::now();
     int spins = 0;
     for (;;) {
@@ -371,4 +433,9 @@ extern "C" size_t velo_cmd_size(void)
 extern "C" void* velo_ctx_stream(velo_ctx* c)
 {
     return c ? (void*)c->stream : nullptr;
+}
+
+extern "C" uint64_t velo_ctx_launches(velo_ctx* c)
+{
+    return (c && c->dq) ? velo::dq_launches(c->dq) : 0;
 }

@@ -672,12 +672,11 @@ struct SegAgg {
         __syncthreads();
     }
 
-    // pass D: out[q] = sum over tiles of tile_out[tile][q]; CTA q of
-    // G*(1+V) CTAs, SEG_THREADS threads
-    __device__ static void finish(const int64_t* tile_out, int ntiles, int G, int64_t* out)
+    // pass D: out[q] = sum over tiles of tile_out[tile][q]; one CTA of
+    // SEG_THREADS threads per output word q (0 .. G*(1+V)-1)
+    __device__ static void finish(const int64_t* tile_out, int ntiles, int G, int64_t* out, int q)
     {
         __shared__ int64_t part[SEG_THREADS / 32];
-        const int q = blockIdx.x;
         const int QN = G * (1 + V);
         int64_t sum = 0;
         for (int t = threadIdx.x; t < ntiles; t += SEG_THREADS) {

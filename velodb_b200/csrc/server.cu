@@ -11,6 +11,11 @@
 // and the next waiting query is admitted.  Every wait is bounded.  Tables
 // stay resident on the device for the server's lifetime.
 //
+// With VELO_SERVE_PERSISTENT the admitted queries run as jobs of one
+// persistent command queue (dq.cu) instead of on per-slot streams: each query
+// is planned into one job whose last steps copy its result words into the
+// slot's mapped host buffer, and the loop polls the jobs' completion words.
+//
 // The reference has no serving layer: ExecutionEngine::executeQuery runs one
 // query at a time on the caller's thread (src/execution/execution_engine.cpp:
 // 67-142) and the persistent kernel serialises all commands.
@@ -28,59 +33,37 @@
 #include <vector>
 
 #include "common.hpp"
+#include "dq_host.hpp"
+#include "ops.cuh"
 
 namespace velo {
 
-// ---- small kernels used by the three-way join chain ------------------------
+// ---- small kernels used by the three-way join chain (bodies in ops.cuh) ------
 
 __global__ void k_range_mask_i32(const int32_t* c, size_t n, int32_t lo, int32_t hi, uint8_t* m)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        m[i] = (c[i] >= lo) & (c[i] <= hi);
+    range_mask_body(c, n, lo, hi, m, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_range_mask_i64(const int64_t* c, size_t n, int64_t lo, int64_t hi, uint8_t* m)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        m[i] = (c[i] >= lo) & (c[i] <= hi);
+    range_mask_body(c, n, lo, hi, m, blockIdx.x, gridDim.x);
 }
 
-// rowid of a joined row -> (global key = rowid + offset, mask); -1 -> invalid
 __global__ void k_rowid_keys(const int64_t* rowid, size_t n, int64_t offset, int64_t* key, uint8_t* m)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int64_t r = rowid[i];
-        key[i] = r >= 0 ? r + offset : -1;
-        m[i] = r >= 0;
-    }
+    rowid_keys_body(rowid, n, offset, key, m, blockIdx.x, gridDim.x);
 }
 
-// probe rowid -> u32 request id, -1 -> `missing` (an id past the table)
 __global__ void k_rowid_rids(const int64_t* rowid, size_t n, uint32_t missing, uint32_t* rid)
 {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int64_t r = rowid[i];
-        rid[i] = r >= 0 ? (uint32_t)r : missing;
-    }
+    rowid_rids_body(rowid, n, missing, rid, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_sum_u64(const uint64_t* v, size_t n, unsigned long long* out)
 {
     __shared__ unsigned long long s[32];
-    unsigned long long acc = 0;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        acc += v[i];
-    for (int o = 16; o > 0; o >>= 1)
-        acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0)
-        s[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++)
-            t += s[w];
-        atomicAdd(out, t); // one add per CTA at a fixed address
-    }
+    sum_u64_body(v, n, out, blockIdx.x, gridDim.x, s);
 }
 
 static unsigned grid_n(size_t n)
@@ -171,7 +154,9 @@ struct Query {
 struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
-    int64_t* h_out = nullptr; // pinned result staging: 96 int64 + 2 u64
+    int64_t* h_out = nullptr; // pinned, mapped result staging: 96 int64 + 2 u64
+    int64_t* d_out_h = nullptr; // device address of h_out
+    uint64_t job = 0;           // persistent mode: the query's job
     Query* q = nullptr;
 };
 
@@ -194,6 +179,7 @@ struct velo_server {
     Clock::time_point t0 = Clock::now();
     uint64_t admitted = 0, completed = 0, peak_inflight = 0;
     size_t peak_arena = 0;
+    velo::DqEngine* dq = nullptr; // VELO_SERVE_PERSISTENT
 };
 
 namespace velo {
@@ -245,9 +231,94 @@ static bool query_valid(const velo_server* s, const velo_query& q)
     }
 }
 
+// plans a query's whole pipeline as one job of the persistent queue; its
+// last steps copy the result words into the slot's mapped host buffer
+static velo_status launch_query_dq(velo_server* s, Query* qq, Slot& sl)
+{
+    const velo_query& q = qq->q;
+    const velo_served_tables& t = s->t;
+    char* p = qq->scratch;
+    std::memset(sl.h_out, 0, 100 * sizeof(int64_t));
+    auto take = [&](size_t b) {
+        char* r = p;
+        p += align_up(b ? b : 1, 256);
+        return r;
+    };
+    int64_t* d_out = reinterpret_cast<int64_t*>(take(96 * 8));
+    uint64_t* d_counts = reinterpret_cast<uint64_t*>(take(16));
+    DqPlan plan;
+    velo_status rc = VELO_OK;
+    uint32_t out_words = 0;
+    if (q.shape == VELO_Q_FILTER_GROUPBY) {
+        velo_lineitem c = t.fact;
+        c.qty += q.offset;
+        c.price += q.offset;
+        c.disc += q.offset;
+        c.tax += q.offset;
+        c.shipdate += q.offset;
+        c.flag1 += q.offset;
+        c.flag2 += q.offset;
+        const size_t nb = velo_filter_groupby_scratch_bytes(q.n, 8);
+        rc = dq_plan_filter_groupby(plan, &c, q.n, &q.pred, 8, d_out, d_counts, take(nb), nb);
+        out_words = 8 * 6;
+    } else if (q.shape == VELO_Q_JOIN_TOPK) {
+        velo_join_tables jt { t.dim_key32 + q.dim_offset, t.dim_date + q.dim_offset, q.dim_n,
+                              t.fact_fk32 + q.offset, t.fact.price + q.offset, q.n };
+        const size_t nb = velo_join_groupby_topk_scratch_bytes(q.dim_n, q.n);
+        rc = dq_plan_join_topk(plan, &jt, &q.jpred, 10, d_out, d_counts, take(nb), nb);
+        out_words = 10 * 3;
+    } else {
+        // three-way chain dim <- fact <- fact2, as on the stream path
+        uint8_t* dmask = reinterpret_cast<uint8_t*>(take(q.dim_n));
+        uint8_t* fmask = reinterpret_cast<uint8_t*>(take(q.n));
+        int64_t* j1b = reinterpret_cast<int64_t*>(take(q.n * 8));
+        int64_t* j1p = reinterpret_cast<int64_t*>(take(q.n * 8));
+        int64_t* fkey = reinterpret_cast<int64_t*>(take(q.n * 8));
+        uint8_t* fkmask = reinterpret_cast<uint8_t*>(take(q.n));
+        uint8_t* f2mask = reinterpret_cast<uint8_t*>(take(q.f2_n));
+        int64_t* j2b = reinterpret_cast<int64_t*>(take(q.f2_n * 8));
+        int64_t* j2p = reinterpret_cast<int64_t*>(take(q.f2_n * 8));
+        uint32_t* rids = reinterpret_cast<uint32_t*>(take(q.f2_n * 4));
+        uint64_t* vals = reinterpret_cast<uint64_t*>(take(q.f2_n * 8));
+        const size_t j1n = velo_ojoin_scratch_bytes(q.dim_n, q.n), j2n = velo_ojoin_scratch_bytes(q.n, q.f2_n),
+                     gn = velo_ogather_scratch_bytes(q.f2_n, q.f2_n);
+        size_t mx = j1n > j2n ? j1n : j2n;
+        mx = mx > gn ? mx : gn;
+        char* sc = take(mx);
+        dq_plan_range_mask_i32(plan, t.dim_date + q.dim_offset, q.dim_n, INT32_MIN, q.jpred.date_hi - 1, dmask);
+        dq_plan_range_mask_i64(plan, t.fact.price + q.offset, q.n, INT64_MIN, q.jpred.price_hi - 1, fmask);
+        rc = dq_plan_ojoin_pkfk(plan, t.dim_key + q.dim_offset, dmask, q.dim_n, t.fact_fk + q.offset, fmask, q.n,
+                                VELO_BIGINT, j1b, j1p, d_counts, sc, mx);
+        if (rc == VELO_OK) {
+            dq_plan_rowid_keys(plan, j1p, q.n, (int64_t)q.offset, fkey, fkmask);
+            dq_plan_fill_u8(plan, f2mask, 1, q.f2_n);
+            rc = dq_plan_ojoin_pkfk(plan, fkey, fkmask, q.n, t.fact2_fk + q.f2_offset, f2mask, q.f2_n, VELO_BIGINT,
+                                    j2b, j2p, d_counts, sc, mx);
+        }
+        if (rc == VELO_OK) {
+            dq_plan_rowid_rids(plan, j2p, q.f2_n, (uint32_t)q.f2_n, rids);
+            rc = dq_plan_ogather(plan, reinterpret_cast<const uint64_t*>(t.fact2_price + q.f2_offset), q.f2_n, rids,
+                                 q.f2_n, vals, sc, mx);
+        }
+        if (rc == VELO_OK) {
+            dq_plan_set_words(plan, reinterpret_cast<uint64_t*>(d_out), 0, 1);
+            dq_plan_sum_u64(plan, vals, q.f2_n, reinterpret_cast<unsigned long long*>(d_out));
+        }
+        out_words = 1;
+    }
+    if (rc != VELO_OK)
+        return rc;
+    dq_plan_copy_words(plan, reinterpret_cast<const uint64_t*>(d_out), reinterpret_cast<uint64_t*>(sl.d_out_h),
+                       out_words);
+    dq_plan_copy_words(plan, d_counts, reinterpret_cast<uint64_t*>(sl.d_out_h + 96), 2);
+    return dq_publish(s->dq, plan, 0, &sl.job);
+}
+
 // enqueues a query's whole pipeline on its slot's stream
 static velo_status launch_query(velo_server* s, Query* qq, Slot& sl)
 {
+    if (s->dq)
+        return launch_query_dq(s, qq, sl);
     const velo_query& q = qq->q;
     const velo_served_tables& t = s->t;
     cudaStream_t st = sl.stream;
@@ -365,6 +436,15 @@ static void serve(velo_server* s)
                 Slot& sl = s->slots[i];
                 if (!sl.q)
                     continue;
+                if (s->dq) {
+                    velo_status st = VELO_OK;
+                    if (!dq_poll(s->dq, sl.job, &st))
+                        continue;
+                    finish(s, sl.q, st);
+                    idle = false;
+                    s->cv.notify_all();
+                    continue;
+                }
                 const cudaError_t e = cudaEventQuery(sl.done);
                 if (e == cudaErrorNotReady)
                     continue;
@@ -400,7 +480,8 @@ static void serve(velo_server* s)
                 s->peak_arena = s->arena.in_use() > s->peak_arena ? s->arena.in_use() : s->peak_arena;
                 const velo_status rc = launch_query(s, q, sl);
                 if (rc != VELO_OK) {
-                    cudaStreamSynchronize(sl.stream);
+                    if (!s->dq)
+                        cudaStreamSynchronize(sl.stream);
                     finish(s, q, rc);
                     s->cv.notify_all();
                 }
@@ -438,16 +519,21 @@ extern "C" velo_status velo_server_create(const velo_server_config* cfg, const v
         rc = cuda_fail(e, "cudaSetDevice");
     if (rc == VELO_OK)
         rc = s->arena.init(cfg->hbm_budget_bytes);
+    if (rc == VELO_OK && (cfg->flags & VELO_SERVE_PERSISTENT))
+        rc = dq_create(cfg->device, cfg->idle_us, &s->dq);
     s->slots.resize(cfg->slots);
     for (auto& sl : s->slots) {
         if (rc != VELO_OK)
             break;
         if ((e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaMallocHost(&sl.h_out, 100 * 8)) != cudaSuccess)
+            (e = cudaHostAlloc(&sl.h_out, 100 * 8, cudaHostAllocMapped)) != cudaSuccess ||
+            (e = cudaHostGetDevicePointer((void**)&sl.d_out_h, sl.h_out, 0)) != cudaSuccess)
             rc = cuda_fail(e, "velo_server_create");
     }
     if (rc != VELO_OK) {
+        if (s->dq)
+            dq_destroy(s->dq, 10000);
         for (auto& sl : s->slots) {
             if (sl.stream)
                 cudaStreamDestroy(sl.stream);
@@ -561,6 +647,12 @@ extern "C" velo_status velo_server_destroy(velo_server* s, uint32_t timeout_ms)
         return rc;
     }
     s->loop.join();
+    if (s->dq) {
+        rc = dq_destroy(s->dq, timeout_ms);
+        if (rc != VELO_OK)
+            return rc; // the queue keeps its memory; the server object stays
+        s->dq = nullptr;
+    }
     for (auto& kv : s->all)
         delete kv.second;
     for (auto& sl : s->slots) {

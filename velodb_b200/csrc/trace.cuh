@@ -102,6 +102,7 @@ enum VeloTraceSite : uint32_t {
     TS_K_COUNT_MARKS,
     TS_K_SCAN_TILES,
     TS_K_SCHED,
+    TS_K_DQ,
     TS_LI_IN = 200,
     TS_LI_OUT,
     TS_SEG_LOAD,

@@ -115,14 +115,13 @@ __device__ __forceinline__ FillCarry block_fill_scan_excl(const FillCarry& mine,
 
 // Src: static FillCarry src(w0, w1, w2) -- has = row is a source
 //      static void apply(uint64_t& w0, uint64_t& w1, uint64_t& w2, const FillCarry& last)
+// the last source row of fill tile `blk` (FL_THREADS threads); sm, idx:
+// FL_THREADS / 32 entries of shared memory each
 template <class F>
-__global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, const uint64_t* w1, const uint64_t* w2,
-                                                         FillCarry* tile_last)
+__device__ __forceinline__ void fill_sum_tile(const uint64_t* w0, const uint64_t* w1, const uint64_t* w2,
+                                              FillCarry* tile_last, size_t blk, FillCarry* sm, int* idx)
 {
-    VELO_TRACE_KERNEL(velo_site_hash("k_fill_sum"));
-    __shared__ FillCarry sm[FL_THREADS / 32];
-    __shared__ int idx[FL_THREADS / 32];
-    const size_t base = (size_t)blockIdx.x * FL_TS;
+    const size_t base = blk * FL_TS;
     FillCarry c { 0, 0, 0, 0 };
     int last = -1;
     for (int i = threadIdx.x; i < FL_TS; i += FL_THREADS) {
@@ -154,23 +153,18 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, con
             b = take ? sm[w] : b;
             bi = take ? idx[w] : bi;
         }
-        VELO_TRACE_AT(TS_FILL, tile_last + blockIdx.x);
-        tile_last[blockIdx.x] = b;
+        VELO_TRACE_AT(TS_FILL, tile_last + blk);
+        tile_last[blk] = b;
     }
 }
 
-// exclusive scan of the tile carries (one CTA of 1024 threads), defined in
-// ops.cu
-__global__ void k_fill_scan(const FillCarry* tile_last, int ntiles, FillCarry* carry);
-
+// fill of tile `blk` from its carry; wsm: 33 entries, tmp: 33 words of shared
+// memory
 template <class F>
-__global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_t* w1, uint64_t* w2,
-                                                           const FillCarry* carry, unsigned long long* d_stat)
+__device__ __forceinline__ void fill_apply_tile(uint64_t* w0, uint64_t* w1, uint64_t* w2, const FillCarry* carry,
+                                                unsigned long long* d_stat, size_t blk, FillCarry* wsm, uint32_t* tmp)
 {
-    VELO_TRACE_KERNEL(velo_site_hash("k_fill_apply"));
-    __shared__ FillCarry wsm[33];
-    __shared__ uint32_t tmp[33];
-    const size_t base = (size_t)blockIdx.x * FL_TS + (size_t)threadIdx.x * FL_RPT;
+    const size_t base = blk * FL_TS + (size_t)threadIdx.x * FL_RPT;
     uint64_t a[FL_RPT], b[FL_RPT], c[FL_RPT];
     FillCarry mine { 0, 0, 0, 0 };
 #pragma unroll
@@ -181,7 +175,7 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_
         c[r] = w2[base + r];
         mine = fill_combine(mine, F::src(a[r], b[r], c[r]));
     }
-    FillCarry run = fill_combine(carry[blockIdx.x], block_fill_scan_excl(mine, wsm));
+    FillCarry run = fill_combine(carry[blk], block_fill_scan_excl(mine, wsm));
     uint32_t stat = 0;
 #pragma unroll
     for (int r = 0; r < FL_RPT; r++) {
@@ -198,6 +192,30 @@ __global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_
     block_exclusive_scan(stat, tmp, &total);
     if (threadIdx.x == 0 && d_stat)
         atomicAdd(d_stat, (unsigned long long)total);
+}
+
+template <class F>
+__global__ void __launch_bounds__(FL_THREADS) k_fill_sum(const uint64_t* w0, const uint64_t* w1, const uint64_t* w2,
+                                                         FillCarry* tile_last)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_sum"));
+    __shared__ FillCarry sm[FL_THREADS / 32];
+    __shared__ int idx[FL_THREADS / 32];
+    fill_sum_tile<F>(w0, w1, w2, tile_last, blockIdx.x, sm, idx);
+}
+
+// exclusive scan of the tile carries (one CTA of 1024 threads), defined in
+// ops.cu
+__global__ void k_fill_scan(const FillCarry* tile_last, int ntiles, FillCarry* carry);
+
+template <class F>
+__global__ void __launch_bounds__(FL_THREADS) k_fill_apply(uint64_t* w0, uint64_t* w1, uint64_t* w2,
+                                                           const FillCarry* carry, unsigned long long* d_stat)
+{
+    VELO_TRACE_KERNEL(velo_site_hash("k_fill_apply"));
+    __shared__ FillCarry wsm[33];
+    __shared__ uint32_t tmp[33];
+    fill_apply_tile<F>(w0, w1, w2, carry, d_stat, blockIdx.x, wsm, tmp);
 }
 
 template <class F>
@@ -247,7 +265,9 @@ inline UnionScratch union_layout(char* base, size_t rows)
     };
     for (int i = 0; i < 3; i++)
         s.w[i] = reinterpret_cast<uint64_t*>(take(rows * 8));
-    const size_t nft = rows / FL_TS, nct = rows >> OP_LT;
+    // tile counts sized for 2^(OP_LT-1)-row tiles: the persistent command
+    // queue compacts three-word records in 2048-row tiles
+    const size_t nft = rows / FL_TS, nct = rows >> (OP_LT - 1);
     s.tl = reinterpret_cast<FillCarry*>(take(nft * sizeof(FillCarry)));
     s.carry = reinterpret_cast<FillCarry*>(take(nft * sizeof(FillCarry)));
     s.counts = reinterpret_cast<uint32_t*>(take(nct * 4));

@@ -44,7 +44,7 @@ void check(velo_status st, const char* what)
 
 ExecutionContext::ExecutionContext(int device)
 {
-    velo_config cfg { device, 0 };
+    velo_config cfg { device, 0, 0, 0 };
     check(velo_init(&cfg, &ctx_), "ExecutionContext");
     stream_ = velo_ctx_stream(ctx_);
 }

@@ -116,13 +116,21 @@ def arrivals(count: int, rate_qps: float, seed: int = W.SEED_SERVE) -> np.ndarra
     return np.cumsum(-np.log(u) / rate_qps)
 
 
+SERVE_PERSISTENT = 1
+
+
 class Server:
-    def __init__(self, tables: ServedTables, slots: int, budget_bytes: int, device: int = 0):
+    """The serving layer (velo_server_*); persistent=True runs the admitted
+    queries as jobs of one persistent command queue instead of per-slot
+    streams."""
+
+    def __init__(self, tables: ServedTables, slots: int, budget_bytes: int, device: int = 0,
+                 persistent: bool = False, idle_us: int = 0):
         self.tables = tables
         self._tab = tables.struct()
         self.ptr = C.c_void_p()
-        check(lib().velo_server_create(C.byref(VeloServerConfig(device, slots, budget_bytes)), C.byref(self._tab),
-                                       C.byref(self.ptr)), "velo_server_create")
+        cfg = VeloServerConfig(device, slots, budget_bytes, SERVE_PERSISTENT if persistent else 0, idle_us)
+        check(lib().velo_server_create(C.byref(cfg), C.byref(self._tab), C.byref(self.ptr)), "velo_server_create")
 
     def submit(self, q: VeloQuery) -> int:
         qid = C.c_uint64()
