@@ -752,15 +752,34 @@ def _lat(results, t_key="submit_ms"):
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
 
 
-def measure_serve(torch, nq=256, slots=16):
+def _served_form(S, tab, qs, budget, slots, plain_qps, persistent):
+    """One server form at saturation (every query offered at once) and under
+    Poisson arrivals at 0.9x and 3x the plain capacity."""
+    nq = len(qs)
+    srv = S.Server(tab, slots=slots, budget_bytes=budget, persistent=persistent)
+    S.run_open_loop(srv, qs[:32], np.zeros(32))
+    sat_res, sat_s = S.run_open_loop(srv, qs, np.zeros(nq))
+    loads = {}
+    for f in (0.9, 3.0):
+        r, s = S.run_open_loop(srv, qs, S.arrivals(nq, f * plain_qps, seed=int(f * 1000)))
+        loads[f"{f}x_plain_capacity"] = {"offered_qps": f * plain_qps, "achieved_qps": nq / s, **_lat(r)}
+    st = srv.stats()
+    srv.close()
+    form = {"qps_saturation": nq / sat_s, **_lat(sat_res), "slots": slots,
+            "peak_inflight": st["peak_inflight"], "peak_arena_bytes": st["peak_arena_bytes"], "poisson": loads}
+    return form, sat_res
+
+
+def measure_serve(torch, nq=256, slots=16, persistent_slots=64):
     """A seeded query stream (50 % filter + group-by, 35 % two-way join +
     top-10, 15 % three-way chain; slice sizes 2^10..2^18) over resident tables
     of 60 M / 15 M / 150 M rows, admitted by a 120 GB HBM budget.  Plain = the
     same request loop with one slot, each query submitted after the previous
-    one returned.  Served = up to 16 queries in flight on their own streams,
-    at saturation (every query offered at once) and under Poisson arrivals at
-    0.9x and 3x the plain capacity.  Latency is submit -> result in host
-    memory, on the host clock."""
+    one returned.  Served = up to 16 queries in flight on their own streams;
+    served_persistent = up to 64 queries in flight as jobs of one persistent
+    command queue.  Each at saturation (every query offered at once) and under
+    Poisson arrivals at 0.9x and 3x the plain capacity.  Latency is submit ->
+    result in host memory, on the host clock."""
     from velodb_b200 import serving as S
 
     t0 = time.perf_counter()
@@ -777,28 +796,24 @@ def measure_serve(torch, nq=256, slots=16):
     plain_qps = nq / plain_s
     r09, _ = S.run_open_loop(srv, qs, S.arrivals(nq, 0.9 * plain_qps, seed=900))
     srv.close()
-    srv = S.Server(tab, slots=slots, budget_bytes=budget)
-    S.run_open_loop(srv, qs[:32], np.zeros(32))
-    sat_res, sat_s = S.run_open_loop(srv, qs, np.zeros(nq))
-    loads = {}
-    for f in (0.9, 3.0):
-        r, s = S.run_open_loop(srv, qs, S.arrivals(nq, f * plain_qps, seed=int(f * 1000)))
-        loads[f"{f}x_plain_capacity"] = {"offered_qps": f * plain_qps, "achieved_qps": nq / s, **_lat(r)}
-    st = srv.stats()
-    srv.close()
-    same = all(S.result_key(a) == S.result_key(b) and a.status == 0 and b.status == 0
-               for a, b in zip(plain_res, sat_res))
+    served, sat_res = _served_form(S, tab, qs, budget, slots, plain_qps, False)
+    served_p, sat_p = _served_form(S, tab, qs, budget, persistent_slots, plain_qps, True)
+
+    def same(rs):
+        return bool(all(S.result_key(a) == S.result_key(b) and a.status == 0 and b.status == 0
+                        for a, b in zip(plain_res, rs)))
+
     shapes = {S.SHAPE_NAMES[k]: int(sum(1 for q in qs if q.shape == k)) for k in S.SHAPE_NAMES}
     out = {
         "tables_rows": dict(S.FULL_SCALE), "resident_bytes": int(tab.bytes), "table_build_s": build_s,
         "hbm_budget_bytes": budget, "sizes_log2": [lo, hi], "queries": nq, "mix": shapes,
         "plain": {"qps": plain_qps, **_lat(plain_res),
                   "poisson_0.9x": {"offered_qps": 0.9 * plain_qps, **_lat(r09)}},
-        "served": {"qps_saturation": nq / sat_s, **_lat(sat_res), "slots": slots,
-                   "peak_inflight": st["peak_inflight"], "peak_arena_bytes": st["peak_arena_bytes"],
-                   "poisson": loads},
-        "speedup_served_vs_plain": (nq / sat_s) / plain_qps,
-        "results_identical_alone_and_in_mix": bool(same),
+        "served": served,
+        "served_persistent": served_p,
+        "speedup_served_vs_plain": served["qps_saturation"] / plain_qps,
+        "speedup_served_persistent_vs_plain": served_p["qps_saturation"] / plain_qps,
+        "results_identical_alone_and_in_mix": same(sat_res) and same(sat_p),
         "timing": "host clock, submit -> result in host memory",
     }
     del tab
@@ -923,6 +938,40 @@ def make_workload(name, torch, capi, W, device):
     raise SystemExit(f"unknown workload {name}")
 
 
+def batch_persistent(torch, capi, wl, reps=5):
+    """The same 512 instances as jobs of one persistent command queue
+    (velo_batch_submit on a VELO_QUEUE_PERSISTENT context: the instances run
+    beside each other, every CTA of the consumer claiming work items of any
+    of them).  Host clock from the submission to the last completion, best
+    of `reps`."""
+    scr = []
+    cmds = []
+    for it in wl.items:
+        if it["kind"] == "sort":
+            cmds.append(capi.make_cmd("OSORT_KP", it["keys"], it["pay"], it["n"], it["keys"].numel()))
+        else:
+            cap = it["keys"].numel()
+            sc = torch.empty(capi.compact_scratch_bytes(cap), dtype=torch.uint8, device=it["keys"].device)
+            scr.append(sc)
+            cmds.append(capi.make_cmd("OCOMPACT_KPM", it["keys"], it["pay"], it["marks"], it["n"], cap,
+                                      it["count"], sc, sc.numel()))
+    torch.cuda.synchronize()
+    best = None
+    with capi.Queue(persistent=True) as q:
+        for r in range(reps + 1):
+            t0 = time.perf_counter()
+            tix = q.submit_batch(cmds)
+            for t in tix:
+                q.wait(t)
+            dt = time.perf_counter() - t0
+            if r > 0:
+                best = dt if best is None else min(best, dt)
+        launches = q.launches()
+    return {"ms_per_step": best * 1e3, "value": wl.n / best / 1e6, "unit": "Mrows/s", "runs": reps,
+            "consumer_launches": launches,
+            "timing": "host clock, velo_batch_submit of the 512 commands -> last velo_wait returned"}
+
+
 def batch_plain(torch, wl, args):
     """The plain path of the batch (512 launch sequences back to back) and the
     batch's network bytes against both."""
@@ -1011,6 +1060,8 @@ def run_extras(torch, capi, W, device, args, peak, peak_kind, orc):
             wl = Batched(torch, capi, W, device)
             r = measure(torch, capi, wl, sub, 1, device, peak, peak_kind, with_e2e=False)
             r.update(batch_plain(torch, wl, sub))
+            r["persistent_queue"] = batch_persistent(torch, capi, wl)
+            r["speedup_persistent_queue_vs_plain"] = r["plain_path"]["ms_per_step"] / r["persistent_queue"]["ms_per_step"]
             r["checked_against_oracle"] = wl.check(orc)
             out["batched"] = r
             del wl

@@ -296,3 +296,18 @@ def test_wait_is_bounded_and_unsupported_opcodes_are_refused(pq):
     pq.wait(t)
     assert pq.submit_raw(capi.make_cmd("OJOIN_MN")) == ENOTSUP
     assert pq.wait_raw(10**9, 1000) == -1  # unknown ticket
+
+
+def test_rapid_publication_of_tiny_jobs(pq):
+    # thousands of tiny jobs published back to back while the consumer runs:
+    # every one is ingested once, runs, and reports success
+    n = 3
+    keys = [torch.from_numpy(W.splitmix64(i, 4, 9).view(np.int64)).cuda() for i in range(2000)]
+    pays = [torch.from_numpy(np.arange(4, dtype=np.int32)).cuda() for _ in range(2000)]
+    ready()
+    tix = [pq.submit(capi.make_cmd("OSORT_KP", k, p, n, 4, flags=capi.CMD_UNORDERED)) for k, p in zip(keys, pays)]
+    for t in tix:
+        pq.wait(t)
+    for i, k in enumerate(keys):
+        h = k.cpu().numpy().view(np.uint64)
+        assert np.array_equal(h[:3], np.sort(W.splitmix64(i, 4, 9)[:3]))

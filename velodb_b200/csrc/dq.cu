@@ -71,7 +71,8 @@ public:
     void step(uint32_t kind, uint64_t ntiles, uint32_t arg, NetPass pass = NetPass {})
     {
         const uint64_t items = j_.h.nitems;
-        if (j_.h.nsteps >= (uint32_t)DQ_MAX_STEPS || ntiles == 0 || items + ntiles > 0xFFFFFFFFull) {
+        if (j_.h.nsteps >= (uint32_t)DQ_MAX_STEPS || ntiles == 0 || ntiles > DQ_MAX_ITEMS_PER_STEP
+            || items + ntiles > 0xFFFFFFFFull) {
             fail();
             return;
         }
@@ -883,7 +884,10 @@ void retire(DqEngine* e)
     }
 }
 
-// (re)launch the consumer when it is not running and a job is pending (mu held)
+// (re)launch the consumer when it is not running and a job is pending (mu
+// held).  The consumer writes the number of the launch that decided to exit
+// into the control words, so no CUDA call is needed to see that it left; a
+// relaunch queues behind the leaving grid on the same stream.
 velo_status ensure_running(DqEngine* e)
 {
     if (vctl(e)->fault)
@@ -898,15 +902,11 @@ velo_status ensure_running(DqEngine* e)
         e->launches++;
         return VELO_OK;
     }
+    if (vctl(e)->exited_launch != e->launches)
+        return VELO_OK; // the current launch is running
     retire(e);
     if (e->retired_below >= e->next_seq)
         return VELO_OK; // nothing pending
-    const cudaError_t q = cudaStreamQuery(e->stream);
-    if (q == cudaErrorNotReady)
-        return VELO_OK; // running
-    if (q != cudaSuccess)
-        return cuda_fail(q, "persistent queue");
-    // the consumer exited (idle) before the pending jobs were published
     VELO_CUDA_TRY(cudaSetDevice(e->device), "cudaSetDevice");
     velo_status rc = dq_launch(e->prm, false, e->stream, nullptr);
     if (rc == VELO_OK)
@@ -1004,6 +1004,17 @@ velo_status dq_publish(DqEngine* e, DqPlan& p, uint64_t after, uint64_t* seq_out
 bool dq_poll(DqEngine* e, uint64_t seq, velo_status* status)
 {
     std::lock_guard<std::mutex> lock(e->mu);
+    if (seq >= e->retired_below && seq < e->next_seq) {
+        // jobs complete out of order: read the job's own ring slot, which is
+        // not reused before the job is retired
+        const int hs = (int)((seq - 1) % DQ_HOST_RING);
+        if (vctl(e)->done_seq[hs] == seq) {
+            std::atomic_thread_fence(std::memory_order_acquire);
+            if (status)
+                *status = (velo_status)vctl(e)->status[hs];
+            return true;
+        }
+    }
     retire(e);
     if (seq < e->retired_below) {
         velo_status st = VELO_OK;

@@ -8,13 +8,12 @@
 // into a job -- a list of steps, each step one pass of the oblivious pipeline
 // split into tile-sized work items -- and writes it into a host-mapped ring.
 // A persistent kernel (one CTA per SM slot) ingests published jobs into a
-// device-side job table and runs their items: every CTA claims the next item
-// of one global sequence, waits (bounded) until the item's job has finished
-// all items of the previous steps, runs it and counts it done.  Jobs are
-// numbered in publication order and their items follow that order, so an
-// item only ever waits for earlier items and several jobs run at once.  The
-// kernel exits by itself once nothing is left to do for a short idle time
-// and the host relaunches it when new jobs arrive.
+// device-side job table.  Each job has one open step at a time; every CTA
+// takes a ready item of the oldest open job that has one, runs it and counts
+// it done, and the step's last item opens the next step.  Many jobs run at
+// once, and an item never waits for another.  The kernel exits by itself
+// once nothing is left to do for a short idle time, and the host relaunches
+// it when new jobs arrive.
 #pragma once
 
 #include <cstdint>
@@ -281,24 +280,35 @@ struct DqCopyArgs {
 
 // ---- device-side state ---------------------------------------------------------
 
-struct DqSlot {
-    unsigned long long begin; // first item of the job in the global sequence
+// A job's slot in the device job table.  Only the job's current step is
+// open for claims: `claim` packs the step, its item count and the items
+// handed out so far, and a CTA takes item k by a compare-and-swap of k -> k+1.
+// The CTA that completes the step's last item opens the next step (or marks
+// the job complete with step DQ_STEP_DONE), so no CTA ever waits on an item
+// dependency: it only takes items that are ready.
+constexpr unsigned long long DQ_STEP_DONE = 0xFFFFull;
+__host__ __device__ constexpr unsigned long long dq_claim_word(unsigned long long step, unsigned long long ntiles)
+{
+    return (step << 48) | (ntiles << 24);
+}
+constexpr uint64_t DQ_MAX_ITEMS_PER_STEP = (1ull << 24) - 1;
+
+struct alignas(16) DqSlot {
+    unsigned long long claim; // [63:48] step | [47:24] items of the step | [23:0] items handed out
     unsigned long long seq;   // job held by the slot (0: none yet)
-    unsigned int nitems;
-    unsigned int done;     // completed items
-    int status;            // VELO_OK, or the first error of the job
-    unsigned int complete; // 1 once every item is done
+    unsigned int done;        // completed items of the current step
+    int status;               // VELO_OK, or the first error of the job
+    unsigned int nsteps;
+    unsigned int pad_;
 };
 
 struct DqState {
-    unsigned long long next_item;       // claim counter
-    unsigned long long published;       // items of every ingested job
-    unsigned long long ingested;        // jobs ingested (seqs 1..ingested)
-    unsigned long long completed_items; // items done
-    unsigned long long complete_below;  // every job with seq < complete_below is complete
-    int lock;                           // held while a CTA ingests or decides to exit
-    int exiting;                        // the grid is leaving; no more ingests
+    unsigned long long ingested;       // jobs ingested (seqs 1..ingested)
+    unsigned long long complete_below; // every job with seq < complete_below is complete
+    unsigned long long last_poll;      // %globaltimer of the last read of the host ring head
     unsigned long long launches;
+    int lock;    // held while a CTA ingests or decides to exit
+    int exiting; // the grid is leaving; no more ingests
     DqSlot slot[DQ_DEV_RING];
 };
 
@@ -310,6 +320,8 @@ struct DqHostCtl {
     unsigned long long done_seq[DQ_HOST_RING]; // seq of the last job completed in each ring slot
     int status[DQ_HOST_RING];
     int fault; // set when the consumer stopped on an inconsistent job table
+    int pad2_;
+    unsigned long long exited_launch; // the consumer launch that decided to exit (launches count from 1)
 };
 
 struct DqParams {

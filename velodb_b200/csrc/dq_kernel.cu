@@ -1,24 +1,24 @@
 // Device consumer of the persistent command queue (job format: dq.cuh).
 //
-// One CTA of 256 threads per SM slot (two per SM) loops: thread 0 decides
-// what the CTA does next, the CTA does it.
-//   WORK    thread 0 holds a claimed item of the global item sequence that
-//           lies inside a published job: it finds the job (a short forward
-//           walk over the device job table) and the step (binary search over
-//           the job's steps), claims the following item ahead, and waits --
-//           bounded on %globaltimer -- until the job has completed every item
-//           of the earlier steps (and, for the first step, until every job
-//           the job was ordered after is complete).  The CTA stages the
-//           step's argument block in shared memory and runs the tile.
-//   INGEST  the CTA whose claim is the first unpublished item copies the
-//           next job from the host-mapped ring into the device job table and
-//           publishes its items.
-//   WAIT    nothing to run yet: back off with __nanosleep.
-//   EXIT    every published job is done and either the host asked the
-//           queue to stop or nothing arrived for the idle time.
-// Every wait is bounded: a dependency wait that runs out records
-// VELO_ETIMEDOUT in the job's status and the item runs anyway, so the
-// launch always terminates; the host reads the status with the job.
+// One CTA of 256 threads per SM slot (two per SM) loops: warp 0 decides what
+// the CTA does next, the CTA does it.
+//   WORK    warp 0 took an item of a job's open step: its lanes read the
+//           claim words of up to 32 open jobs at once (oldest first) and the
+//           oldest job with an unclaimed item wins a compare-and-swap.  The
+//           CTA stages the step's argument block in shared memory, runs the
+//           tile and counts it done; the step's last item opens the job's
+//           next step, or completes the job and reports it to the host.  An
+//           item is only ever taken when its step is open, so no CTA waits
+//           on another item.
+//   INGEST  a new job is in the host-mapped ring: copy it into the device
+//           job table and open its first step.
+//   WAIT    nothing to take: back off with __nanosleep.
+//   EXIT    no open job, and the host asked the queue to stop or nothing
+//           arrived for the idle time.
+// A job ordered after others opens its first step only once they are all
+// complete.  If open jobs offer nothing to take for a whole wait limit the
+// grid stops and reports a fault word to the host, so the launch always
+// terminates.
 #include "dq.cuh"
 #include "net_host.cuh"
 
@@ -445,169 +445,154 @@ __device__ void dq_run(const DqStep& step, const unsigned char* s_args, uint32_t
     }
 }
 
-// ---- thread 0: the next action ---------------------------------------------------
+// ---- warp 0: the next action ------------------------------------------------------
 
 struct DqLocal {
-    unsigned long long cursor; // lowest job that can hold this CTA's next item
     uint64_t idle_since;
     uint32_t backoff;
 };
 
 struct alignas(16) DqShared {
-    unsigned long long next;  // the claim this CTA holds
-    unsigned long long seq;   // job to ingest
-    DqJobHdr hdr;             // header of the job being ingested
-    DqStep step;
-    uint32_t ds;              // device slot of the item's job
-    uint32_t tile;            // item index within the step
-    uint32_t rel;             // item index within the job
+    DqJobHdr hdr;       // header of the job being ingested
+    DqStep step;        // step of the claimed item
+    unsigned long long seq; // job to ingest
+    uint32_t ds;        // device slot of the item's job
+    uint32_t sidx;      // index of the step in its job
+    uint32_t tile;      // item index within the step
+    uint32_t nsteps;    // steps of the item's job
     int action;
 };
 
 __device__ __forceinline__ void dq_backoff(DqLocal& L)
 {
     __nanosleep(L.backoff);
-    L.backoff = L.backoff < 4096 ? L.backoff * 2 : 4096;
+    L.backoff = L.backoff < 2048 ? L.backoff * 2 : 2048;
 }
 
-// job holding claimed item x (x < published); false if none is found
-__device__ __forceinline__ bool dq_find_job(const DqParams& a, unsigned long long x, DqLocal& L, uint32_t& ds,
-                                            unsigned long long& begin, uint32_t& nsteps, uint64_t& after)
+__device__ __forceinline__ bool dq_claimable(unsigned long long claim)
+{
+    const unsigned long long step = claim >> 48, nt = (claim >> 24) & 0xFFFFFFull, k = claim & 0xFFFFFFull;
+    return step != DQ_STEP_DONE && k < nt;
+}
+
+// Warp 0: takes a ready item of the oldest open job.  The lanes read the
+// claim words of 32 consecutive jobs at once; the oldest claimable job's lane
+// adds one to its claim word and owns item k if the word it replaced still
+// had k below the step's item count (a lost race leaves the count past the
+// end, which nothing reads, and the warp looks again).  Claims only follow a
+// read that saw an unclaimed item, so the count exceeds the step's items by
+// at most one per CTA.
+__device__ bool dq_claim(const DqParams& a, DqShared& S)
 {
     DqState* st = a.st;
-    const unsigned long long ing = dq_vol(st->ingested);
-    // jobs more than a host ring behind the newest are complete (the host
-    // reuses a ring slot only after its job completed), so they cannot
-    // hold an unfinished item
-    const unsigned long long lo = ing > (unsigned long long)DQ_HOST_RING ? ing - DQ_HOST_RING + 1 : 1;
-    if (L.cursor < lo)
-        L.cursor = lo;
-    for (; L.cursor <= ing; L.cursor++) {
-        const uint32_t d = (uint32_t)((L.cursor - 1) % DQ_DEV_RING);
-        const DqSlot& sl = st->slot[d];
-        if (dq_acq(&sl.seq) != L.cursor)
-            continue;
-        const unsigned long long b = dq_vol(sl.begin);
-        const unsigned int n = dq_vol(sl.nitems);
-        if (x >= b && x < b + n) {
-            ds = d;
-            begin = b;
-            const DqJob& J = a.table[d];
-            nsteps = __ldcg(&J.h.nsteps);
-            after = __ldcg(&J.h.after);
-            return true;
+    const int lane = threadIdx.x & 31;
+    unsigned long long lo = 0, hi = 0;
+    if (lane == 0) {
+        lo = dq_acq(&st->complete_below);
+        hi = dq_vol(st->ingested);
+    }
+    lo = __shfl_sync(0xFFFFFFFFu, lo, 0);
+    hi = __shfl_sync(0xFFFFFFFFu, hi, 0);
+    for (unsigned long long base = lo; base <= hi; base += 32) {
+        const unsigned long long j = base + (unsigned long long)lane;
+        const uint32_t ds = (uint32_t)((j - 1) % DQ_DEV_RING);
+        DqSlot* sl = &st->slot[ds];
+        unsigned long long claim = 0;
+        bool ok = false;
+        if (j <= hi) {
+            const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(sl)); // { claim, seq }
+            claim = v.x;
+            ok = v.y == j && dq_claimable(claim);
+            if (ok && (claim >> 48) == 0 && (claim & 0xFFFFFFull) == 0) {
+                // the job's first item waits for the jobs it is ordered after
+                const uint64_t after = __ldcg(&a.table[ds].h.after);
+                ok = after == 0 || after < lo;
+            }
+        }
+        unsigned mask = __ballot_sync(0xFFFFFFFFu, ok);
+        for (int tries = 0; mask != 0 && tries < 64; tries++) {
+            const int leader = __ffs(mask) - 1;
+            bool got = false;
+            if (lane == leader) {
+                const unsigned long long old = atomicAdd(&sl->claim, 1ull);
+                got = dq_claimable(old);
+                claim = old;
+                ok = false;
+            }
+            got = __shfl_sync(0xFFFFFFFFu, got ? 1 : 0, leader) != 0;
+            if (got) {
+                if (lane == leader) {
+                    __threadfence(); // the item's inputs: everything the earlier steps wrote
+                    const uint32_t sidx = (uint32_t)(claim >> 48);
+                    S.ds = ds;
+                    S.sidx = sidx;
+                    S.tile = (uint32_t)(claim & 0xFFFFFFull);
+                    S.nsteps = __ldcg(&a.table[ds].h.nsteps);
+                    const uint4* src = reinterpret_cast<const uint4*>(&a.table[ds].steps[sidx]);
+                    reinterpret_cast<uint4*>(&S.step)[0] = __ldcg(src);
+                    reinterpret_cast<uint4*>(&S.step)[1] = __ldcg(src + 1);
+                }
+                __syncwarp();
+                return true;
+            }
+            mask = __ballot_sync(0xFFFFFFFFu, ok);
         }
     }
     return false;
 }
 
-__device__ int dq_decide(const DqParams& a, DqLocal& L, DqShared& S)
+// lane 0 of warp 0, nothing claimable: ingest, exit or back off
+__device__ int dq_idle(const DqParams& a, DqLocal& L, DqShared& S)
 {
     DqState* st = a.st;
-    const unsigned long long x = S.next;
-    const unsigned long long pub = dq_acq(&st->published);
-    if (x < pub) {
-        uint32_t ds = 0, nsteps = 0;
-        unsigned long long begin = 0;
-        uint64_t after = 0;
-        if (!dq_find_job(a, x, L, ds, begin, nsteps, after)) {
-            // the job table lost the item's job: stop the grid rather than
-            // run unknown work (never expected); the host fails every
-            // pending job when it sees the fault word
+    if (dq_vol(st->exiting))
+        return DQ_A_EXIT;
+    const uint64_t now = dq_now();
+    // the host ring head is read over the bus: at most once a microsecond
+    // for the whole grid
+    const unsigned long long last = dq_vol(st->last_poll);
+    if (now - last > 1000 && atomicCAS(&st->last_poll, last, (unsigned long long)now) == last) {
+        const unsigned long long head = dq_acq_sys(&a.ctl->head);
+        if (head > dq_vol(st->ingested) && atomicCAS(&st->lock, 0, 1) == 0) {
+            if (dq_vol(st->exiting)) {
+                atomicExch(&st->lock, 0);
+                return DQ_A_EXIT;
+            }
+            // another CTA may have ingested since `head` was compared: the
+            // next job must still be published
+            const unsigned long long ing = dq_vol(st->ingested);
+            if (head > ing) {
+                S.seq = ing + 1;
+                L.idle_since = 0;
+                return DQ_A_INGEST;
+            }
+            atomicExch(&st->lock, 0);
+        }
+    }
+    if (L.idle_since == 0)
+        L.idle_since = now;
+    const bool open_jobs = dq_acq(&st->complete_below) <= dq_vol(st->ingested);
+    if (open_jobs) {
+        if (now - L.idle_since > a.wait_ns) {
+            // open jobs, yet nothing to take for a whole wait limit: the job
+            // table is inconsistent (never expected); stop, and let the host
+            // fail the pending jobs
             atomicExch(&st->exiting, 1);
             *const_cast<volatile int*>(&a.ctl->fault) = 1;
             __threadfence_system();
             return DQ_A_EXIT;
         }
-        const DqJob& J = a.table[ds];
-        const uint32_t rel = (uint32_t)(x - begin);
-        uint32_t lo = 0, hi = nsteps - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (__ldcg(&J.steps[mid].begin) <= rel)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        DqStep step;
-        {
-            const uint4* src = reinterpret_cast<const uint4*>(&J.steps[lo]);
-            uint4* dst = reinterpret_cast<uint4*>(&step);
-            dst[0] = __ldcg(src);
-            dst[1] = __ldcg(src + 1);
-        }
-        S.step = step;
-        S.ds = ds;
-        S.rel = rel;
-        S.tile = rel - step.begin;
-        // claim the following item now, so the claim overlaps this item
-        S.next = atomicAdd(&st->next_item, 1ull);
-        const uint64_t t0 = dq_now();
-        bool late = false;
-        if (lo == 0 && after != 0) {
-            uint32_t spins = 0;
-            while (dq_acq(&st->complete_below) <= after) {
-                if (dq_now() - t0 > a.wait_ns) {
-                    late = true;
-                    break;
-                }
-                __nanosleep(spins++ < 64 ? 64 : 512);
-            }
-        }
-        if (step.begin != 0) {
-            uint32_t spins = 0;
-            while (dq_acq32(&st->slot[ds].done) < step.begin) {
-                if (dq_now() - t0 > a.wait_ns) {
-                    late = true;
-                    break;
-                }
-                __nanosleep(spins++ < 64 ? 32 : 256);
-            }
-        }
-        if (late)
-            atomicCAS(&st->slot[ds].status, (int)VELO_OK, (int)VELO_ETIMEDOUT);
-        L.idle_since = 0;
-        L.backoff = 32;
-        return DQ_A_WORK;
-    }
-    if (dq_vol(st->exiting))
-        return DQ_A_EXIT;
-    if (x != pub) {
-        // another CTA holds the first unpublished item and polls the host
-        dq_backoff(L);
-        return DQ_A_WAIT;
-    }
-    const unsigned long long head = dq_acq_sys(&a.ctl->head);
-    if (head > dq_vol(st->ingested)) {
-        if (atomicCAS(&st->lock, 0, 1) == 0) {
-            if (dq_vol(st->exiting)) {
-                atomicExch(&st->lock, 0);
-                return DQ_A_EXIT;
-            }
-            S.seq = dq_vol(st->ingested) + 1;
-            return DQ_A_INGEST;
-        }
-        dq_backoff(L);
-        return DQ_A_WAIT;
-    }
-    const uint64_t now = dq_now();
-    if (L.idle_since == 0)
-        L.idle_since = now;
-    if (now - L.idle_since > a.wait_ns) {
-        // published items neither finished nor claimable for a whole wait
-        // limit: the job table is inconsistent (never expected); stop
-        atomicExch(&st->exiting, 1);
-        *const_cast<volatile int*>(&a.ctl->fault) = 1;
-        __threadfence_system();
-        return DQ_A_EXIT;
-    }
-    if (dq_vol(a.ctl->stop) != 0 || now - L.idle_since > a.idle_ns) {
+    } else if (dq_vol(a.ctl->stop) != 0 || now - L.idle_since > a.idle_ns) {
         if (atomicCAS(&st->lock, 0, 1) == 0) {
             const bool drained = dq_acq_sys(&a.ctl->head) == dq_vol(st->ingested)
-                && dq_acq(&st->completed_items) == dq_acq(&st->published);
+                && dq_acq(&st->complete_below) > dq_vol(st->ingested);
             if (drained) {
                 st->exiting = 1;
                 __threadfence();
+                // tell the host this launch is leaving: a job it publishes
+                // from now on needs a new launch
+                *const_cast<volatile unsigned long long*>(&a.ctl->exited_launch) = dq_vol(st->launches);
+                __threadfence_system();
             }
             atomicExch(&st->lock, 0);
             if (drained)
@@ -616,6 +601,20 @@ __device__ int dq_decide(const DqParams& a, DqLocal& L, DqShared& S)
     }
     dq_backoff(L);
     return DQ_A_WAIT;
+}
+
+// warp 0
+__device__ int dq_decide(const DqParams& a, DqLocal& L, DqShared& S)
+{
+    if (dq_claim(a, S)) {
+        L.idle_since = 0;
+        L.backoff = 32;
+        return DQ_A_WORK;
+    }
+    int act = DQ_A_WAIT;
+    if ((threadIdx.x & 31) == 0)
+        act = dq_idle(a, L, S);
+    return __shfl_sync(0xFFFFFFFFu, act, 0);
 }
 
 // ---- the CTA: ingest a job ------------------------------------------------------
@@ -632,7 +631,7 @@ __device__ void dq_ingest(const DqParams& a, DqShared& S)
     }
     __syncthreads();
     const DqJobHdr h = S.hdr;
-    const bool ok = h.seq == seq && h.nsteps >= 1 && h.nsteps <= (uint32_t)DQ_MAX_STEPS && h.nitems >= 1
+    const bool ok = h.seq == seq && h.nsteps >= 1 && h.nsteps <= (uint32_t)DQ_MAX_STEPS
         && h.arg_bytes <= (uint32_t)DQ_ARG_BYTES;
     if (ok) {
         const uint4* ss = reinterpret_cast<const uint4*>(src->steps);
@@ -653,27 +652,27 @@ __device__ void dq_ingest(const DqParams& a, DqShared& S)
         if (!ok) {
             // a malformed job (never written by this library's planner): a
             // one-item job that reports VELO_EINVAL
-            __stcg(&dst->h.nsteps, 1u);
-            __stcg(&dst->h.after, (uint64_t)0);
+            DqJobHdr bad {};
+            bad.seq = seq;
+            bad.nsteps = 1;
+            bad.nitems = 1;
             DqStep nop {};
             nop.kind = DQ_K_NOP;
             nop.ntiles = 1;
-            const uint4* np = reinterpret_cast<const uint4*>(&nop);
-            __stcg(reinterpret_cast<uint4*>(&dst->steps[0]), np[0]);
-            __stcg(reinterpret_cast<uint4*>(&dst->steps[0]) + 1, np[1]);
+            for (int i = 0; i < 4; i++)
+                __stcg(reinterpret_cast<uint4*>(&dst->h) + i, reinterpret_cast<const uint4*>(&bad)[i]);
+            __stcg(reinterpret_cast<uint4*>(&dst->steps[0]), reinterpret_cast<const uint4*>(&nop)[0]);
+            __stcg(reinterpret_cast<uint4*>(&dst->steps[0]) + 1, reinterpret_cast<const uint4*>(&nop)[1]);
         }
-        const unsigned int nitems = ok ? h.nitems : 1u;
-        sl.complete = 0;
+        __threadfence();
         sl.done = 0;
         sl.status = ok ? (int)VELO_OK : (int)VELO_EINVAL;
-        sl.nitems = nitems;
-        sl.begin = dq_vol(st->published);
+        sl.nsteps = ok ? h.nsteps : 1u;
+        sl.claim = dq_claim_word(0, __ldcg(&dst->steps[0].ntiles));
         __threadfence();
         sl.seq = seq;
         __threadfence();
         st->ingested = seq;
-        __threadfence();
-        atomicAdd(&st->published, (unsigned long long)nitems);
         __threadfence();
         atomicExch(&st->lock, 0);
     }
@@ -681,31 +680,39 @@ __device__ void dq_ingest(const DqParams& a, DqShared& S)
 
 // ---- thread 0: count an item done ----------------------------------------------
 
-__device__ void dq_complete(const DqParams& a, uint32_t ds)
+__device__ void dq_complete(const DqParams& a, const DqShared& S)
 {
     DqState* st = a.st;
-    DqSlot& sl = st->slot[ds];
+    DqSlot& sl = st->slot[S.ds];
     __threadfence();
     const unsigned int old = atomicAdd(&sl.done, 1u);
-    if (old + 1 == dq_vol(sl.nitems)) {
-        const unsigned long long seq = dq_vol(sl.seq);
-        const int hs = (int)((seq - 1) % DQ_HOST_RING);
-        a.ctl->status[hs] = dq_vol(sl.status);
-        __threadfence_system();
-        *const_cast<volatile unsigned long long*>(&a.ctl->done_seq[hs]) = seq;
-        __threadfence_system();
-        sl.complete = 1;
+    if (old + 1 != S.step.ntiles)
+        return;
+    // the step's last item: open the next step, or complete the job
+    sl.done = 0;
+    const uint32_t next = S.sidx + 1;
+    if (next < S.nsteps) {
+        const uint32_t nt = __ldcg(&a.table[S.ds].steps[next].ntiles);
         __threadfence();
-        // advance the "every job below is complete" mark over finished jobs
-        for (int it = 0; it < DQ_DEV_RING; it++) {
-            const unsigned long long c = dq_acq(&st->complete_below);
-            const DqSlot& cs = st->slot[(c - 1) % DQ_DEV_RING];
-            if (dq_acq(&cs.seq) != c || dq_acq32(&cs.complete) == 0)
-                break;
-            atomicCAS(&st->complete_below, c, c + 1);
-        }
+        atomicExch(&sl.claim, dq_claim_word(next, nt));
+        return;
     }
-    atomicAdd(&st->completed_items, 1ull);
+    const unsigned long long seq = dq_vol(sl.seq);
+    const int hs = (int)((seq - 1) % DQ_HOST_RING);
+    a.ctl->status[hs] = dq_vol(sl.status);
+    __threadfence_system();
+    *const_cast<volatile unsigned long long*>(&a.ctl->done_seq[hs]) = seq;
+    __threadfence_system();
+    atomicExch(&sl.claim, dq_claim_word(DQ_STEP_DONE, 0));
+    __threadfence();
+    // advance the "every job below is complete" mark over finished jobs
+    for (int it = 0; it < DQ_DEV_RING; it++) {
+        const unsigned long long c = dq_acq(&st->complete_below);
+        const DqSlot& cs = st->slot[(c - 1) % DQ_DEV_RING];
+        if (dq_acq(&cs.seq) != c || (dq_acq(&cs.claim) >> 48) != DQ_STEP_DONE)
+            break;
+        atomicCAS(&st->complete_below, c, c + 1);
+    }
 }
 
 __global__ void __launch_bounds__(DQ_THREADS, 2) k_dq(DqParams a)
@@ -715,12 +722,13 @@ __global__ void __launch_bounds__(DQ_THREADS, 2) k_dq(DqParams a)
     __shared__ DqSmall s_small;
     __shared__ __align__(16) DqShared S;
     VELO_TRACE_KERNEL(TS_K_DQ);
-    DqLocal L { 1, 0, 32 };
-    if (threadIdx.x == 0)
-        S.next = atomicAdd(&a.st->next_item, 1ull);
+    DqLocal L { 0, 32 };
     for (;;) {
-        if (threadIdx.x == 0)
-            S.action = dq_decide(a, L, S);
+        if (threadIdx.x < 32) {
+            const int act = dq_decide(a, L, S);
+            if (threadIdx.x == 0)
+                S.action = act;
+        }
         __syncthreads();
         const int act = S.action;
         if (act == DQ_A_EXIT)
@@ -735,39 +743,35 @@ __global__ void __launch_bounds__(DQ_THREADS, 2) k_dq(DqParams a)
             continue;
         }
         const DqStep step = S.step;
-        const uint32_t ds = S.ds;
         {
-            const uint4* src = reinterpret_cast<const uint4*>(a.table[ds].args + step.arg);
+            const uint4* src = reinterpret_cast<const uint4*>(a.table[S.ds].args + step.arg);
             for (int i = threadIdx.x; i < DQ_STEP_ARG_MAX / 16; i += DQ_THREADS)
                 reinterpret_cast<uint4*>(s_args)[i] = __ldcg(src + i);
         }
-        VELO_TRACE_WORK(S.rel);
+        VELO_TRACE_WORK(step.begin + S.tile);
         __syncthreads();
         dq_run(step, s_args, S.tile, sm, s_small);
         __syncthreads();
         if (threadIdx.x == 0)
-            dq_complete(a, ds);
+            dq_complete(a, S);
     }
 }
 
 // state before a launch: a fresh queue (first launch) or a resumed one
-// (claims of the previous grid are void; nothing is in flight)
 __global__ void k_dq_reset(DqState* st, int fresh)
 {
     if (threadIdx.x != 0)
         return;
     if (fresh) {
-        st->published = 0;
         st->ingested = 0;
-        st->completed_items = 0;
         st->complete_below = 1;
+        st->last_poll = 0;
         st->launches = 0;
         for (int i = 0; i < DQ_DEV_RING; i++) {
             st->slot[i].seq = 0;
-            st->slot[i].complete = 0;
+            st->slot[i].claim = dq_claim_word(DQ_STEP_DONE, 0);
         }
     }
-    st->next_item = st->published;
     st->lock = 0;
     st->exiting = 0;
     st->launches++;
