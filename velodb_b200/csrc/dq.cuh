@@ -293,7 +293,10 @@ __host__ __device__ constexpr unsigned long long dq_claim_word(unsigned long lon
 }
 constexpr uint64_t DQ_MAX_ITEMS_PER_STEP = (1ull << 24) - 1;
 
-struct alignas(16) DqSlot {
+// one 128-byte line per slot: every CTA adds to the claim and done words of
+// the open jobs, which must not share lines with each other or with the
+// queue-wide words below
+struct alignas(128) DqSlot {
     unsigned long long claim; // [63:48] step | [47:24] items of the step | [23:0] items handed out
     unsigned long long seq;   // job held by the slot (0: none yet)
     unsigned int done;        // completed items of the current step
@@ -303,12 +306,15 @@ struct alignas(16) DqSlot {
 };
 
 struct DqState {
-    unsigned long long ingested;       // jobs ingested (seqs 1..ingested)
-    unsigned long long complete_below; // every job with seq < complete_below is complete
-    unsigned long long last_poll;      // %globaltimer of the last read of the host ring head
+    // read by every idle CTA: one line of their own
+    alignas(128) unsigned long long ingested; // jobs ingested (seqs 1..ingested)
+    unsigned long long complete_below;        // every job with seq < complete_below is complete
+    int exiting;                              // the grid is leaving; no more ingests
+    unsigned int host_stop;                   // device copy of the host's stop word
+    // the host-ring poller's words
+    alignas(128) unsigned long long last_poll; // %globaltimer of the last read of the host ring
     unsigned long long launches;
-    int lock;    // held while a CTA ingests or decides to exit
-    int exiting; // the grid is leaving; no more ingests
+    int lock; // held while a CTA ingests or decides to exit
     DqSlot slot[DQ_DEV_RING];
 };
 

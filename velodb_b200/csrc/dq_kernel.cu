@@ -68,11 +68,29 @@ __device__ __forceinline__ unsigned long long dq_acq(const unsigned long long* p
     return v;
 }
 
-__device__ __forceinline__ unsigned int dq_acq32(const unsigned int* p)
+// claim: the item's inputs (what the earlier steps wrote) become visible
+__device__ __forceinline__ unsigned long long dq_add_acquire(unsigned long long* p, unsigned long long v)
 {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
+    unsigned long long old;
+    asm volatile("atom.acquire.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
+
+// item done: the CTA's writes are released with the count, and the step's
+// last item acquires every other item's
+__device__ __forceinline__ unsigned int dq_add_acq_rel(unsigned int* p, unsigned int v)
+{
+    unsigned int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
+// opening a step releases everything the step's items wrote
+__device__ __forceinline__ void dq_exch_release(unsigned long long* p, unsigned long long v)
+{
+    unsigned long long old;
+    asm volatile("atom.release.gpu.global.exch.b64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    (void)old;
 }
 
 template <class T>
@@ -463,10 +481,13 @@ struct alignas(16) DqShared {
     int action;
 };
 
+// idle CTAs back off to 4 us (a sleep lasts up to twice the request): a CTA that finishes a step's last item takes
+// the next step's items itself, so the sleepers only add latency to steps
+// wider than the awake CTAs
 __device__ __forceinline__ void dq_backoff(DqLocal& L)
 {
     __nanosleep(L.backoff);
-    L.backoff = L.backoff < 2048 ? L.backoff * 2 : 2048;
+    L.backoff = L.backoff < 4096 ? L.backoff * 2 : 4096;
 }
 
 __device__ __forceinline__ bool dq_claimable(unsigned long long claim)
@@ -488,7 +509,7 @@ __device__ bool dq_claim(const DqParams& a, DqShared& S)
     const int lane = threadIdx.x & 31;
     unsigned long long lo = 0, hi = 0;
     if (lane == 0) {
-        lo = dq_acq(&st->complete_below);
+        lo = dq_vol(st->complete_below);
         hi = dq_vol(st->ingested);
     }
     lo = __shfl_sync(0xFFFFFFFFu, lo, 0);
@@ -514,7 +535,7 @@ __device__ bool dq_claim(const DqParams& a, DqShared& S)
             const int leader = __ffs(mask) - 1;
             bool got = false;
             if (lane == leader) {
-                const unsigned long long old = atomicAdd(&sl->claim, 1ull);
+                const unsigned long long old = dq_add_acquire(&sl->claim, 1ull);
                 got = dq_claimable(old);
                 claim = old;
                 ok = false;
@@ -522,7 +543,6 @@ __device__ bool dq_claim(const DqParams& a, DqShared& S)
             got = __shfl_sync(0xFFFFFFFFu, got ? 1 : 0, leader) != 0;
             if (got) {
                 if (lane == leader) {
-                    __threadfence(); // the item's inputs: everything the earlier steps wrote
                     const uint32_t sidx = (uint32_t)(claim >> 48);
                     S.ds = ds;
                     S.sidx = sidx;
@@ -548,11 +568,15 @@ __device__ int dq_idle(const DqParams& a, DqLocal& L, DqShared& S)
     if (dq_vol(st->exiting))
         return DQ_A_EXIT;
     const uint64_t now = dq_now();
-    // the host ring head is read over the bus: at most once a microsecond
-    // for the whole grid
+    // host memory is read over the bus: the ring head and the stop word at
+    // most once every two microseconds for the whole grid, by whichever idle
+    // CTA wins the poll, with plain (relaxed) loads; the others read the
+    // device copy of the stop word.  Polling loads are relaxed throughout:
+    // ordering comes from the claim and done atomics and the ingest's fence.
     const unsigned long long last = dq_vol(st->last_poll);
-    if (now - last > 1000 && atomicCAS(&st->last_poll, last, (unsigned long long)now) == last) {
-        const unsigned long long head = dq_acq_sys(&a.ctl->head);
+    if (now - last > 2000 && atomicCAS(&st->last_poll, last, (unsigned long long)now) == last) {
+        st->host_stop = dq_vol(a.ctl->stop);
+        const unsigned long long head = dq_vol(a.ctl->head);
         if (head > dq_vol(st->ingested) && atomicCAS(&st->lock, 0, 1) == 0) {
             if (dq_vol(st->exiting)) {
                 atomicExch(&st->lock, 0);
@@ -571,7 +595,7 @@ __device__ int dq_idle(const DqParams& a, DqLocal& L, DqShared& S)
     }
     if (L.idle_since == 0)
         L.idle_since = now;
-    const bool open_jobs = dq_acq(&st->complete_below) <= dq_vol(st->ingested);
+    const bool open_jobs = dq_vol(st->complete_below) <= dq_vol(st->ingested);
     if (open_jobs) {
         if (now - L.idle_since > a.wait_ns) {
             // open jobs, yet nothing to take for a whole wait limit: the job
@@ -582,7 +606,7 @@ __device__ int dq_idle(const DqParams& a, DqLocal& L, DqShared& S)
             __threadfence_system();
             return DQ_A_EXIT;
         }
-    } else if (dq_vol(a.ctl->stop) != 0 || now - L.idle_since > a.idle_ns) {
+    } else if (dq_vol(st->host_stop) != 0 || now - L.idle_since > a.idle_ns) {
         if (atomicCAS(&st->lock, 0, 1) == 0) {
             const bool drained = dq_acq_sys(&a.ctl->head) == dq_vol(st->ingested)
                 && dq_acq(&st->complete_below) > dq_vol(st->ingested);
@@ -625,6 +649,8 @@ __device__ void dq_ingest(const DqParams& a, DqShared& S)
     const unsigned long long seq = S.seq;
     const DqJob* src = a.ring + (seq - 1) % DQ_HOST_RING;
     DqJob* dst = a.table + (seq - 1) % DQ_DEV_RING;
+    // the job was written before the head that announced it
+    asm volatile("fence.acq_rel.sys;" ::: "memory");
     if (threadIdx.x < 4) {
         // the header, uncached: the host rewrites this ring slot for later jobs
         reinterpret_cast<uint4*>(&S.hdr)[threadIdx.x] = __ldcv(reinterpret_cast<const uint4*>(&src->h) + threadIdx.x);
@@ -684,8 +710,7 @@ __device__ void dq_complete(const DqParams& a, const DqShared& S)
 {
     DqState* st = a.st;
     DqSlot& sl = st->slot[S.ds];
-    __threadfence();
-    const unsigned int old = atomicAdd(&sl.done, 1u);
+    const unsigned int old = dq_add_acq_rel(&sl.done, 1u);
     if (old + 1 != S.step.ntiles)
         return;
     // the step's last item: open the next step, or complete the job
@@ -693,8 +718,7 @@ __device__ void dq_complete(const DqParams& a, const DqShared& S)
     const uint32_t next = S.sidx + 1;
     if (next < S.nsteps) {
         const uint32_t nt = __ldcg(&a.table[S.ds].steps[next].ntiles);
-        __threadfence();
-        atomicExch(&sl.claim, dq_claim_word(next, nt));
+        dq_exch_release(&sl.claim, dq_claim_word(next, nt));
         return;
     }
     const unsigned long long seq = dq_vol(sl.seq);
@@ -765,6 +789,7 @@ __global__ void k_dq_reset(DqState* st, int fresh)
     if (fresh) {
         st->ingested = 0;
         st->complete_below = 1;
+        st->host_stop = 0;
         st->last_poll = 0;
         st->launches = 0;
         for (int i = 0; i < DQ_DEV_RING; i++) {
