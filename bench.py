@@ -15,9 +15,11 @@ At N = 1 the same run also measures, each in its own key of `extras` and
 each checked against the oracle: the plain sort of 2^20 (u64 key, u32
 payload) rows and of 2^24 rows (inputs far beyond L2: the HBM case), the
 filter + group-by over the 6,001,215-row fact table, the batch of 512 uneven
-sorts and compactions (one persistent launch from a CUDA graph against 512
-plain launch sequences), and the served query stream (p50/p99 latency and
-throughput, served against plain one-at-a-time).
+sorts and compactions (one persistent launch from a CUDA graph, and as jobs of
+the persistent command queue, against 512 plain launch sequences), and the
+served query stream (p50/p99 latency and throughput, served on per-query
+streams and through the persistent command queue, against plain
+one-at-a-time).
 
 Every network pass is also timed on its own with CUDA events (the library's
 pass timer) and the line reports the achieved HBM bandwidth per pass kind:
@@ -752,34 +754,41 @@ def _lat(results, t_key="submit_ms"):
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
 
 
-def _served_form(S, tab, qs, budget, slots, plain_qps, persistent):
-    """One server form at saturation (every query offered at once) and under
-    Poisson arrivals at 0.9x and 3x the plain capacity."""
+def _served_form(S, tab, qs, qs_poisson, budget, slots, plain_qps, persistent, loads):
+    """One server form at saturation (every query of `qs` offered at once) and
+    under Poisson arrivals of `qs_poisson` at the given multiples of the plain
+    capacity."""
     nq = len(qs)
     srv = S.Server(tab, slots=slots, budget_bytes=budget, persistent=persistent)
     S.run_open_loop(srv, qs[:32], np.zeros(32))
     sat_res, sat_s = S.run_open_loop(srv, qs, np.zeros(nq))
-    loads = {}
-    for f in (0.9, 3.0):
-        r, s = S.run_open_loop(srv, qs, S.arrivals(nq, f * plain_qps, seed=int(f * 1000)))
-        loads[f"{f}x_plain_capacity"] = {"offered_qps": f * plain_qps, "achieved_qps": nq / s, **_lat(r)}
+    out_loads = {}
+    for f in loads:
+        r, s = S.run_open_loop(srv, qs_poisson, S.arrivals(len(qs_poisson), f * plain_qps, seed=int(f * 1000)))
+        out_loads[f"{f}x_plain_capacity"] = {"offered_qps": f * plain_qps, "achieved_qps": len(qs_poisson) / s,
+                                             **_lat(r)}
     st = srv.stats()
     srv.close()
     form = {"qps_saturation": nq / sat_s, **_lat(sat_res), "slots": slots,
-            "peak_inflight": st["peak_inflight"], "peak_arena_bytes": st["peak_arena_bytes"], "poisson": loads}
+            "peak_inflight": st["peak_inflight"], "peak_arena_bytes": st["peak_arena_bytes"], "poisson": out_loads}
     return form, sat_res
 
 
-def measure_serve(torch, nq=256, slots=16, persistent_slots=64):
+def measure_serve(torch, nq=256, n_poisson=1024, slots=16, persistent_slots=64):
     """A seeded query stream (50 % filter + group-by, 35 % two-way join +
     top-10, 15 % three-way chain; slice sizes 2^10..2^18) over resident tables
-    of 60 M / 15 M / 150 M rows, admitted by a 120 GB HBM budget.  Plain = the
-    same request loop with one slot, each query submitted after the previous
-    one returned.  Served = up to 16 queries in flight on their own streams;
+    of 60 M / 15 M / 150 M rows, admitted by a 120 GB HBM budget.
+
+    Plain = the same request loop with one slot: each query submitted after
+    the previous one returned (its capacity), and Poisson arrivals at 0.9x
+    that capacity.  Served = up to 16 queries in flight on their own streams;
     served_persistent = up to 64 queries in flight as jobs of one persistent
-    command queue.  Each at saturation (every query offered at once) and under
-    Poisson arrivals at 0.9x and 3x the plain capacity.  Latency is submit ->
-    result in host memory, on the host clock."""
+    command queue.  Each form at saturation (256 queries offered at once) and
+    under Poisson arrivals (1024 queries) at multiples of the plain capacity.
+    Latency is submit -> result in host memory, on the host clock.  `target`
+    compares each load point against the plain path's p99 under Poisson
+    arrivals at 0.9x its capacity (the same arrival process) and against its
+    closed-loop p99 (no queueing at all)."""
     from velodb_b200 import serving as S
 
     t0 = time.perf_counter()
@@ -790,29 +799,46 @@ def measure_serve(torch, nq=256, slots=16, persistent_slots=64):
     budget = int(min(120 << 30, free - (4 << 30)))
     lo, hi = SERVE_SIZES_LOG2
     qs = S.query_stream(tab, nq, seed=0xB200000000000004, lo_log2=lo, hi_log2=hi)
+    qp = S.query_stream(tab, n_poisson, seed=0xB200000000000005, lo_log2=lo, hi_log2=hi)
     srv = S.Server(tab, slots=1, budget_bytes=budget)
     S.run_closed_one_at_a_time(srv, qs[:16])
     plain_res, plain_s = S.run_closed_one_at_a_time(srv, qs)
     plain_qps = nq / plain_s
-    r09, _ = S.run_open_loop(srv, qs, S.arrivals(nq, 0.9 * plain_qps, seed=900))
+    r09, _ = S.run_open_loop(srv, qp, S.arrivals(n_poisson, 0.9 * plain_qps, seed=900))
     srv.close()
-    served, sat_res = _served_form(S, tab, qs, budget, slots, plain_qps, False)
-    served_p, sat_p = _served_form(S, tab, qs, budget, persistent_slots, plain_qps, True)
+    plain = {"qps": plain_qps, **_lat(plain_res), "poisson_0.9x": {"offered_qps": 0.9 * plain_qps, **_lat(r09)}}
+    served, sat_res = _served_form(S, tab, qs, qp, budget, slots, plain_qps, False, (0.9, 3.0))
+    served_p, sat_p = _served_form(S, tab, qs, qp, budget, persistent_slots, plain_qps, True,
+                                   (0.9, 3.0, 4.0, 5.0, 6.0))
 
     def same(rs):
         return bool(all(S.result_key(a) == S.result_key(b) and a.status == 0 and b.status == 0
                         for a, b in zip(plain_res, rs)))
 
+    def target(form):
+        # load points with >= 3x the plain throughput and a p99 no higher than
+        # the plain path's
+        pts = {k: v for k, v in form["poisson"].items() if v["achieved_qps"] >= 3.0 * plain_qps}
+        best = max(pts.items(), key=lambda kv: kv[1]["achieved_qps"], default=(None, None))
+        return {
+            "loads_at_3x_plain_throughput": sorted(pts),
+            "p99_vs_plain_poisson_0.9x": {k: v["p99_ms"] <= plain["poisson_0.9x"]["p99_ms"] for k, v in pts.items()},
+            "p99_vs_plain_closed_loop": {k: v["p99_ms"] <= plain["p99_ms"] for k, v in pts.items()},
+            "best": best[0],
+        }
+
     shapes = {S.SHAPE_NAMES[k]: int(sum(1 for q in qs if q.shape == k)) for k in S.SHAPE_NAMES}
     out = {
         "tables_rows": dict(S.FULL_SCALE), "resident_bytes": int(tab.bytes), "table_build_s": build_s,
-        "hbm_budget_bytes": budget, "sizes_log2": [lo, hi], "queries": nq, "mix": shapes,
-        "plain": {"qps": plain_qps, **_lat(plain_res),
-                  "poisson_0.9x": {"offered_qps": 0.9 * plain_qps, **_lat(r09)}},
+        "hbm_budget_bytes": budget, "sizes_log2": [lo, hi], "queries": nq, "poisson_queries": n_poisson,
+        "mix": shapes,
+        "plain": plain,
         "served": served,
         "served_persistent": served_p,
         "speedup_served_vs_plain": served["qps_saturation"] / plain_qps,
         "speedup_served_persistent_vs_plain": served_p["qps_saturation"] / plain_qps,
+        "target_served": target(served),
+        "target_served_persistent": target(served_p),
         "results_identical_alone_and_in_mix": same(sat_res) and same(sat_p),
         "timing": "host clock, submit -> result in host memory",
     }
@@ -1118,7 +1144,8 @@ def main():
         from velodb_b200._lib import VeloQuery, VeloQueryResult
 
         res = measure_serve(torch)
-        value, _ = aggregate_throughput(res["served"]["qps_saturation"], 1e3, world, device, scale=1.0)
+        # the served stream through the persistent command queue
+        value, _ = aggregate_throughput(res["served_persistent"]["qps_saturation"], 1e3, world, device, scale=1.0)
         line = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": res["queries"],
                 "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "int64", "data": "synthetic",

@@ -481,13 +481,15 @@ struct alignas(16) DqShared {
     int action;
 };
 
-// idle CTAs back off to 4 us (a sleep lasts up to twice the request): a CTA that finishes a step's last item takes
-// the next step's items itself, so the sleepers only add latency to steps
-// wider than the awake CTAs
-__device__ __forceinline__ void dq_backoff(DqLocal& L)
+// Idle CTAs back off exponentially (a sleep lasts up to twice the request):
+// to 1 us while jobs are open, so that the items of a newly opened step are
+// taken quickly, and to 4 us when nothing is open.  A CTA that finishes a
+// step's last item takes the next step's first item itself.
+__device__ __forceinline__ void dq_backoff(DqLocal& L, bool open_jobs)
 {
-    __nanosleep(L.backoff);
-    L.backoff = L.backoff < 4096 ? L.backoff * 2 : 4096;
+    const uint32_t cap = open_jobs ? 1024u : 4096u;
+    __nanosleep(L.backoff < cap ? L.backoff : cap);
+    L.backoff = L.backoff < cap ? L.backoff * 2 : cap;
 }
 
 __device__ __forceinline__ bool dq_claimable(unsigned long long claim)
@@ -623,7 +625,7 @@ __device__ int dq_idle(const DqParams& a, DqLocal& L, DqShared& S)
                 return DQ_A_EXIT;
         }
     }
-    dq_backoff(L);
+    dq_backoff(L, open_jobs);
     return DQ_A_WAIT;
 }
 
