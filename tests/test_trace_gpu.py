@@ -442,3 +442,54 @@ def test_ogroupby_bigint_trace_is_data_independent(T):
              (np.full(n, 2**63 - 1, np.int64), 1.0),                                    # one key, the maximum
              (rng.choice(np.array([-(2**63), 0, 2**63 - 1], np.int64), n), 0.0)]        # nothing selected
     assert_same_trace([trace_of(T, run(k, d)) for k, d in cases])
+
+
+# ---- persistent command queue ---------------------------------------------------------------
+
+def test_persistent_queue_traces_are_data_independent(T):
+    # a filter + group-by and a (key, payload) sort run as jobs of a fresh
+    # persistent queue: logical threads are numbered by the item within its
+    # job, so the trace does not depend on which CTA takes which item
+    from velodb_b200 import capi
+
+    n = 60_001
+    G = 8
+    tabs = [W.lineitem(n, seed=21), W.lineitem(n, seed=22)]
+    none_pass = W.lineitem(n, seed=23)
+    none_pass["disc"][:] = 3
+    tabs.append(none_pass)
+    cols = {k: torch.from_numpy(v).cuda() for k, v in tabs[0].items()}
+    li = _lib.VeloLineitem(*[cols[k].data_ptr() for k in capi.LINEITEM_COLS])
+    pr = W.LINEITEM_PRED
+    pred = _lib.VeloLineitemPred(pr["ship_lo"], pr["ship_hi"], pr["disc_lo"], pr["disc_hi"], pr["qty_lo"],
+                                 pr["qty_hi"])
+    sb = T.velo_filter_groupby_scratch_bytes(n, G)
+    scratch = torch.empty(sb, dtype=torch.uint8, device="cuda")
+    out = torch.empty((G, 6), dtype=torch.int64, device="cuda")
+    counts = torch.empty(2, dtype=torch.int64, device="cuda")
+    ns = 70_001
+    cap = 1 << 17
+    k = torch.empty(cap, dtype=torch.int64, device="cuda")
+    p = torch.empty(cap, dtype=torch.int32, device="cuda")
+
+    def run(i, tab):
+        def f():
+            for key, v in tab.items():
+                cols[key].copy_(torch.from_numpy(v))
+            keys, pay = W.sort_kp(ns, seed=i + 1) if i < 2 else (np.zeros(ns, np.uint64), np.zeros(ns, np.uint32))
+            dev_copy(k, keys.view(np.int64))
+            dev_copy(p, pay.view(np.int32))
+            torch.cuda.synchronize()
+            q = C.c_void_p()
+            # a long idle time: one consumer launch for the whole run
+            assert T.velo_init(C.byref(_lib.VeloConfig(0, 0, capi.QUEUE_PERSISTENT, 10_000_000)), C.byref(q)) == 0
+            t1, t2 = C.c_uint64(), C.c_uint64()
+            g = capi.make_cmd("FILTER_GROUPBY", C.addressof(li), n, C.addressof(pred), G, out, counts, scratch, sb)
+            s = capi.make_cmd("OSORT_KP", k, p, ns, cap)
+            assert T.velo_submit(q, C.byref(g), C.byref(t1)) == 0, T.velo_last_error_text()
+            assert T.velo_submit(q, C.byref(s), C.byref(t2)) == 0, T.velo_last_error_text()
+            assert T.velo_wait(q, t2.value, 30_000_000_000) == 0
+            assert T.velo_shutdown(q, 30_000) == 0
+        return f
+
+    assert_same_trace([trace_of(T, run(i, t)) for i, t in enumerate(tabs)])
