@@ -104,6 +104,12 @@ typedef struct velo_pass_time {
     float ms;
 } velo_pass_time;
 void velo_set_pass_timing(int on);
+/* Tune: run the in-tile merge passes of 4096-row sorts (key-payload rows and
+ * two- or three-word records) as one persistent CTA per SM that prefetches
+ * the next tile with bulk copies into a second shared-memory buffer while
+ * the current tile's levels run (0 = off, the default).  Same network, same
+ * results.  No reference counterpart. */
+void velo_set_merge_pipeline(int on);
 void velo_pass_times_clear(void);
 int velo_last_pass_times(velo_pass_time* out, int capacity);
 

@@ -84,6 +84,8 @@ void store_stage_times(const float* ms, int n);
 // after each network pass and appends (kind, log2 rows, row bytes, ms) of
 // every pass to the calling thread's list.
 bool pass_timing_on();
+// merge passes with bulk-copy prefetch (velo_set_merge_pipeline)
+bool merge_pipe_on();
 void store_pass_time(int kind, int log_n, int row_bytes, float ms);
 
 class StageTimer {

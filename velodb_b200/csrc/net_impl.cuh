@@ -4,6 +4,7 @@
 #pragma once
 
 #include "net_host.cuh"
+#include "pipe.cuh"
 
 namespace velo {
 
@@ -129,6 +130,44 @@ private:
     std::vector<cudaEvent_t> ev_;
 };
 
+// fault word of the bulk-copy merge kernels of this translation unit
+static __device__ int s_pipe_fault;
+
+// The bulk-copy merge pass (pipe.cuh) for this row type and tile shape, when
+// it is switched on (velo_set_merge_pipeline) and the word arrays allow bulk
+// copies; returns the grid (one CTA per SM) or 0 for the plain merge kernel.
+template <class R, int LOG_NT, int LOG_E>
+inline unsigned merge_pipe_grid(const typename R::Cols& c, size_t ntiles, cudaStream_t)
+{
+#ifdef VELO_TRACE
+    return 0;
+#else
+    if constexpr (!pipe_capable<R, LOG_NT, LOG_E>()) {
+        return 0;
+    } else {
+        if (!merge_pipe_on() || ntiles < 2 || !Stage<R>::aligned(c))
+            return 0;
+        static int done[64] = {};
+        static int sms_of[64] = {};
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+            return 0;
+        constexpr size_t smem = 2 * pipe_buf_bytes<R, PIPE_LOG_NT, PIPE_LOG_E>();
+        if (smem > MAX_SMEM_BYTES - 1024)
+            return 0;
+        if (!done[dev]) {
+            if (cudaFuncSetAttribute(k_merge_pipe<R, PIPE_LOG_NT, PIPE_LOG_E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem)
+                    != cudaSuccess
+                || cudaDeviceGetAttribute(&sms_of[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+                return 0;
+            done[dev] = 1;
+        }
+        return (unsigned)(ntiles < (size_t)sms_of[dev] ? ntiles : (size_t)sms_of[dev]);
+    }
+#endif
+}
+
 template <class R, int LOG_NT, int LOG_E>
 velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::vector<NetPass>& passes,
                        const uint32_t* tile_prefix, cudaStream_t st)
@@ -163,6 +202,10 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
+    const unsigned pipe_grid = compact ? 0u : merge_pipe_grid<R, LOG_NT, LOG_E>(c, grid, st);
+    int* pipe_fault = nullptr;
+    if (pipe_grid)
+        VELO_CUDA_TRY(cudaGetSymbolAddress((void**)&pipe_fault, s_pipe_fault), "cudaGetSymbolAddress");
     PassTimer timer(st, passes.size());
     for (size_t i = 0; i < passes.size(); i++) {
         cudaLaunchConfig_t cfg = {};
@@ -172,8 +215,19 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
         cfg.stream = st;
         cfg.attrs = attr;
         cfg.numAttrs = (i > 0 && !timer.on()) ? 1 : 0;
-        auto kern = compact ? k_comp : passes[i].kind == P_SORT_GLOBAL ? k_global : k_local;
-        VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, c, g, passes[i], tile_prefix), "network pass launch");
+        if (pipe_grid && passes[i].kind == P_SORT_MERGE) {
+            if constexpr (pipe_capable<R, LOG_NT, LOG_E>()) {
+                cfg.gridDim = dim3(pipe_grid);
+                cfg.blockDim = dim3(1u << PIPE_LOG_NT);
+                cfg.dynamicSmemBytes = 2 * pipe_buf_bytes<R, PIPE_LOG_NT, PIPE_LOG_E>();
+                VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_merge_pipe<R, PIPE_LOG_NT, PIPE_LOG_E>, c, g, passes[i].K,
+                                                 (int)grid, pipe_fault),
+                              "network merge pass launch");
+            }
+        } else {
+            auto kern = compact ? k_comp : passes[i].kind == P_SORT_GLOBAL ? k_global : k_local;
+            VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, c, g, passes[i], tile_prefix), "network pass launch");
+        }
         timer.mark(i);
     }
     timer.finish(passes, g.logN, RowBytes<R>::value);

@@ -119,6 +119,12 @@ extern "C" void velo_set_pass_timing(int on)
 
 extern "C" void velo_pass_times_clear(void) { g_pass_n = 0; }
 
+static std::atomic<int> g_merge_pipe { 0 };
+
+bool velo::merge_pipe_on() { return g_merge_pipe.load(std::memory_order_relaxed) != 0; }
+
+extern "C" void velo_set_merge_pipeline(int on) { g_merge_pipe.store(on ? 1 : 0, std::memory_order_relaxed); }
+
 extern "C" int velo_last_pass_times(velo_pass_time* out, int capacity)
 {
     const int n = capacity < g_pass_n ? capacity : g_pass_n;
