@@ -479,6 +479,7 @@ struct alignas(16) DqShared {
     uint32_t tile;      // item index within the step
     uint32_t nsteps;    // steps of the item's job
     int action;
+    int cont;           // 1: the CTA keeps the next step's first item (set after an item)
 };
 
 // Idle CTAs back off exponentially (a sleep lasts up to twice the request):
@@ -708,20 +709,27 @@ __device__ void dq_ingest(const DqParams& a, DqShared& S)
 
 // ---- thread 0: count an item done ----------------------------------------------
 
-__device__ void dq_complete(const DqParams& a, const DqShared& S)
+// Returns true when this CTA keeps the next step's first item: the CTA that
+// completes a step opens the next one with item 0 already taken, and S
+// describes that item.
+__device__ bool dq_complete(const DqParams& a, DqShared& S)
 {
     DqState* st = a.st;
     DqSlot& sl = st->slot[S.ds];
     const unsigned int old = dq_add_acq_rel(&sl.done, 1u);
     if (old + 1 != S.step.ntiles)
-        return;
+        return false;
     // the step's last item: open the next step, or complete the job
     sl.done = 0;
     const uint32_t next = S.sidx + 1;
     if (next < S.nsteps) {
-        const uint32_t nt = __ldcg(&a.table[S.ds].steps[next].ntiles);
-        dq_exch_release(&sl.claim, dq_claim_word(next, nt));
-        return;
+        const uint4* src = reinterpret_cast<const uint4*>(&a.table[S.ds].steps[next]);
+        reinterpret_cast<uint4*>(&S.step)[0] = __ldcg(src);
+        reinterpret_cast<uint4*>(&S.step)[1] = __ldcg(src + 1);
+        dq_exch_release(&sl.claim, dq_claim_word(next, S.step.ntiles) + 1);
+        S.sidx = next;
+        S.tile = 0;
+        return true;
     }
     const unsigned long long seq = dq_vol(sl.seq);
     const int hs = (int)((seq - 1) % DQ_HOST_RING);
@@ -739,6 +747,7 @@ __device__ void dq_complete(const DqParams& a, const DqShared& S)
             break;
         atomicCAS(&st->complete_below, c, c + 1);
     }
+    return false;
 }
 
 __global__ void __launch_bounds__(DQ_THREADS, 2) k_dq(DqParams a)
@@ -749,24 +758,27 @@ __global__ void __launch_bounds__(DQ_THREADS, 2) k_dq(DqParams a)
     __shared__ __align__(16) DqShared S;
     VELO_TRACE_KERNEL(TS_K_DQ);
     DqLocal L { 0, 32 };
+    bool have = false; // S already holds this CTA's next item
     for (;;) {
-        if (threadIdx.x < 32) {
-            const int act = dq_decide(a, L, S);
-            if (threadIdx.x == 0)
-                S.action = act;
-        }
-        __syncthreads();
-        const int act = S.action;
-        if (act == DQ_A_EXIT)
-            return;
-        if (act == DQ_A_WAIT) {
+        if (!have) {
+            if (threadIdx.x < 32) {
+                const int act = dq_decide(a, L, S);
+                if (threadIdx.x == 0)
+                    S.action = act;
+            }
             __syncthreads();
-            continue;
-        }
-        if (act == DQ_A_INGEST) {
-            dq_ingest(a, S);
-            __syncthreads();
-            continue;
+            const int act = S.action;
+            if (act == DQ_A_EXIT)
+                return;
+            if (act == DQ_A_WAIT) {
+                __syncthreads();
+                continue;
+            }
+            if (act == DQ_A_INGEST) {
+                dq_ingest(a, S);
+                __syncthreads();
+                continue;
+            }
         }
         const DqStep step = S.step;
         {
@@ -779,7 +791,9 @@ __global__ void __launch_bounds__(DQ_THREADS, 2) k_dq(DqParams a)
         dq_run(step, s_args, S.tile, sm, s_small);
         __syncthreads();
         if (threadIdx.x == 0)
-            dq_complete(a, S);
+            S.cont = dq_complete(a, S) ? 1 : 0;
+        __syncthreads();
+        have = S.cont != 0;
     }
 }
 
