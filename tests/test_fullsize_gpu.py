@@ -2,14 +2,16 @@
 
 * The batch of 512 instances (log-uniform 2^10..2^22 rows, even instances
   sorts of (u64 key, u32 payload), odd ones compactions with Bernoulli(0.3)
-  keep flags), run as one persistent launch replayed from a CUDA graph, must
-  equal the plain path (one launch sequence per instance) bit for bit on every
-  instance, and a stride sample of instances must equal the oracle.
+  keep flags), run as one persistent launch replayed from a CUDA graph and as
+  jobs of the persistent command queue, must equal the plain path (one launch
+  sequence per instance) bit for bit on every instance, and a stride sample
+  of instances must equal the oracle.
 * The served stream over the full resident tables (60 M-row fact table, 15 M
   dimension rows, 150 M-row second fact table) must give every query the same
-  result alone and in the mix, and a sample of each query shape must equal
-  the oracle (filter + group-by, two-way join) or a numpy computation
-  (three-way chain).
+  result alone and in the mix -- on per-query streams and through the
+  persistent command queue -- and a sample of each query shape must equal the
+  oracle (filter + group-by, two-way join) or a numpy computation (three-way
+  chain).
 """
 import numpy as np
 import pytest
@@ -100,6 +102,30 @@ def test_batch_512_instances_graph_replay_matches_plain_and_oracle(cuda, orc):
                                   np.ascontiguousarray(od[:, :8]).view(np.uint64).reshape(-1))
     del g
     b.close()
+    # the same 512 instances as jobs of one persistent command queue
+    _restore(items, insts)
+    scr, cmds = [], []
+    for d in items:
+        cap = capi.next_pow2(d["n"])
+        if d["kind"] == "sort":
+            cmds.append(capi.make_cmd("OSORT_KP", d["keys"], d["pay"], d["n"], cap))
+        else:
+            sc = torch.empty(capi.compact_scratch_bytes(cap), dtype=torch.uint8, device=cuda)
+            scr.append(sc)
+            d["count"].fill_(-1)
+            cmds.append(capi.make_cmd("OCOMPACT_KPM", d["keys"], d["pay"], d["marks"], d["n"], cap, d["count"], sc,
+                                      sc.numel()))
+    torch.cuda.synchronize()
+    with capi.Queue(persistent=True) as q:
+        for t in q.submit_batch(cmds):
+            q.wait(t)
+    for d, r in zip(items, ref):
+        cap = capi.next_pow2(d["n"])
+        for k in ("keys", "pay", "marks"):
+            if k in d:
+                assert torch.equal(d[k][:cap], r[k][:cap]), ("persistent queue", d["kind"], d["n"], k)
+        if "count" in d:
+            assert int(d["count"].item()) == int(r["count"].item())
 
 
 @pytest.fixture(scope="module")
@@ -167,3 +193,11 @@ def test_served_full_tables_alone_and_in_the_mix(full_tables, orc):
             _check_query(orc, tab, q, r)
             seen[q.shape] += 1
     assert all(v > 0 for v in seen.values())
+    # the same stream through one persistent command queue: every result as alone
+    pq = S.Server(tab, slots=64, budget_bytes=budget, persistent=True)
+    rp, _ = S.run_open_loop(pq, qs, np.zeros(len(qs)))
+    st = pq.stats()
+    pq.close()
+    assert st["peak_inflight"] > 1
+    for a, p in zip(ra, rp):
+        assert p.status == 0 and S.result_key(a) == S.result_key(p)
