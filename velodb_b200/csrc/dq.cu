@@ -42,18 +42,13 @@ uint32_t DqPlan::steps() const
     return job_->h.nsteps;
 }
 
-bool DqPlan::ok() const
-{
-    return job_->h.pad_[0] == 0;
-}
-
 namespace {
 
 // appends steps and argument blocks to a plan; a job that outgrows the limits
-// is marked failed (header pad word 0), reported when it is published
+// is marked, and refused when it is published
 class B {
 public:
-    explicit B(DqPlan& p) : j_(p.job()) {}
+    explicit B(DqPlan& p) : p_(p), j_(p.job()) {}
     template <class A>
     uint32_t arg(const A& a)
     {
@@ -120,9 +115,10 @@ public:
         const uint64_t items = (n + DQ_ELEM_ITEM - 1) / DQ_ELEM_ITEM;
         step(kind, items ? items : 1, arg(e));
     }
-    void fail() { j_.h.pad_[0] = 1; }
+    void fail() { p_.overflow(); }
 
 private:
+    DqPlan& p_;
     DqJob& j_;
 };
 

@@ -24,10 +24,13 @@ public:
     DqJob& job() { return *job_; }
     // steps so far and whether every append fitted the job limits
     uint32_t steps() const;
-    bool ok() const;
+    bool ok() const { return !overflow_; }
+    // an append did not fit (too many steps, items or argument bytes)
+    void overflow() { overflow_ = true; }
 
 private:
     DqJob* job_;
+    bool overflow_ = false;
 };
 
 // appends one command of the command set; VELO_ENOTSUP for commands the
