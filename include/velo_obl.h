@@ -110,6 +110,19 @@ void velo_set_pass_timing(int on);
  * the current tile's levels run (0 = off, the default).  Same network, same
  * results.  No reference counterpart. */
 void velo_set_merge_pipeline(int on);
+/* Tune: load the rows of each in-tile merge and fused global pass of sorts
+ * in 4096-row tiles (key-payload rows, two- or three-word records) with one
+ * 3-D tensor-map copy per word array into shared memory instead of
+ * per-thread loads (0 = off, the default).  Same grid, same network, same
+ * results.  The tensor maps cover the calling GPU's own arrays.  No
+ * reference counterpart. */
+void velo_set_tensor_tile_loads(int on);
+/* Status of the tensor-map pass kernels on the current device since the
+ * first of them ran (synchronizes with the device): 0 none, 1 a tile copy
+ * did not complete in time, 2 / 3 a shared-memory destination / tensor map
+ * off its required alignment (the CTA then skipped its rows); -1 if it
+ * cannot be read.  No reference counterpart. */
+int velo_tensor_tile_status(void);
 void velo_pass_times_clear(void);
 int velo_last_pass_times(velo_pass_time* out, int capacity);
 

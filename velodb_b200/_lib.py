@@ -20,6 +20,8 @@ PROTOS = {
     "velo_set_stage_timing": (None, [i32]),
     "velo_set_pass_timing": (None, [i32]),
     "velo_set_merge_pipeline": (None, [i32]),
+    "velo_set_tensor_tile_loads": (None, [i32]),
+    "velo_tensor_tile_status": (i32, []),
     "velo_pass_times_clear": (None, []),
     "velo_last_pass_times": (i32, [vp, i32]),
     "velo_trace_enabled": (i32, []),

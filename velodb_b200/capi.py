@@ -44,6 +44,27 @@ def set_pass_timing(on: bool) -> None:
     lib().velo_set_pass_timing(1 if on else 0)
 
 
+def set_merge_pipeline(on: bool) -> None:
+    """Tune: in-tile merge passes as persistent CTAs with bulk-copy prefetch
+    (velo_set_merge_pipeline); off by default."""
+    lib().velo_set_merge_pipeline(1 if on else 0)
+
+
+def set_tensor_tile_loads(on: bool) -> None:
+    """Tune: merge and fused global passes load their rows with tensor-map
+    tile copies (velo_set_tensor_tile_loads); off by default."""
+    lib().velo_set_tensor_tile_loads(1 if on else 0)
+
+
+def tensor_tile_status() -> int:
+    """0 unless a tensor-map pass kernel recorded a fault code
+    (velo_tensor_tile_status)."""
+    return int(lib().velo_tensor_tile_status())
+
+
+TUNES = {"merge_pipeline": set_merge_pipeline, "tensor_tile_loads": set_tensor_tile_loads}
+
+
 def clear_pass_times() -> None:
     lib().velo_pass_times_clear()
 

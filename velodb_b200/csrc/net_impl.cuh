@@ -5,6 +5,7 @@
 
 #include "net_host.cuh"
 #include "pipe.cuh"
+#include "tma.cuh"
 
 namespace velo {
 
@@ -133,6 +134,30 @@ private:
 // fault word of the bulk-copy merge kernels of this translation unit
 static __device__ int s_pipe_fault;
 
+// The tensor-map pass kernels exist for this row type and tile shape (4096
+// rows or more, so that a fused global pass of up to 8 levels keeps at least
+// 16 contiguous rows; not in the instrumented trace build) ...
+template <class R, int LOG_NT, int LOG_E>
+constexpr bool tma_capable()
+{
+#ifdef VELO_TRACE
+    return false;
+#else
+    return TmaRows<R>::ok && Stage<R>::ok && LOG_NT + LOG_E >= 12;
+#endif
+}
+// ... and are switched on (velo_set_tensor_tile_loads), and the word arrays
+// allow tensor-map copies
+template <class R, int LOG_NT, int LOG_E>
+inline bool tma_passes_on(const typename R::Cols& c)
+{
+    if constexpr (!tma_capable<R, LOG_NT, LOG_E>()) {
+        return false;
+    } else {
+        return tensor_tiles_on() && Stage<R>::aligned(c) && tma_smem_bytes<R, LOG_NT, LOG_E>() <= MAX_SMEM_BYTES - 1024;
+    }
+}
+
 // The bulk-copy merge pass (pipe.cuh) for this row type and tile shape, when
 // it is switched on (velo_set_merge_pipeline) and the word arrays allow bulk
 // copies; returns the grid (one CTA per SM) or 0 for the plain merge kernel.
@@ -206,6 +231,8 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
     int* pipe_fault = nullptr;
     if (pipe_grid)
         VELO_CUDA_TRY(cudaGetSymbolAddress((void**)&pipe_fault, s_pipe_fault), "cudaGetSymbolAddress");
+    const bool tma = !compact && tma_passes_on<R, LOG_NT, LOG_E>(c);
+    int* tma_fault = tma ? tma_fault_word() : nullptr;
     PassTimer timer(st, passes.size());
     for (size_t i = 0; i < passes.size(); i++) {
         cudaLaunchConfig_t cfg = {};
@@ -223,6 +250,29 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
                 VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_merge_pipe<R, PIPE_LOG_NT, PIPE_LOG_E>, c, g, passes[i].K,
                                                  (int)grid, pipe_fault),
                               "network merge pass launch");
+            }
+        } else if (tma && (passes[i].kind == P_SORT_GLOBAL || passes[i].kind == P_SORT_MERGE)) {
+            if constexpr (tma_capable<R, LOG_NT, LOG_E>()) {
+                const NetPass& q = passes[i];
+                const bool gl = q.kind == P_SORT_GLOBAL;
+                TmaMaps maps;
+                void* base[3] = {};
+                int es[3] = {};
+                TmaRows<R>::arrays(c, base, es);
+                if (!tma_encode_pass(base, es, TmaRows<R>::NARR, g.logN, lt, gl ? q.L : 0, gl ? q.b_hi - q.L + 1 : lt,
+                                     &maps))
+                    return einval("tensor map encode failed");
+                auto kern = gl ? (wide_g ? k_sort_pass_tma<R, LOG_NT, LOG_E, N::PK_GLOBAL, MBG, true>
+                                         : k_sort_pass_tma<R, LOG_NT, LOG_E, N::PK_GLOBAL, MB, false>)
+                               : (wide ? k_sort_pass_tma<R, LOG_NT, LOG_E, N::PK_LOCAL, MBW, true>
+                                       : k_sort_pass_tma<R, LOG_NT, LOG_E, N::PK_LOCAL, MB, false>);
+                static int done_tma[4][64] = {};
+                const velo_status er =
+                    ensure_smem(kern, MAX_SMEM_BYTES, done_tma[(gl ? 2 : 0) + ((gl ? wide_g : wide) ? 1 : 0)]);
+                if (er != VELO_OK)
+                    return er;
+                cfg.dynamicSmemBytes = tma_smem_bytes<R, LOG_NT, LOG_E>();
+                VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, c, g, q, maps, tma_fault), "network pass launch");
             }
         } else {
             auto kern = compact ? k_comp : passes[i].kind == P_SORT_GLOBAL ? k_global : k_local;

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "net_host.cuh"
+#include "tma.cuh"
 
 namespace velo {
 
@@ -124,6 +125,98 @@ static std::atomic<int> g_merge_pipe { 0 };
 bool velo::merge_pipe_on() { return g_merge_pipe.load(std::memory_order_relaxed) != 0; }
 
 extern "C" void velo_set_merge_pipeline(int on) { g_merge_pipe.store(on ? 1 : 0, std::memory_order_relaxed); }
+
+static std::atomic<int> g_tensor_tiles { 0 };
+
+bool velo::tensor_tiles_on() { return g_tensor_tiles.load(std::memory_order_relaxed) != 0; }
+
+extern "C" void velo_set_tensor_tile_loads(int on) { g_tensor_tiles.store(on ? 1 : 0, std::memory_order_relaxed); }
+
+static std::mutex g_tma_fault_mu;
+static int* g_tma_fault[64] = {};
+
+int* velo::tma_fault_word()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return nullptr;
+    std::lock_guard<std::mutex> lk(g_tma_fault_mu);
+    if (!g_tma_fault[dev]) {
+        int* p = nullptr;
+        if (cudaMalloc((void**)&p, sizeof(int)) != cudaSuccess)
+            return nullptr;
+        if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) {
+            cudaFree(p);
+            return nullptr;
+        }
+        g_tma_fault[dev] = p;
+    }
+    return g_tma_fault[dev];
+}
+
+extern "C" int velo_tensor_tile_status(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return -1;
+    int* p = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_tma_fault_mu);
+        p = g_tma_fault[dev];
+    }
+    int code = 0;
+    if (p && cudaMemcpy(&code, p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return -1;
+    return code;
+}
+
+namespace {
+// cuTensorMapEncodeTiled, taken from the driver through the runtime (no
+// link against the driver library)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled()
+{
+    static std::once_flag once;
+    static EncodeTiled fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q {};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess
+            && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    return fn;
+}
+} // namespace
+
+bool velo::tma_encode_pass(void* const (&base)[3], const int (&es)[3], int narr, int log_n, int LT, int L, int b_lo,
+                           TmaMaps* out)
+{
+    const EncodeTiled enc = encode_tiled();
+    const int C = LT - L;
+    if (!enc || narr < 1 || narr > 3 || C < 4 || b_lo < C || b_lo > log_n || L < 0 || L > 8)
+        return false;
+    const int log_d0 = C < 8 ? C : 8;
+    for (int x = 0; x < narr; x++) {
+        if (es[x] != 4 && es[x] != 8)
+            return false;
+        const cuuint64_t dims[3] = { (cuuint64_t)1 << log_d0, (cuuint64_t)1 << (b_lo - log_d0),
+                                     (cuuint64_t)1 << (log_n - b_lo) };
+        const cuuint64_t strides[2] = { ((cuuint64_t)es[x]) << log_d0, ((cuuint64_t)es[x]) << b_lo };
+        const cuuint32_t box[3] = { 1u << log_d0, 1u << (C - log_d0), 1u << L };
+        const cuuint32_t estr[3] = { 1, 1, 1 };
+        const CUresult r = enc(&out->m[x], es[x] == 8 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_UINT32,
+                               3, base[x], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
 
 extern "C" int velo_last_pass_times(velo_pass_time* out, int capacity)
 {

@@ -412,8 +412,11 @@ struct Net {
     // SORT = true compiles only the bitonic pass kinds, false only ORCompact.
     // PK: the pass kinds this instantiation handles (a separate kernel each,
     // so that each gets its own register allocation)
+    // ST (not void): the pass's rows are already in shared memory in local
+    // row order, staged by a tensor-map tile load; ST::read(sm, T, l) reads
+    // row l (merge and fused global passes only)
     enum : int { PK_ANY = 0, PK_LOCAL = 1, PK_GLOBAL = 2 };
-    template <bool SORT, int PK = PK_ANY, bool WIDE = false>
+    template <bool SORT, int PK = PK_ANY, bool WIDE = false, class ST = void>
     __device__ static void run(const Cols& c, const NetGeom& g, const NetPass& p, const uint32_t* tile_prefix,
                                int cta, char* sm)
     {
@@ -441,7 +444,14 @@ struct Net {
         R v[E];
         int s = (p.kind == P_COMPACT_GLOBAL) ? smin : S0;
         const bool first = (p.kind == P_SORT_TILE) || (p.kind == P_COMPACT_TILE);
-        {
+        if constexpr (!std::is_void_v<ST>) {
+            // the first transpose's barrier ends these reads before the
+            // staged tile is overwritten
+            const int tp = tidpart(s);
+#pragma unroll
+            for (int e = 0; e < E; e++)
+                v[e] = ST::read(sm, T, tp | (e << s));
+        } else {
             const int tp = tidpart(s);
 #pragma unroll
             for (int e = 0; e < E; e++) {
