@@ -316,7 +316,8 @@ __device__ __forceinline__ void jseg_emit_topk_tile(const JRec::Cols& c, int nti
     uint64_t* k1 = k0 + SEG_TS;
     if (cand == 16) {
         // the 16 best in registers and warp shuffles (rows 4t .. 4t + 3 of
-        // thread t), then through 2 x 128 words of shared memory
+        // thread t), then through 2 x 128 words of shared memory; thread
+        // t < 16 stores row tk_row16(t)
         static_assert(SEG_TS == 4 * SEG_THREADS && SEG_THREADS == 256, "4 rows a thread, 8 warps");
         uint64_t x0[4], x1[4];
 #pragma unroll
@@ -324,15 +325,13 @@ __device__ __forceinline__ void jseg_emit_topk_tile(const JRec::Cols& c, int nti
             const int i = 4 * threadIdx.x + e;
             topk_key(so[seg_slot(i)], so[SEG_TS_PAD + seg_slot(i)], so[2 * SEG_TS_PAD + seg_slot(i)], x0[e], x1[e]);
         }
-        topk16_block(x0, x1, k0, TK_M1);
-        if (threadIdx.x < 4) {
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const size_t o = blk * 16 + 4 * threadIdx.x + e;
-                VELO_TRACE_AT(TS_TOPK, out0 + o);
-                out0[o] = x0[e];
-                out1[o] = x1[e];
-            }
+        uint64_t r0, r1;
+        topk16_block(x0, x1, k0, TK_M1, r0, r1);
+        if (threadIdx.x < 16) {
+            const size_t o = blk * 16 + tk_row16(threadIdx.x);
+            VELO_TRACE_AT(TS_TOPK, out0 + o);
+            out0[o] = r0;
+            out1[o] = r1;
         }
         return;
     }

@@ -140,23 +140,86 @@ __device__ __forceinline__ void tk_merge16(uint64_t (&x0)[4], uint64_t (&x1)[4],
     tk_cx_reg(x0[2], x1[2], x0[3], x1[3], asc, m1);
 }
 
-// Runs of 16 rows (lanes 4q .. 4q + 3 hold run q) sorted ascending for even
-// q, descending for odd q, are halved three times (lanes ^ 4, ^ 8, ^ 16: the
-// element-wise minimum of a run pair holds its 16 best rows as a bitonic
-// sequence, merged again); afterwards every 4-lane group holds the warp's 16
-// best rows ascending.
-__device__ __forceinline__ void tk_warp_rounds16(uint64_t (&x0)[4], uint64_t (&x1)[4], int lane, uint64_t m1)
+// keeps the smaller of row a and row b in a (a on equal keys)
+__device__ __forceinline__ void tk_min(uint64_t& a0, uint64_t& a1, uint64_t b0, uint64_t b1, uint64_t m1)
 {
+    const bool take = tk_gt(a0, a1, b0, b1, m1);
+    a0 = take ? b0 : a0;
+    a1 = take ? b1 : a1;
+}
+
+// Runs of 16 rows (lanes 4q .. 4q + 3 hold run q, row 4(l & 3) + e in
+// register e) sorted ascending for even q, descending for odd q, are halved
+// three times: the element-wise minimum of a run pair holds its 16 best rows
+// as a bitonic sequence, which four merge levels sort again.  Each round
+// keeps only the survivors, so the rows a lane works on halve with the rows:
+//   round 1 (runs q, q ^ 1: lane ^ 4): the lower lane keeps the minima of
+//     registers 0 and 1, the upper lane those of registers 2 and 3; the
+//     merged run p = l >> 3 is row 4(l & 3) + 2 h + j in register j
+//     (h = lane bit 2), merged by lane ^ 2, ^ 1, ^ 4 and the registers;
+//   round 2 (runs p, p ^ 1: lane ^ 8): the lower lane keeps register 0's
+//     minimum, the upper register 1's; run l >> 4 is row
+//     i(l) = 4(l & 3) + 2((l >> 2) & 1) + ((l >> 3) & 1), one a lane,
+//     merged by lane ^ 2, ^ 1, ^ 4, ^ 8;
+//   round 3 (lane ^ 16): both halves keep the minimum and merge ascending.
+// On return (r0, r1) of lane l holds row i(l & 15) of the warp's 16 best,
+// ascending; lanes l and l ^ 16 hold the same row.  Every partner and
+// direction depends only on the lane.
+__device__ __forceinline__ void tk_warp_rounds16(const uint64_t (&x0)[4], const uint64_t (&x1)[4], int lane,
+                                                 uint64_t m1, uint64_t& r0, uint64_t& r1)
+{
+    uint64_t a0[2], a1[2];
+    {
+        const bool h = (lane & 4) != 0;
 #pragma unroll
-    for (int r = 0; r < 3; r++) {
-        const int d = 4 << r;
+        for (int j = 0; j < 2; j++) {
+            const uint64_t p0 = __shfl_xor_sync(0xFFFFFFFFu, h ? x0[j] : x0[2 + j], 4);
+            const uint64_t p1 = __shfl_xor_sync(0xFFFFFFFFu, h ? x1[j] : x1[2 + j], 4);
+            a0[j] = h ? x0[2 + j] : x0[j];
+            a1[j] = h ? x1[2 + j] : x1[j];
+            tk_min(a0[j], a1[j], p0, p1, m1);
+        }
+        const bool asc = (lane & 8) == 0;
 #pragma unroll
-        for (int e = 0; e < 4; e++)
-            tk_cx_lane(x0[e], x1[e], d, true, m1);
-        // the merged run's index is the lane's bits above d; even ascending
-        const bool asc = r == 2 ? true : ((lane >> (3 + r)) & 1) == 0;
-        tk_merge16(x0, x1, lane, asc, m1);
+        for (int q = 0; q < 3; q++) {
+            const int d = q == 0 ? 2 : q == 1 ? 1 : 4;
+            const bool lower = (lane & d) == 0;
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+                tk_cx_lane(a0[j], a1[j], d, lower == asc, m1);
+        }
+        tk_cx_reg(a0[0], a1[0], a0[1], a1[1], asc, m1);
     }
+    {
+        const bool h = (lane & 8) != 0;
+        const uint64_t p0 = __shfl_xor_sync(0xFFFFFFFFu, h ? a0[0] : a0[1], 8);
+        const uint64_t p1 = __shfl_xor_sync(0xFFFFFFFFu, h ? a1[0] : a1[1], 8);
+        r0 = h ? a0[1] : a0[0];
+        r1 = h ? a1[1] : a1[0];
+        tk_min(r0, r1, p0, p1, m1);
+        const bool asc = (lane & 16) == 0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int d = q == 0 ? 2 : q == 1 ? 1 : q == 2 ? 4 : 8;
+            tk_cx_lane(r0, r1, d, ((lane & d) == 0) == asc, m1);
+        }
+    }
+    {
+        const uint64_t p0 = __shfl_xor_sync(0xFFFFFFFFu, r0, 16);
+        const uint64_t p1 = __shfl_xor_sync(0xFFFFFFFFu, r1, 16);
+        tk_min(r0, r1, p0, p1, m1);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int d = q == 0 ? 2 : q == 1 ? 1 : q == 2 ? 4 : 8;
+            tk_cx_lane(r0, r1, d, (lane & d) == 0, m1);
+        }
+    }
+}
+
+// row index held by lane l after tk_warp_rounds16
+__device__ __forceinline__ int tk_row16(int lane)
+{
+    return 4 * (lane & 3) + 2 * ((lane >> 2) & 1) + ((lane >> 3) & 1);
 }
 
 // Sorts the warp's runs of 16 rows, even runs ascending and odd descending
@@ -190,25 +253,24 @@ __device__ __forceinline__ void tk_warp_runs16(uint64_t (&x0)[4], uint64_t (&x1)
     tk_merge16(x0, x1, lane, (lane & 4) == 0, m1);
 }
 
-// The 16 best of the CTA's rows (4 a thread, blockDim.x = 256) ascending in
-// lanes 0..3 of warp 0 (x0/x1 of those lanes on return; other threads' rows
-// are unspecified).  scratch: 2 x 128 u64 of shared memory.
-__device__ __forceinline__ void topk16_block(uint64_t (&x0)[4], uint64_t (&x1)[4], uint64_t* scratch, uint64_t m1)
+// The 16 best of the CTA's rows (4 a thread, blockDim.x = 256): on return
+// lane l < 16 of warp 0 holds row tk_row16(l) of them, ascending, in (r0, r1)
+// (other threads' values are unspecified).  scratch: 2 x 128 u64 of shared
+// memory.
+__device__ __forceinline__ void topk16_block(uint64_t (&x0)[4], uint64_t (&x1)[4], uint64_t* scratch, uint64_t m1,
+                                             uint64_t& r0, uint64_t& r1)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     tk_warp_runs16(x0, x1, lane, m1);
-    tk_warp_rounds16(x0, x1, lane, m1);
+    tk_warp_rounds16(x0, x1, lane, m1, r0, r1);
     // the 8 warps' results: warp w's 16 rows to rows 16w .. 16w + 15, odd
     // warps reversed so that neighbouring runs form bitonic sequences
     __syncthreads();
-    if (lane < 4) {
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int r = 4 * lane + e;
-            const int slot = 16 * warp + ((warp & 1) ? 15 - r : r);
-            scratch[slot] = x0[e];
-            scratch[128 + slot] = x1[e];
-        }
+    if (lane < 16) {
+        const int r = tk_row16(lane);
+        const int slot = 16 * warp + ((warp & 1) ? 15 - r : r);
+        scratch[slot] = r0;
+        scratch[128 + slot] = r1;
     }
     __syncthreads();
     if (warp == 0) {
@@ -217,7 +279,7 @@ __device__ __forceinline__ void topk16_block(uint64_t (&x0)[4], uint64_t (&x1)[4
             x0[e] = scratch[4 * lane + e];
             x1[e] = scratch[128 + 4 * lane + e];
         }
-        tk_warp_rounds16(x0, x1, lane, m1);
+        tk_warp_rounds16(x0, x1, lane, m1, r0, r1);
     }
 }
 
