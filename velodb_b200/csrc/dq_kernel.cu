@@ -41,7 +41,7 @@ constexpr size_t DQ_SMEM = dq_max(
            dq_max(NetLI2::smem_bytes_compact(), NetLI3::smem_bytes_compact())),
     dq_max(dq_max(NetJ::smem_bytes_compact(), dq_max(NetR3::smem_bytes_sort(), NetR3K2::smem_bytes_compact())),
            dq_max(dq_max(LiTypes<3>::Seg::SMEM, JSEG_TOPK_SMEM),
-                  dq_max((size_t)2 * TK_RED_ROWS * 8, (size_t)FILL_TS * 8))));
+                  dq_max((size_t)2 * TK_RED_ROWS * 8, (size_t)FILL_TS_PAD * 8))));
 static_assert(DQ_SMEM <= 110 * 1024, "two consumer CTAs fit on an SM");
 static_assert(TK_RED_ROWS / 2 % DQ_THREADS == 0, "top-k rounds: whole compare-exchanges a thread");
 

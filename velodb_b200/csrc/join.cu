@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(1024) k_fill_carries(const DimCarry* tile_last
 __global__ void __launch_bounds__(FILL_THREADS) k_fill_apply(uint64_t* w0, const DimCarry* carry)
 {
     VELO_TRACE_KERNEL(velo_site_hash("k_fill_apply"));
-    __shared__ uint64_t sw[FILL_TS];
+    __shared__ uint64_t sw[FILL_TS_PAD];
     __shared__ DimCarry wsm[33];
     fill_apply_tile(w0, carry, blockIdx.x, sw, wsm);
 }

@@ -202,18 +202,24 @@ __device__ __forceinline__ void fill_carries_body(const DimCarry* tile_last, int
 }
 
 
-// joined flags of fill tile `blk`; sw: FILL_TS words, wsm: 33 entries of
+// shared-memory slot of fill-tile row i: one pad word after every 8 rows, so
+// that the 8 rows of each of 16 neighbouring threads fall in different banks
+constexpr int FILL_TS_PAD = FILL_TS + FILL_TS / 8;
+__device__ __forceinline__ int fill_slot(int i) { return i + (i >> 3); }
+
+// joined flags of fill tile `blk`; sw: FILL_TS_PAD words, wsm: 33 entries of
 // shared memory
 __device__ __forceinline__ void fill_apply_tile(uint64_t* w0, const DimCarry* carry, size_t blk, uint64_t* sw,
                                                 DimCarry* wsm)
 {
+    static_assert(FILL_RPT == 8, "fill_slot pads after each thread's 8 rows");
     const size_t base = blk * FILL_TS;
     for (int i = threadIdx.x; i < FILL_TS; i += FILL_THREADS) {
         VELO_TRACE_AT(TS_FILL, w0 + base + i);
-        sw[i] = w0[base + i];
+        sw[fill_slot(i)] = w0[base + i];
     }
     __syncthreads();
-    const int r0 = threadIdx.x * FILL_RPT;
+    const int r0 = threadIdx.x * (FILL_RPT + 1);
     DimCarry mine { 0, 0, 0 };
 #pragma unroll
     for (int r = 0; r < FILL_RPT; r++)
@@ -231,7 +237,7 @@ __device__ __forceinline__ void fill_apply_tile(uint64_t* w0, const DimCarry* ca
     __syncthreads();
     for (int i = threadIdx.x; i < FILL_TS; i += FILL_THREADS) {
         VELO_TRACE_AT(TS_FILL, w0 + base + i);
-        w0[base + i] = sw[i];
+        w0[base + i] = sw[fill_slot(i)];
     }
 }
 

@@ -3,7 +3,9 @@
 
 namespace velo {
 
-// the tile configurations compiled for record sorts (see net_inst_rec*.cu)
+// the tile configurations compiled for record sorts (see net_inst_rec*.cu);
+// a fused global pass keeps 16 contiguous rows (a 128-byte line of each word
+// array), so up to LT - 4 levels
 #define VELO_FOR_REC_TUNES(X)                                                                                          \
     X(8, 3)                                                                                                            \
     X(9, 3)                                                                                                            \
@@ -29,7 +31,7 @@ static velo_status rec_sort(uint64_t* const* words, uint64_t mask, size_t n, int
 #define X(a, b)                                                                                                        \
     if (log_nt == a && log_e == b) {                                                                                   \
         const int lt = a + b;                                                                                          \
-        plan_sort(logN, lt, lt - 5 < 8 ? lt - 5 : 8, passes);                                                          \
+        plan_sort(logN, lt, lt - 4 < 8 ? lt - 4 : 8, passes);                                                          \
         return launch_net<R, a, b>(c, g, passes, nullptr, st);                                                         \
     }
     VELO_FOR_REC_TUNES(X)

@@ -233,7 +233,9 @@ static velo_status run_fill(uint64_t* w0, uint64_t* w1, uint64_t* w2, size_t row
 using Rec3 = RowRec<3, 1, false>;
 using Rec3K2 = RowRec<3, 2, false>;
 constexpr int OP_LT = 12; // 4096-row tiles (CTA shape per record width: Tile12)
-constexpr int OP_LMAX = OP_LT - 5 < 8 ? OP_LT - 5 : 8;
+// up to 8 fused global levels: the 16 contiguous rows a segment keeps of
+// each 8-byte word array fill a 128-byte line
+constexpr int OP_LMAX = OP_LT - 4 < 8 ? OP_LT - 4 : 8;
 
 // scratch of the union-sort operators: 3 words x rows + fill carries + compaction
 inline size_t union_rows(size_t n)
