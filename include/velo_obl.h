@@ -57,8 +57,9 @@ typedef enum velo_type {
 } velo_type;
 
 /* Tile configuration of the network kernels: tile = 2^tile_log2 rows per CTA
- * (11..13), threads = 256/512/1024.  NULL = defaults (velo_osort_kp: 4096-row
- * tiles of 256 threads; compaction: 8192-row tiles of 512 threads). */
+ * (11..13), threads = 256/512/1024.  NULL = defaults (velo_osort_kp and
+ * velo_ocompact_kpm: 2048-row tiles of 256 threads up to 2^18 rows, 4096-row
+ * tiles of 256 threads above). */
 typedef struct velo_tune {
     uint32_t tile_log2;
     uint32_t threads;
@@ -187,8 +188,8 @@ velo_status velo_ocompact_kpm(uint64_t* d_keys, uint32_t* d_payload, uint8_t* d_
                               void* stream);
 size_t velo_compact_scratch_bytes(size_t capacity, const velo_tune* tune);
 
-/* Same compaction as velo_ocompact_kpm with the default tile configuration,
- * for callers that cannot allocate device memory -- an engine whose HBM is
+/* Same compaction as velo_ocompact_kpm (same output; 8192-row tiles of 512
+ * threads, which keep the fixed scratch small), for callers that cannot allocate device memory -- an engine whose HBM is
  * owned by its own pool allocator, a latency-critical path that cannot take
  * cudaMalloc's implicit device synchronisation, a plugin host without an
  * allocation hook.  It takes no scratch argument and allocates nothing: its

@@ -66,10 +66,11 @@ def test_compact_scratch_size():
     small = L.velo_compact_scratch_bytes(1000, None)
     big = L.velo_compact_scratch_bytes(1 << 23, None)
     assert 0 < small <= big
-    # one u32 count and one u32 prefix per 4096-row tile (the persistent
-    # queue's tiles; the plain path's 8192-row tiles need half), 256-byte
-    # aligned
+    # one u32 count and one u32 prefix per 4096-row tile (the default tiles
+    # above 2^18 rows and the persistent queue's), 256-byte aligned
     assert big == 2 * ((1 << 11) * 4) + 256
+    # up to 2^18 rows the default tiles hold 2048 rows: 128 of them
+    assert L.velo_compact_scratch_bytes(1 << 18, None) == 512 + 768  # 128 counts, 129 prefix words
     # with an explicit tune: that tune's tiles only (8192 rows here)
     t = _lib.VeloTune(13, 512)
     assert L.velo_compact_scratch_bytes(1 << 23, C.byref(t)) == 2 * ((1 << 10) * 4) + 256
