@@ -643,27 +643,34 @@ def aggregate_throughput(units_per_rank: float, ms: float, world: int, device=No
     return world * units_per_rank / (ms_max / 1e3) / scale, ms_max
 
 
+E2E_SETS = 3
+
+
 def e2e_pipelined_ms(torch, wl, steps):
-    """The end-to-end form with two input/output sets in flight: step i's
-    host -> device copy (one copy stream) and step i-1's device -> host copy
-    (another) run while a pipeline runs on the compute stream.  Every step
-    still moves all its bytes through PCIe; the two copy directions and the
-    SMs work at once.  Returns ms per step (CUDA events on the compute stream
-    around `steps` steps, the last result copy included)."""
-    sets = [wl.e2e_set(), wl.e2e_set()]
+    """The end-to-end form with E2E_SETS input/output sets in flight: step
+    i's host -> device copy (one copy stream) and step i-1's device -> host
+    copy (another) run while a pipeline runs on the compute stream.  Every
+    step still moves all its bytes through PCIe; the two copy directions and
+    the SMs work at once.  With three sets a set's round trip (copy in,
+    pipeline, copy out) may take up to three steps, so a step is bound by
+    the slowest of the three, not by their sum over two steps.  Returns ms
+    per step (CUDA events on the compute stream around `steps` steps, the
+    last result copy included)."""
+    n = E2E_SETS
+    sets = [wl.e2e_set() for _ in range(n)]
     hs, ds = torch.cuda.Stream(), torch.cuda.Stream()
     ms = torch.cuda.current_stream()
-    ev_in = [torch.cuda.Event(), torch.cuda.Event()]
-    ev_done = [torch.cuda.Event(), torch.cuda.Event()]
-    ev_free = [torch.cuda.Event(), torch.cuda.Event()]
+    ev_in = [torch.cuda.Event() for _ in range(n)]
+    ev_done = [torch.cuda.Event() for _ in range(n)]
+    ev_free = [torch.cuda.Event() for _ in range(n)]
 
     def run(k, start=None):
         for i in range(k):
-            b = i % 2
+            b = i % n
             with torch.cuda.stream(hs):
                 if start is not None and i == 0:
                     hs.wait_event(start)
-                if i >= 2:
+                if i >= n:
                     hs.wait_event(ev_free[b])  # set b's result has left the device
                 wl.e2e_in(sets[b])
                 ev_in[b].record(hs)
@@ -674,10 +681,10 @@ def e2e_pipelined_ms(torch, wl, steps):
                 ds.wait_event(ev_done[b])
                 wl.e2e_out(sets[b])
                 ev_free[b].record(ds)
-        for b in range(min(k, 2)):
+        for b in range(min(k, n)):
             ms.wait_event(ev_free[b])
 
-    run(4)
+    run(2 * n)
     torch.cuda.synchronize()
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.record(ms)
@@ -723,8 +730,8 @@ def measure(torch, capi, wl, args, world, device, peak, peak_kind, with_e2e=True
             e2e_value, ems = aggregate_throughput(wl.n, e2e_pipelined_ms(torch, wl, max(4, args.steps)), world,
                                                   device)
             e2e.update(value=e2e_value, ms_per_step=ems,
-                       form=("two input/output sets in flight: step i's host-to-device copy and step i-1's "
-                             "device-to-host copy overlap the pipeline"),
+                       form=(f"{E2E_SETS} input/output sets in flight: step i's host-to-device copy and step "
+                             "i-1's device-to-host copy overlap the pipeline"),
                        serial={"value": serial_value, "ms_per_step": serial_ms, "form": serial_form})
         else:
             # the batch replays one captured graph over fixed buffers and
