@@ -613,11 +613,24 @@ __device__ __forceinline__ void count_tile(const typename R::Cols& c, size_t n, 
     const size_t base = (size_t)cta << LT;
     const int T = 1 << LT;
     uint32_t cnt = 0;
-    for (int i = threadIdx.x; i < T; i += blockDim.x) {
-        const size_t gi = base + i;
-        const bool in = gi < n;
-        const size_t gs = in ? gi : 0; // every row index is public: read row 0 for pads
-        cnt += (in & MarkAt<R>::get(c, gs)) ? 1u : 0u;
+    // U loads a thread in flight before any is summed
+    constexpr int U = 8;
+    for (int i0 = threadIdx.x; i0 < T; i0 += U * (int)blockDim.x) {
+        bool m[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int i = i0 + u * (int)blockDim.x;
+            m[u] = false;
+            if (i < T) {
+                const size_t gi = base + i;
+                const bool in = gi < n;
+                const size_t gs = in ? gi : 0; // every row index is public: read row 0 for pads
+                m[u] = in & MarkAt<R>::get(c, gs);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            cnt += m[u] ? 1u : 0u;
     }
     uint32_t total;
     block_exclusive_scan(cnt, tmp, &total);

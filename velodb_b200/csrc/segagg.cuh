@@ -30,10 +30,12 @@ constexpr int SEG_TS = 1024;     // rows per tile
 constexpr int SEG_THREADS = 256; // 4 contiguous rows per thread
 constexpr int SEG_RPT = SEG_TS / SEG_THREADS;
 constexpr int SEG_MAX_G = 16;
-// smem row slot with one pad word per 8 rows, so the 8 contiguous rows of each
-// thread start on different banks
-__device__ __forceinline__ int seg_slot(int i) { return i + (i >> 3); }
-constexpr int SEG_TS_PAD = SEG_TS + SEG_TS / 8;
+// smem row slot with one pad word per 4 rows, so that the 4 contiguous rows
+// of each of 16 neighbouring threads (8-byte words, a half-warp a shared
+// memory wavefront) fall in different banks: thread t's row r at 5t + r
+__device__ __forceinline__ int seg_slot(int i) { return i + (i >> 2); }
+constexpr int SEG_TS_PAD = SEG_TS + SEG_TS / 4;
+static_assert(SEG_RPT == 4, "seg_slot pads after each thread's 4 rows");
 
 struct SegTileAgg {
     uint64_t head_key;
