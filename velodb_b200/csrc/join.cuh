@@ -316,21 +316,21 @@ __device__ __forceinline__ void jseg_emit_topk_tile(const JRec::Cols& c, int nti
                                                     const int64_t* carry_in, int cand, uint64_t* out0, uint64_t* out1,
                                                     size_t blk, char* sm)
 {
-    JSeg::emit_stage(c.w, (int)blk, ntiles, aggs, carry_in, JoinAgg::Params {}, sm);
-    const uint64_t* so = reinterpret_cast<const uint64_t*>(sm);
     uint64_t* k0 = reinterpret_cast<uint64_t*>(sm + JSEG_KEYS_OFF);
     uint64_t* k1 = k0 + SEG_TS;
     if (cand == 16) {
         // the 16 best in registers and warp shuffles (rows 4t .. 4t + 3 of
-        // thread t), then through 2 x 128 words of shared memory; thread
-        // t < 16 stores row tk_row16(t)
-        static_assert(SEG_TS == 4 * SEG_THREADS && SEG_THREADS == 256, "4 rows a thread, 8 warps");
+        // thread t, handed over in registers by the group-by's last pass),
+        // then through 2 x 128 words of shared memory; thread t < 16 stores
+        // row tk_row16(t)
+        static_assert(SEG_TS == 4 * SEG_THREADS && SEG_THREADS == 256 && SEG_RPT == 4, "4 rows a thread, 8 warps");
+        static_assert(JSeg::OW == 3, "group records (flag | key, sum, count)");
+        uint64_t o[SEG_RPT][JSeg::OW];
+        JSeg::emit_stage<true>(c.w, (int)blk, ntiles, aggs, carry_in, JoinAgg::Params {}, sm, o);
         uint64_t x0[4], x1[4];
 #pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int i = 4 * threadIdx.x + e;
-            topk_key(so[seg_slot(i)], so[SEG_TS_PAD + seg_slot(i)], so[2 * SEG_TS_PAD + seg_slot(i)], x0[e], x1[e]);
-        }
+        for (int e = 0; e < 4; e++)
+            topk_key(o[e][0], o[e][1], o[e][2], x0[e], x1[e]);
         uint64_t r0, r1;
         topk16_block(x0, x1, k0, TK_M1, r0, r1);
         if (threadIdx.x < 16) {
@@ -341,6 +341,8 @@ __device__ __forceinline__ void jseg_emit_topk_tile(const JRec::Cols& c, int nti
         }
         return;
     }
+    JSeg::emit_stage(c.w, (int)blk, ntiles, aggs, carry_in, JoinAgg::Params {}, sm);
+    const uint64_t* so = reinterpret_cast<const uint64_t*>(sm);
     for (int i = threadIdx.x; i < SEG_TS; i += SEG_THREADS)
         topk_key(so[seg_slot(i)], so[SEG_TS_PAD + seg_slot(i)], so[2 * SEG_TS_PAD + seg_slot(i)], k0[i], k1[i]);
     topk_net<SEG_TS / 2 / SEG_THREADS>(k0, k1, SEG_TS, cand, TK_M1, false);

@@ -579,8 +579,13 @@ struct SegAgg {
 
     // emit_rows without the stores: leaves the tile's OW output words of
     // row i at smem word x * SEG_TS_PAD + seg_slot(i) (after a barrier)
+    // REGS: the thread's SEG_RPT rows r0 .. r0 + SEG_RPT - 1 (r0 = 4t) go
+    // to regs[r][0 .. OW-1] instead of shared memory (no staging, no final
+    // barriers), for a consumer that only needs the thread's own rows
+    template <bool REGS = false>
     __device__ static void emit_stage(uint64_t* const* words, int tile, int ntiles, const SegTileAgg* aggs,
-                                      const int64_t* carry_in, const Params& prm, char* smem)
+                                      const int64_t* carry_in, const Params& prm, char* smem,
+                                      uint64_t (*regs)[OW] = nullptr)
     {
         uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
         int64_t* svals = reinterpret_cast<int64_t*>(smem + (size_t)SEG_TS_PAD * TW * 8);
@@ -651,6 +656,24 @@ struct SegAgg {
             uint64_t wp[W];
             row(sw, r0 - 1, wp);
             lead = (Agg::key(wp) == keys[0]);
+        }
+        if constexpr (REGS) {
+#pragma unroll
+            for (int r = 0; r < SEG_RPT; r++) {
+                if (r > 0)
+                    lead = lead & (keys[r] == keys[r - 1]);
+                const bool first_run_of_tile = (keys[r] == head_key);
+                if constexpr (FW == 1) {
+                    regs[r][0] = Agg::out_bits(keys[r]);
+                    regs[r][1] = (uint64_t)(!tail[r]) << 63;
+                } else {
+                    regs[r][0] = ((uint64_t)(!tail[r]) << 63) | Agg::out_bits(keys[r]);
+                }
+#pragma unroll
+                for (int i = 0; i < V; i++)
+                    regs[r][1 + FW + i] = (uint64_t)(pref[r][i] + (lead ? cin[i] : 0) + (first_run_of_tile ? tc[i] : 0));
+            }
+            return;
         }
         __syncthreads();
         // stage the output records in smem so the global stores stay coalesced
