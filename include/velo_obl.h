@@ -422,7 +422,8 @@ typedef struct velo_batch velo_batch;
  * previous pass of the same command.  Replaces the reference's one-command-
  * at-a-time persistent grid (src/cuda/persistent_kernel.cu:76-124,
  * src/cuda/task_manager.cu:26-78).  Results are identical to running each
- * command through velo_osort_kp / velo_ocompact_kpm with the same tune.
+ * command through velo_osort_kp / velo_ocompact_kpm with the same tune
+ * (NULL: 4096-row tiles of 256 threads).
  * Allocates the batch's device plan (cudaMalloc) here, never at launch. */
 velo_status velo_batch_create(const velo_batch_item* items, size_t n_items, const velo_tune* tune,
                               velo_batch** out);
