@@ -26,6 +26,12 @@ pass timer) and the line reports the achieved HBM bandwidth per pass kind:
 tile sort, in-tile merge, fused global levels, ORCompact tile and global
 passes.
 
+`e2e` is the same pipeline through the public API from pinned host buffers,
+every step's host -> device and device -> host copies inside the timed
+region, with three input/output sets in flight so that the copies of
+neighbouring steps overlap the pipeline; `e2e.serial` is the one step at a
+time form (copy in, pipeline, copy out).
+
 Multi-GPU: one process per GPU (torchrun); the path does not shard, so every
 rank runs an independent replica of the headline workload ("replicas only")
 and the aggregate throughput is the total rows of all ranks over the slowest
