@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(1024) k_seg_carries(const SegTileAgg* aggs, co
 }
 
 template <int W>
-__global__ void __launch_bounds__(SEG_THREADS) k_seg_emit(typename LiTypes<W>::Rec::Cols c, int ntiles,
+__global__ void __launch_bounds__(SEG_THREADS, 3) k_seg_emit(typename LiTypes<W>::Rec::Cols c, int ntiles,
                                                           const SegTileAgg* aggs, const int64_t* carry_in,
                                                           const uint32_t* tail_prefix, int G, int64_t* tile_out,
                                                           LiParams prm)

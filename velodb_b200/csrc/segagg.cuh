@@ -121,15 +121,16 @@ __device__ __forceinline__ int64_t warp_sum_i64(int64_t x)
     return x;
 }
 
-// Warp reduce-scatter of 32 int64 values a lane: five halving steps (each
-// lane keeps the half its lane bit selects and adds the partner's copy of
-// it); afterwards a[0] of lane L is the warp sum of value L.
-__device__ __forceinline__ void warp_reduce_scatter32(int64_t (&a)[32], int lane)
+// Warp reduce-scatter of 16 int64 values a lane: four halving steps over
+// lane bits 4..1 (each lane keeps the half its lane bit selects and adds the
+// partner's copy of it) and one add across lane bit 0; afterwards a[0] of
+// lane L is the warp sum of value L >> 1.
+__device__ __forceinline__ void warp_reduce_scatter16(int64_t (&a)[16], int lane)
 {
 #pragma unroll
-    for (int step = 0; step < 5; step++) {
+    for (int step = 0; step < 4; step++) {
         const int o = 16 >> step;
-        const int h = 16 >> step; // current length / 2
+        const int h = 8 >> step; // current length / 2
         const bool up = (lane & o) != 0;
 #pragma unroll
         for (int k = 0; k < h; k++) {
@@ -138,6 +139,7 @@ __device__ __forceinline__ void warp_reduce_scatter32(int64_t (&a)[32], int lane
             a[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
         }
     }
+    a[0] += __shfl_xor_sync(0xffffffffu, a[0], 1);
 }
 
 // Group records with a separate flag word (Agg::FLAG_WORD = true): o0 = the
@@ -514,15 +516,17 @@ struct SegAgg {
         // every row is folded into every slot with a mask
         __syncthreads();
         int64_t* red = reinterpret_cast<int64_t*>(smem); // reuse the tile area
-        // slots in chunks of 4: every lane folds its rows into 4 x 8 values
+        // slots in chunks of 2: every lane folds its rows into 2 x 8 values
         // (slot, value; values past 1+V stay zero), then a warp reduce-scatter
-        // leaves lane L with the warp sum of value L
+        // leaves lanes 2L and 2L + 1 with the warp sum of value L (chunks of
+        // 4 slots kept 32 sums a lane live: 102 registers, two CTAs an SM)
         static_assert(1 + V <= 8, "a slot's key and values fit 8 words");
+        constexpr int SLOTS = 2;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        for (int j0 = 0; j0 < G; j0 += 4) {
-            int64_t acc[32];
+        for (int j0 = 0; j0 < G; j0 += SLOTS) {
+            int64_t acc[8 * SLOTS];
 #pragma unroll
-            for (int q = 0; q < 32; q++)
+            for (int q = 0; q < 8 * SLOTS; q++)
                 acc[q] = 0;
             // the ranks of a thread's tails are distinct, so each slot takes
             // at most one of its rows: a select, not an add (the block sum
@@ -532,7 +536,7 @@ struct SegAgg {
             for (int r = 0; r < SEG_RPT; r++) {
                 const int64_t kv = Agg::out_key_from(keys[r]);
 #pragma unroll
-                for (int jj = 0; jj < 4; jj++) {
+                for (int jj = 0; jj < SLOTS; jj++) {
                     const bool hit = tail[r] & (rank == (uint32_t)(j0 + jj));
                     acc[jj * 8] = hit ? kv : acc[jj * 8];
 #pragma unroll
@@ -541,10 +545,11 @@ struct SegAgg {
                 }
                 rank += tail[r] ? 1u : 0u;
             }
-            warp_reduce_scatter32(acc, lane);
-            red[lane * 8 + warp] = acc[0];
+            warp_reduce_scatter16(acc, lane);
+            if ((lane & 1) == 0)
+                red[(lane >> 1) * 8 + warp] = acc[0];
             __syncthreads();
-            const int gn = G - j0 < 4 ? G - j0 : 4;
+            const int gn = G - j0 < SLOTS ? G - j0 : SLOTS;
             for (int q = threadIdx.x; q < gn * (1 + V); q += SEG_THREADS) {
                 const int jj = q / (1 + V), i = q - jj * (1 + V);
                 const size_t o = (size_t)tile * G * (1 + V) + (size_t)(j0 + jj) * (1 + V) + i;
