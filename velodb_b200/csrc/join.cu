@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(1024) k_jseg_carries(const SegTileAgg* aggs, c
     JSeg::carries(aggs, runs, ntiles, carry_in, tail_prefix, n_groups, sm);
 }
 
-__global__ void __launch_bounds__(SEG_THREADS) k_jseg_emit_topk(JRec::Cols c, int ntiles, const SegTileAgg* aggs,
+__global__ void __launch_bounds__(SEG_THREADS, 5) k_jseg_emit_topk(JRec::Cols c, int ntiles, const SegTileAgg* aggs,
                                                                 const int64_t* carry_in, int cand, uint64_t* out0,
                                                                 uint64_t* out1)
 {
@@ -198,8 +198,8 @@ extern "C" velo_status velo_join_groupby_topk(const velo_join_tables* t, const v
     k_jseg_summary<<<nts, SEG_THREADS, JSeg::SMEM_IN, st>>>(uc, s.aggs, s.runs);
     k_jseg_carries<<<1, 1024, JoinAgg::V * 1024 * 8 + 2 * 1024 * 4, st>>>(s.aggs, s.runs, nts, s.carry,
                                                                             s.tail_prefix, s.n_groups);
-    k_jseg_emit_topk<<<nts, SEG_THREADS, JSEG_TOPK_SMEM, st>>>(uc, nts, s.aggs, s.carry, cand, s.cand[0],
-                                                              s.cand[1]);
+    const size_t topk_smem = cand == 16 ? JSEG_TOPK16_SMEM : JSEG_TOPK_SMEM;
+    k_jseg_emit_topk<<<nts, SEG_THREADS, topk_smem, st>>>(uc, nts, s.aggs, s.carry, cand, s.cand[0], s.cand[1]);
     VELO_CUDA_TRY(cudaGetLastError(), "join group-by launch");
     tm.mark();
     // 6. top-k rounds over blocks of candidates (the union area is free now)

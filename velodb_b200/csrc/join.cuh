@@ -310,8 +310,12 @@ __device__ __forceinline__ void topk_out_body(const uint64_t* t0, const uint64_t
 // rows become top-k keys in shared memory and only its best `cand` are stored
 constexpr size_t JSEG_KEYS_OFF = (JSeg::SMEM + 15) & ~(size_t)15;
 constexpr size_t JSEG_TOPK_SMEM = JSEG_KEYS_OFF + (size_t)2 * SEG_TS * 8;
+// with 16 candidates a tile only 2 x 128 words of key scratch (topk16_block):
+// five CTAs an SM
+constexpr size_t JSEG_TOPK16_SMEM = JSEG_KEYS_OFF + (size_t)2 * 128 * 8;
 
 // group-by tile `blk` (SEG_THREADS threads); sm: JSEG_TOPK_SMEM bytes
+// (JSEG_TOPK16_SMEM when cand == 16)
 __device__ __forceinline__ void jseg_emit_topk_tile(const JRec::Cols& c, int ntiles, const SegTileAgg* aggs,
                                                     const int64_t* carry_in, int cand, uint64_t* out0, uint64_t* out1,
                                                     size_t blk, char* sm)
