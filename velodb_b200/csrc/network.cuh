@@ -415,16 +415,17 @@ struct Net {
     // ST (not void): the pass's rows are already in shared memory in local
     // row order, staged by a tensor-map tile load; ST::read(sm, T, l) reads
     // row l (merge and fused global passes only)
-    enum : int { PK_ANY = 0, PK_LOCAL = 1, PK_GLOBAL = 2 };
+    // PK_MERGE: the in-tile merges alone (no tile-sort code)
+    enum : int { PK_ANY = 0, PK_LOCAL = 1, PK_GLOBAL = 2, PK_MERGE = 3 };
     template <bool SORT, int PK = PK_ANY, bool WIDE = false, class ST = void>
     __device__ static void run(const Cols& c, const NetGeom& g, const NetPass& p, const uint32_t* tile_prefix,
                                int cta, char* sm)
     {
-        constexpr bool CT = SORT && PK == PK_LOCAL;
+        constexpr bool CT = SORT && (PK == PK_LOCAL || PK == PK_MERGE);
         constexpr bool BOFF = !WIDE;
         const size_t Np = (size_t)1 << g.logN;
         const bool is_global = PK == PK_GLOBAL ? true
-            : PK == PK_LOCAL                   ? false
+            : PK == PK_LOCAL || PK == PK_MERGE ? false
                                                : (p.kind == P_SORT_GLOBAL) || (p.kind == P_COMPACT_GLOBAL);
         int C = LT, b_lo = 0;
         size_t cta_bits = (size_t)cta << LT;
@@ -464,7 +465,7 @@ struct Net {
         }
 
         if constexpr (SORT) {
-            if (PK != PK_GLOBAL && p.kind == P_SORT_TILE) {
+            if (PK != PK_GLOBAL && PK != PK_MERGE && p.kind == P_SORT_TILE) {
                 for (int K = 1; K <= p.K; K++) {
                     const bool dconst = K >= LT;
                     const bool asc_c = ((cta_bits >> K) & 1) == 0;
@@ -482,9 +483,10 @@ struct Net {
             } else {
                 // MERGE: bits LT-1..0; GLOBAL: local bits C+L-1..C (the L fused
                 // global levels); the direction is fixed for the tile
-                const bool asc_c = (((p.kind == P_SORT_MERGE ? cta_bits : gidx(0)) >> p.K) & 1) == 0;
-                const int top = (p.kind == P_SORT_MERGE) ? LT - 1 : C + p.L - 1;
-                const int bottom = (p.kind == P_SORT_MERGE) ? 0 : C;
+                const bool merge = PK == PK_MERGE || (PK != PK_GLOBAL && p.kind == P_SORT_MERGE);
+                const bool asc_c = (((merge ? cta_bits : gidx(0)) >> p.K) & 1) == 0;
+                const int top = merge ? LT - 1 : C + p.L - 1;
+                const int bottom = merge ? 0 : C;
                 int b = top;
                 while (b >= bottom) {
                     if (b < s || b >= s + LOG_E) {
