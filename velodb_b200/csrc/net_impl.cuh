@@ -67,14 +67,15 @@ __global__ void __launch_bounds__(1 << LOG_NT, MB)
                                                                                      sm);
 }
 
-template <class R, int LOG_NT, int LOG_E>
+// ORCompact passes: PK_LOCAL the tile pass, PK_GLOBAL the fused global passes
+template <class R, int LOG_NT, int LOG_E, int PK>
 __global__ void __launch_bounds__(1 << LOG_NT, net_min_blocks<R, LOG_NT>())
     k_compact_pass(typename R::Cols c, NetGeom g, NetPass p, const uint32_t* __restrict__ tile_prefix)
 {
     extern __shared__ __align__(16) char sm[];
     net_pass_prologue();
     VELO_TRACE_KERNEL(TS_K_COMPACT_PASS);
-    Net<R, LOG_NT, LOG_E>::template run<false>(c, g, p, tile_prefix, blockIdx.x, sm);
+    Net<R, LOG_NT, LOG_E>::template run<false, PK>(c, g, p, tile_prefix, blockIdx.x, sm);
 }
 
 // bytes of one row that a pass reads and writes
@@ -218,7 +219,11 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
                                 : k_sort_pass<R, LOG_NT, LOG_E, N::PK_MERGE, MB>;
     auto k_global = wide_g ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MBG>
                            : k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MB>;
-    auto k_comp = k_compact_pass<R, LOG_NT, LOG_E>;
+    // ORCompact's tile pass and fused global passes are separate kernels too,
+    // each compiled without the other's code: join compaction tile pass
+    // 98.3 -> 94.2 us, global passes 69.6 -> 65.0 us
+    auto k_comp = k_compact_pass<R, LOG_NT, LOG_E, N::PK_LOCAL>;
+    auto k_comp_g = k_compact_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL>;
     const size_t smem = compact ? N::smem_bytes_compact() : N::smem_bytes_sort();
     if (smem > MAX_SMEM_BYTES)
         return einval("tile configuration needs more shared memory than a CTA can have");
@@ -227,6 +232,9 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
                              : ensure_smem(k_local, MAX_SMEM_BYTES, done_local[wide ? 1 : 0]);
     if (rc == VELO_OK && !compact)
         rc = ensure_smem(k_global, MAX_SMEM_BYTES, done_global[wide_g ? 1 : 0]);
+    static int done_compact_g[64] = {};
+    if (rc == VELO_OK && compact)
+        rc = ensure_smem(k_comp_g, MAX_SMEM_BYTES, done_compact_g);
     static int done_merge[2][64] = {};
     if (rc == VELO_OK && !compact && split_merge)
         rc = ensure_smem(k_merge, MAX_SMEM_BYTES, done_merge[wide ? 1 : 0]);
@@ -287,7 +295,7 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
                 VELO_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, c, g, q, maps, tma_fault), "network pass launch");
             }
         } else {
-            auto kern = compact ? k_comp
+            auto kern = compact ? (passes[i].kind == P_COMPACT_GLOBAL ? k_comp_g : k_comp)
                 : passes[i].kind == P_SORT_GLOBAL ? k_global
                 : passes[i].kind == P_SORT_MERGE  ? k_merge
                                                   : k_local;

@@ -501,7 +501,7 @@ struct Net {
                 }
             }
         } else {
-            if (p.kind == P_COMPACT_TILE) {
+            if (PK == PK_LOCAL || (PK != PK_GLOBAL && p.kind == P_COMPACT_TILE)) {
                 // prefix of the original marks over the tile, in local-index order
                 uint32_t* pre = reinterpret_cast<uint32_t*>(sm + smem_rows());
                 uint32_t* tmp = pre + T + T / 16;
