@@ -20,9 +20,10 @@ constexpr int net_min_blocks() { return LOG_NT <= 8 ? 2 : 1; }
 // rows of at most 12 bytes, and two-word records keyed on 32 bits (the
 // group-by's: 2^23-row sort 1.78 -> 1.63 ms), in both the in-tile and the
 // global kernels.  Two-word records compared on a whole word (the join's
-// union) only in the global kernel: their in-tile passes need 128 registers
-// (2^23 union sort: tile 353 -> 390 us at 85), while their global passes gain
-// from the third CTA (56.4 -> 53.2 us a pass).
+// union) only in the global kernel and the merge kernel: their tile sort
+// needs 128 registers (2^23 union sort: tile 353 -> 390 us at 85), while
+// their global passes (56.4 -> 53.2 us a pass) and merges (73.9 -> 71.6 us)
+// gain from the third CTA.
 template <class R>
 struct NetWide {
     static constexpr bool ok = sizeof(R) <= 12;
@@ -214,8 +215,12 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
     // merges 65.6 -> 62.1 us; key-payload rows keep the shared kernel (2^24
     // merges 111.1 -> 112.9 us with the split)
     constexpr bool split_merge = !std::is_same_v<R, RowKP>;
+    // the merges of records that keep a two-CTA tile sort (compared on a
+    // whole word) take the global kernel's three-CTA budget from 2^21 rows:
+    // 80 registers, a few spilled, join union merges 73.9 -> 71.6 us
     auto k_merge = !split_merge ? k_local
         : wide                  ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_MERGE, MBW>
+        : wide_g                ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_MERGE, MBG>
                                 : k_sort_pass<R, LOG_NT, LOG_E, N::PK_MERGE, MB>;
     auto k_global = wide_g ? k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MBG>
                            : k_sort_pass<R, LOG_NT, LOG_E, N::PK_GLOBAL, MB>;
@@ -235,9 +240,9 @@ velo_status launch_net(const typename R::Cols& c, const NetGeom& g, const std::v
     static int done_compact_g[64] = {};
     if (rc == VELO_OK && compact)
         rc = ensure_smem(k_comp_g, MAX_SMEM_BYTES, done_compact_g);
-    static int done_merge[2][64] = {};
+    static int done_merge[3][64] = {};
     if (rc == VELO_OK && !compact && split_merge)
-        rc = ensure_smem(k_merge, MAX_SMEM_BYTES, done_merge[wide ? 1 : 0]);
+        rc = ensure_smem(k_merge, MAX_SMEM_BYTES, done_merge[wide ? 1 : wide_g ? 2 : 0]);
     if (rc != VELO_OK)
         return rc;
     const int lt = N::LT;
