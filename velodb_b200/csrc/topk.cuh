@@ -151,17 +151,17 @@ __device__ __forceinline__ void tk_min(uint64_t& a0, uint64_t& a1, uint64_t b0, 
 // Runs of 16 rows (lanes 4q .. 4q + 3 hold run q, row 4(l & 3) + e in
 // register e) sorted ascending for even q, descending for odd q, are halved
 // three times: the element-wise minimum of a run pair holds its 16 best rows
-// as a bitonic sequence, which four merge levels sort again.  Each round
+// as a bitonic sequence, which four merge levels sort again.  Each halving
 // keeps only the survivors, so the rows a lane works on halve with the rows:
-//   round 1 (runs q, q ^ 1: lane ^ 4): the lower lane keeps the minima of
+//   halving 1 (runs q, q ^ 1: lane ^ 4): the lower lane keeps the minima of
 //     registers 0 and 1, the upper lane those of registers 2 and 3; the
 //     merged run p = l >> 3 is row 4(l & 3) + 2 h + j in register j
 //     (h = lane bit 2), merged by lane ^ 2, ^ 1, ^ 4 and the registers;
-//   round 2 (runs p, p ^ 1: lane ^ 8): the lower lane keeps register 0's
+//   halving 2 (runs p, p ^ 1: lane ^ 8): the lower lane keeps register 0's
 //     minimum, the upper register 1's; run l >> 4 is row
 //     i(l) = 4(l & 3) + 2((l >> 2) & 1) + ((l >> 3) & 1), one a lane,
 //     merged by lane ^ 2, ^ 1, ^ 4, ^ 8;
-//   round 3 (lane ^ 16): both halves keep the minimum and merge ascending.
+//   halving 3 (lane ^ 16): both halves keep the minimum and merge ascending.
 // On return (r0, r1) of lane l holds row i(l & 15) of the warp's 16 best,
 // ascending; lanes l and l ^ 16 hold the same row.  Every partner and
 // direction depends only on the lane.
